@@ -1,0 +1,366 @@
+"""gstore_b200 — B200-native engine for G-Store's tile-grid edge scan.
+
+Python face of ``libgstore_cuda.so`` (declared in ``include/gstore_cuda.h``):
+a thin ctypes layer over the C ABI, used by the tests and the benchmark.  The
+reference-compatible host (``gstoreu``/``gstored`` and the ``algo_t`` adapters)
+is C++ under ``csrc/host``; this module mirrors the same objects:
+
+* :class:`Context`  — ``gs_create``: device, HBM tile budget, directed flag
+* :class:`Graph`    — a resident tile grid (``read_grid_in_mem`` +
+  ``read_degree_in_mem``, gstore.cpp:2953-3011)
+* :class:`State`    — one algorithm run with the ``algo_t`` protocol
+  (``init`` / ``algo_mem_part`` = :meth:`State.sweep` /
+  ``iteration_finalize`` = :meth:`State.finalize`, algo.h:38-44)
+
+There is no CPU fallback: if the CUDA library is missing or no GPU is
+present, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libgstore_cuda.so"
+
+GS_ALGO_BFS, GS_ALGO_PAGERANK, GS_ALGO_KCORE, GS_ALGO_WCC = 0, 1, 2, 3
+ALGOS = {"bfs": GS_ALGO_BFS, "pagerank": GS_ALGO_PAGERANK, "pr": GS_ALGO_PAGERANK,
+         "kcore": GS_ALGO_KCORE, "wcc": GS_ALGO_WCC}
+STATUS = {0: "GS_OK", 1: "GS_ERR_CUDA", 2: "GS_ERR_OOM", 3: "GS_ERR_FORMAT", 4: "GS_ERR_TIMEOUT",
+          5: "GS_ERR_ARG", 6: "GS_ERR_RANGE", 7: "GS_ERR_STATE", 8: "GS_ERR_UNSUPPORTED"}
+
+# Every exported symbol of the C ABI, as declared in include/gstore_cuda.h.
+ABI_SYMBOLS = [
+    "gs_create", "gs_destroy", "gs_last_error", "gs_set_stream", "gs_profile", "gs_kernel_time",
+    "gs_launch_count",
+    "gs_geometry", "gs_upload_graph", "gs_upload_graph_device", "gs_graph_free", "gs_graph_info",
+    "gs_graph_degree", "gs_state_create", "gs_state_free", "gs_state_reset", "gs_sweep", "gs_finalize", "gs_run",
+    "gs_download", "gs_result_count", "gs_bfs_stats", "gs_pagerank_compat",
+    "gs_kron_generate_device", "gs_kron_generate", "gs_convert", "gs_graph_download",
+]
+
+
+class GStoreError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """Load libgstore_cuda.so (built in-tree by ``python -m gstore_b200.build``)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"CUDA engine not built: {LIB_PATH} is missing "
+                               "(run python -m gstore_b200.build)")
+        L = C.CDLL(str(LIB_PATH))
+        vp, u64, i64, i32 = C.c_void_p, C.c_uint64, C.c_int64, C.c_int
+        pvp = C.POINTER(C.c_void_p)
+        pu64 = C.POINTER(C.c_uint64)
+        sig = {
+            "gs_create": [pvp, i32, u64, i32],
+            "gs_destroy": [vp],
+            "gs_set_stream": [vp, vp],
+            "gs_profile": [vp, i32],
+            "gs_kernel_time": [vp, i32, pu64, C.POINTER(C.c_double), pu64],
+            "gs_launch_count": [vp, pu64],
+            "gs_geometry": [u64, i32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), pu64],
+            "gs_upload_graph": [vp, vp, u64, vp, u64, vp, u64, pvp],
+            "gs_upload_graph_device": [vp, vp, u64, vp, u64, vp, u64, pvp],
+            "gs_graph_free": [vp],
+            "gs_graph_info": [vp, pu64, pu64, pu64, pu64],
+            "gs_graph_degree": [vp, vp],
+            "gs_state_create": [vp, i32, i64, pvp],
+            "gs_state_free": [vp],
+            "gs_state_reset": [vp, i64],
+            "gs_sweep": [vp, vp, i32],
+            "gs_finalize": [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int)],
+            "gs_run": [vp, C.POINTER(C.c_int64)],
+            "gs_download": [vp, i32, vp, u64],
+            "gs_result_count": [vp, pu64],
+            "gs_bfs_stats": [vp, pu64, vp, i32, C.POINTER(C.c_int), vp],
+            "gs_pagerank_compat": [vp, i32],
+            "gs_kron_generate_device": [vp, i32, i64, u64, u64, vp],
+            "gs_kron_generate": [vp, i32, i64, u64, u64, vp],
+            "gs_convert": [vp, vp, u64, i32, u64, pvp],
+            "gs_graph_download": [vp, vp, vp, vp],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int32
+        L.gs_last_error.argtypes = [vp]
+        L.gs_last_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "arrays must be C-contiguous"
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def geometry(V: int, directed: bool = False):
+    """(p, p_s, number of .start entries) for vertex count V (grid::init -v)."""
+    p, ps, n = C.c_uint32(), C.c_uint32(), C.c_uint64()
+    lib().gs_geometry(V, int(directed), C.byref(p), C.byref(ps), C.byref(n))
+    return p.value, ps.value, n.value
+
+
+def read_tile_files(prefix, V: int | None = None, with_degree: bool = True):
+    """Read <prefix>.start / .grid / .degree as the reference writes them."""
+    prefix = str(prefix)
+    start = np.fromfile(prefix + ".start", np.uint64)
+    grid = np.fromfile(prefix + ".grid", np.uint32)
+    degree = None
+    if with_degree and os.path.exists(prefix + ".degree"):
+        degree = np.fromfile(prefix + ".degree", np.int32, count=-1 if V is None else V)
+    return start, grid, degree
+
+
+def write_tile_files(prefix, start, grid, degree):
+    """Write .grid/.start/.degree (grid::save_grid, gstore.cpp:2818-2917)."""
+    prefix = str(prefix)
+    np.ascontiguousarray(grid, np.uint32).tofile(prefix + ".grid")
+    np.ascontiguousarray(start, np.uint64).tofile(prefix + ".start")
+    if degree is not None:
+        np.ascontiguousarray(degree, np.int32).tofile(prefix + ".degree")
+
+
+class Context:
+    """A device context (gs_create)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0, directed: bool = False):
+        self._h = C.c_void_p()
+        st = lib().gs_create(C.byref(self._h), device, hbm_budget, int(directed))
+        if st != 0:
+            raise GStoreError(st, "gs_create failed (no usable CUDA device?)")
+        self.directed = bool(directed)
+
+    def _check(self, st):
+        if st != 0:
+            raise GStoreError(st, lib().gs_last_error(self._h).decode())
+
+    def close(self):
+        if self._h:
+            lib().gs_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, cuda_stream_ptr: int | None):
+        self._check(lib().gs_set_stream(self._h, C.c_void_p(cuda_stream_ptr or 0)))
+
+    def profile(self, enable: bool = True):
+        self._check(lib().gs_profile(self._h, int(enable)))
+
+    def kernel_time(self, algo: int):
+        n, ms, b = C.c_uint64(), C.c_double(), C.c_uint64()
+        self._check(lib().gs_kernel_time(self._h, algo, C.byref(n), C.byref(ms), C.byref(b)))
+        return n.value, ms.value, b.value
+
+    def launches(self) -> int:
+        """Kernels launched by this context so far."""
+        n = C.c_uint64()
+        self._check(lib().gs_launch_count(self._h, C.byref(n)))
+        return n.value
+
+    def upload(self, start, grid, degree, V: int) -> "Graph":
+        start = np.ascontiguousarray(start, np.uint64)
+        grid = np.ascontiguousarray(grid, np.uint32)
+        if degree is not None:
+            degree = np.ascontiguousarray(degree, np.int32)
+            assert degree.size >= V, "degree array shorter than V"
+        h = C.c_void_p()
+        self._check(lib().gs_upload_graph(self._h, _ptr(start), start.size, _ptr(grid), grid.size,
+                                          _ptr(degree), V, C.byref(h)))
+        return Graph(self, h)
+
+    def upload_device(self, d_start: int, n_start: int, d_grid: int, n_edges: int, d_degree: int | None,
+                      V: int) -> "Graph":
+        h = C.c_void_p()
+        self._check(lib().gs_upload_graph_device(self._h, C.c_void_p(d_start), n_start, C.c_void_p(d_grid),
+                                                 n_edges, C.c_void_p(d_degree or 0), V, C.byref(h)))
+        return Graph(self, h)
+
+    def kron_generate(self, scale: int, edgefactor: int = 16, seed1: int = 1, seed2: int = 2) -> np.ndarray:
+        out = np.empty(((edgefactor << scale), 2), np.uint32)
+        self._check(lib().gs_kron_generate(self._h, scale, edgefactor, seed1, seed2, _ptr(out)))
+        return out
+
+    def kron_generate_device(self, scale: int, edgefactor: int, seed1: int, seed2: int, d_pairs: int):
+        self._check(lib().gs_kron_generate_device(self._h, scale, edgefactor, seed1, seed2,
+                                                  C.c_void_p(d_pairs)))
+
+    def convert(self, pairs, V: int, n_pairs: int | None = None) -> "Graph":
+        """Edge pairs (numpy (m,2) uint32 on the host, or an int device pointer
+        with n_pairs) -> resident graph (the "-c 1" converter)."""
+        h = C.c_void_p()
+        if isinstance(pairs, int):
+            self._check(lib().gs_convert(self._h, C.c_void_p(pairs), n_pairs, 1, V, C.byref(h)))
+        else:
+            pairs = np.ascontiguousarray(pairs, np.uint32)
+            self._check(lib().gs_convert(self._h, _ptr(pairs), pairs.size // 2, 0, V, C.byref(h)))
+        return Graph(self, h)
+
+
+class Graph:
+    """A resident tile grid (gs_graph)."""
+
+    def __init__(self, ctx: Context, handle):
+        self.ctx = ctx
+        self._h = handle
+        e, t, i, v = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+        ctx._check(lib().gs_graph_info(self._h, C.byref(e), C.byref(t), C.byref(i), C.byref(v)))
+        self.n_edges, self.n_tiles, self.n_items, self.V = e.value, t.value, i.value, v.value
+        self.directed = ctx.directed
+
+    def free(self):
+        if self._h:
+            lib().gs_graph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def degree(self) -> np.ndarray:
+        out = np.empty(self.V, np.int32)
+        self.ctx._check(lib().gs_graph_degree(self._h, _ptr(out)))
+        return out
+
+    def download(self):
+        _, _, ns = geometry(self.V, self.directed)
+        start = np.empty(ns, np.uint64)
+        grid = np.empty(self.n_edges, np.uint32)
+        degree = np.empty(self.V, np.int32)
+        self.ctx._check(lib().gs_graph_download(self._h, _ptr(start), _ptr(grid), _ptr(degree)))
+        return start, grid, degree
+
+    def state(self, algo, arg: int = 0) -> "State":
+        a = ALGOS[algo] if isinstance(algo, str) else int(algo)
+        h = C.c_void_p()
+        self.ctx._check(lib().gs_state_create(self._h, a, arg, C.byref(h)))
+        return State(self, h, a)
+
+    # convenience: whole runs ------------------------------------------------
+    def bfs(self, root: int) -> np.ndarray:
+        with self.state("bfs", root) as s:
+            s.run()
+            return s.download()
+
+    def pagerank(self, iterations: int = 5, compat: bool = False):
+        with self.state("pagerank", iterations) as s:
+            if compat:
+                s.compat()
+            s.run()
+            return s.download(0), s.download(1)
+
+    def wcc(self):
+        with self.state("wcc") as s:
+            s.run()
+            return s.download(), s.count()
+
+    def kcore(self, k: int):
+        with self.state("kcore", k) as s:
+            s.run()
+            return s.download(), s.count()
+
+
+class State:
+    """One algorithm run (gs_state): the algo_t protocol on the device."""
+
+    def __init__(self, graph: Graph, handle, algo: int):
+        self.graph = graph
+        self._h = handle
+        self.algo = algo
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
+
+    def free(self):
+        if self._h:
+            lib().gs_state_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        self.graph.ctx._check(st)
+
+    def reset(self, arg: int):
+        """Start a new run (new root / iterations / k) reusing the device arrays."""
+        self._check(lib().gs_state_reset(self._h, arg))
+
+    def compat(self, enable: bool = True):
+        self._check(lib().gs_pagerank_compat(self._h, int(enable)))
+
+    def sweep(self):
+        """algo_mem_part over every resident tile (algo.h:40)."""
+        self._check(lib().gs_sweep(self._h, None, 0))
+
+    def finalize(self):
+        """iteration_finalize(): returns (frontier, done)."""
+        f, d = C.c_int64(), C.c_int()
+        self._check(lib().gs_finalize(self._h, C.byref(f), C.byref(d)))
+        return f.value, bool(d.value)
+
+    def run(self) -> int:
+        n = C.c_int64()
+        self._check(lib().gs_run(self._h, C.byref(n)))
+        return n.value
+
+    def download(self, what: int = 0) -> np.ndarray:
+        V = self.graph.V
+        dt = {GS_ALGO_BFS: np.uint8, GS_ALGO_PAGERANK: np.float32, GS_ALGO_KCORE: np.int32,
+              GS_ALGO_WCC: np.uint32}[self.algo]
+        out = np.empty(V, dt)
+        self._check(lib().gs_download(self._h, what, _ptr(out), out.nbytes))
+        return out
+
+    def download_into(self, out: np.ndarray, what: int = 0) -> np.ndarray:
+        """Download into a caller-provided (e.g. pinned) host array."""
+        self._check(lib().gs_download(self._h, what, _ptr(out), out.nbytes))
+        return out
+
+    def count(self) -> int:
+        c = C.c_uint64()
+        self._check(lib().gs_result_count(self._h, C.byref(c)))
+        return c.value
+
+    def bfs_stats(self, max_levels: int = 256):
+        e = C.c_uint64()
+        swept = np.zeros(max_levels, np.uint64)
+        counts = np.zeros(max_levels, np.uint64)
+        nl = C.c_int()
+        self._check(lib().gs_bfs_stats(self._h, C.byref(e), _ptr(swept), max_levels, C.byref(nl),
+                                       _ptr(counts)))
+        n = nl.value
+        return {"edges_in_component": e.value, "swept": swept[:n].copy(), "level_counts": counts[:n].copy()}

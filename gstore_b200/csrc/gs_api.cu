@@ -1,0 +1,624 @@
+// C-ABI entry points of libgstore_cuda.so: contexts, resident graphs and the
+// algo_t-style state machine (init / sweep / finalize / download).
+#include "gs_internal.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+
+// ------------------------------------------------------------------ errors --
+gs_status gs_fail(gs_ctx* ctx, gs_status code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+gs_status gs_cuda_fail(gs_ctx* ctx, cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return gs_fail(ctx, GS_ERR_OOM, m);
+    }
+    return gs_fail(ctx, GS_ERR_CUDA, m);
+}
+
+gs_status gs_dev_alloc(gs_ctx* ctx, void** ptr, size_t bytes) {
+    *ptr = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        return gs_cuda_fail(ctx, e, "cudaMalloc");
+    }
+    return GS_OK;
+}
+
+void gs_dev_free(void* ptr) {
+    if (ptr) cudaFree(ptr);
+}
+
+void gs_geometry_of(uint64_t V, int directed, uint32_t* p, uint32_t* p_s, uint64_t* n_tiles) {
+    // grid::init "-v" (gstore.cpp:152-161): p = ceil(V / 2^24), p_s = 256 p.
+    uint64_t pp = (V >> kGroupBits) + ((V & ((1ull << kGroupBits) - 1)) != 0);
+    if (pp == 0) pp = 1;
+    uint64_t ps = pp * kGroupTiles;
+    if (p) *p = (uint32_t)pp;
+    if (p_s) *p_s = (uint32_t)ps;
+    if (n_tiles) *n_tiles = directed ? ps * ps : ps * (ps + 1) / 2;  // calc_total_part
+}
+
+void gs_timer_begin(gs_ctx* ctx) {
+    if (ctx->profile) cudaEventRecord(ctx->ev0, ctx->stream);
+}
+
+void gs_timer_end(gs_ctx* ctx, int algo, uint64_t bytes) {
+    if (!ctx->profile) return;
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    cudaEventSynchronize(ctx->ev1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    KernelTimes& k = ctx->ktime[algo & 3];
+    k.launches += 1;
+    k.ms += ms;
+    k.bytes += bytes;
+}
+
+extern "C" {
+
+const char* gs_last_error(const gs_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+gs_status gs_geometry(uint64_t V, int directed, uint32_t* p, uint32_t* p_s,
+                      uint64_t* n_start_entries) {
+    uint64_t T;
+    gs_geometry_of(V, directed, p, p_s, &T);
+    if (n_start_entries) *n_start_entries = T + 1;
+    return GS_OK;
+}
+
+gs_status gs_create(gs_ctx** out, int device, uint64_t hbm_budget_bytes, int directed) {
+    if (!out) return GS_ERR_ARG;
+    *out = nullptr;
+    gs_ctx* ctx = new (std::nothrow) gs_ctx();
+    if (!ctx) return GS_ERR_OOM;
+    ctx->device = device;
+    ctx->budget = hbm_budget_bytes;
+    ctx->directed = directed ? 1 : 0;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_scalars, 64 * sizeof(uint64_t));
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->h_scalars, 64 * sizeof(uint64_t));
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) {
+        gs_status st = (e == cudaErrorMemoryAllocation) ? GS_ERR_OOM : GS_ERR_CUDA;
+        gs_destroy(ctx);
+        return st;
+    }
+    ctx->own_stream = true;
+    *out = ctx;
+    return GS_OK;
+}
+
+gs_status gs_destroy(gs_ctx* ctx) {
+    if (!ctx) return GS_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->d_scalars) cudaFree(ctx->d_scalars);
+    if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);
+    delete ctx;
+    return GS_OK;
+}
+
+gs_status gs_set_stream(gs_ctx* ctx, void* cuda_stream) {
+    if (!ctx) return GS_ERR_ARG;
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    if (cuda_stream) {
+        ctx->stream = (cudaStream_t)cuda_stream;
+        ctx->own_stream = false;
+    } else {
+        GS_CHECK_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        ctx->own_stream = true;
+    }
+    return GS_OK;
+}
+
+gs_status gs_profile(gs_ctx* ctx, int enable) {
+    if (!ctx) return GS_ERR_ARG;
+    ctx->profile = enable != 0;
+    for (auto& k : ctx->ktime) k = KernelTimes();
+    return GS_OK;
+}
+
+gs_status gs_launch_count(const gs_ctx* ctx, uint64_t* launches) {
+    if (!ctx || !launches) return GS_ERR_ARG;
+    *launches = ctx->launches;
+    return GS_OK;
+}
+
+gs_status gs_kernel_time(gs_ctx* ctx, int algo, uint64_t* launches, double* total_ms,
+                         uint64_t* bytes) {
+    if (!ctx || algo < 0 || algo > 3) return GS_ERR_ARG;
+    if (launches) *launches = ctx->ktime[algo].launches;
+    if (total_ms) *total_ms = ctx->ktime[algo].ms;
+    if (bytes) *bytes = ctx->ktime[algo].bytes;
+    return GS_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ graph --
+static void free_graph_arrays(gs_graph* g) {
+    gs_dev_free(g->d_rec);
+    gs_dev_free(g->d_items);
+    gs_dev_free(g->d_tile_off);
+    gs_dev_free(g->d_tile_rc);
+    gs_dev_free(g->d_degree);
+    g->d_rec = nullptr;
+    g->d_items = nullptr;
+    g->d_tile_off = nullptr;
+    g->d_tile_rc = nullptr;
+    g->d_degree = nullptr;
+}
+
+// Builds the non-empty tile table and the work items from the host .start
+// array, walking the stored tiles in file order (the loops of grid::*_mmap,
+// gstore.cpp:2520-2559), and uploads them.
+static gs_status build_tables(gs_graph* g) {
+    gs_ctx* ctx = g->ctx;
+    const std::vector<uint64_t>& st = g->h_start;
+    std::vector<uint64_t>& tile_off = g->h_tile_off;
+    std::vector<uint32_t>& tile_rc = g->h_tile_rc;
+    std::vector<gs_item> items;
+    tile_off.clear();
+    tile_rc.clear();
+    tile_off.reserve(1024);
+    uint64_t t = 0;
+    const uint64_t p = g->p;
+    for (uint64_t gi = 0; gi < p; ++gi) {
+        for (uint64_t gj = g->directed ? 0 : gi; gj < p; ++gj) {
+            for (uint64_t m = 0; m < kGroupTiles; ++m) {
+                uint64_t n0 = (!g->directed && gi == gj) ? m : 0;
+                for (uint64_t n = n0; n < kGroupTiles; ++n, ++t) {
+                    uint64_t b = st[t], e = st[t + 1];
+                    if (e == b) continue;
+                    uint32_t row = (uint32_t)(gi * kGroupTiles + m);
+                    uint32_t col = (uint32_t)(gj * kGroupTiles + n);
+                    if (row >= g->nw || col >= g->nw)
+                        return gs_fail(ctx, GS_ERR_FORMAT,
+                                       "tile (" + std::to_string(row) + "," + std::to_string(col) +
+                                           ") holds records beyond the vertex count");
+                    uint32_t rc = (row << 16) | col;
+                    tile_off.push_back(b);
+                    tile_rc.push_back(rc);
+                    for (uint64_t x = b; x < e; x += kItemRecords) {
+                        gs_item it;
+                        it.beg = x;
+                        it.cnt = (uint32_t)std::min<uint64_t>(kItemRecords, e - x);
+                        it.rc = rc;
+                        items.push_back(it);
+                    }
+                }
+            }
+        }
+    }
+    tile_off.push_back(st[t]);
+    g->T = tile_rc.size();
+    g->I = items.size();
+    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_tile_off, tile_off.size() * sizeof(uint64_t)));
+    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_tile_rc, std::max<size_t>(1, tile_rc.size()) * sizeof(uint32_t)));
+    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_items, std::max<size_t>(1, items.size()) * sizeof(gs_item)));
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_tile_off, tile_off.data(), tile_off.size() * sizeof(uint64_t),
+                                       cudaMemcpyHostToDevice, ctx->stream));
+    if (!tile_rc.empty())
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_tile_rc, tile_rc.data(), tile_rc.size() * sizeof(uint32_t),
+                                           cudaMemcpyHostToDevice, ctx->stream));
+    if (!items.empty())
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_items, items.data(), items.size() * sizeof(gs_item),
+                                           cudaMemcpyHostToDevice, ctx->stream));
+    // The host vectors die at return: wait for the copies.
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return GS_OK;
+}
+
+static gs_status check_start(gs_graph* g, uint64_t n_start, uint64_t n_edges) {
+    gs_ctx* ctx = g->ctx;
+    if (n_start != g->T_all + 1)
+        return gs_fail(ctx, GS_ERR_FORMAT,
+                       "start has " + std::to_string(n_start) + " entries, geometry needs " +
+                           std::to_string(g->T_all + 1));
+    const std::vector<uint64_t>& st = g->h_start;
+    if (st[0] != 0) return gs_fail(ctx, GS_ERR_FORMAT, "start[0] != 0");
+    for (uint64_t t = 0; t < g->T_all; ++t)
+        if (st[t + 1] < st[t])
+            return gs_fail(ctx, GS_ERR_FORMAT, "start decreases at tile " + std::to_string(t));
+    if (st[g->T_all] != n_edges)
+        return gs_fail(ctx, GS_ERR_FORMAT,
+                       "start[last] = " + std::to_string(st[g->T_all]) + " but grid holds " +
+                           std::to_string(n_edges) + " records");
+    return GS_OK;
+}
+
+static gs_status finish_upload(gs_graph* g, const int32_t* degree, bool degree_on_device) {
+    gs_ctx* ctx = g->ctx;
+    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_degree, g->N * sizeof(int32_t)));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(g->d_degree, 0, g->N * sizeof(int32_t), ctx->stream));
+    if (degree) {
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_degree, degree, g->V * sizeof(int32_t),
+                                           degree_on_device ? cudaMemcpyDeviceToDevice
+                                                            : cudaMemcpyHostToDevice,
+                                           ctx->stream));
+    }
+    GS_TRY(build_tables(g));
+    if ((g->V & 0xFFFF) != 0 && g->E > 0) {
+        int* d_flag = (int*)ctx->d_scalars;
+        GS_CHECK_CUDA(ctx, cudaMemsetAsync(d_flag, 0, sizeof(int), ctx->stream));
+        GS_TRY(launch_validate_records(g, d_flag));
+        int h_flag = 0;
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(&h_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        if (h_flag) return gs_fail(ctx, GS_ERR_FORMAT, "a record addresses a vertex >= V");
+    }
+    if (!degree) {
+        GS_TRY(launch_degree_from_records(g));
+        g->degree_from_records = true;
+    }
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return GS_OK;
+}
+
+static gs_status new_graph(gs_ctx* ctx, uint64_t V, gs_graph** out) {
+    if (!ctx || !out || V == 0 || V > (1ull << 32)) return gs_fail(ctx, GS_ERR_ARG, "bad vertex count");
+    GS_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+    gs_graph* g = new (std::nothrow) gs_graph();
+    if (!g) return GS_ERR_OOM;
+    g->ctx = ctx;
+    g->directed = ctx->directed;
+    g->V = V;
+    gs_geometry_of(V, g->directed, &g->p, &g->p_s, &g->T_all);
+    g->nw = (uint32_t)((V + 0xFFFF) >> kTileBits);
+    g->N = (uint64_t)g->nw << kTileBits;
+    *out = g;
+    return GS_OK;
+}
+
+// Builds a resident graph around records already in device memory
+// (d_rec is adopted; d_start and d_degree are copied and stay the caller's).
+gs_status gs_graph_adopt(gs_ctx* ctx, uint64_t V, const uint64_t* d_start, uint64_t n_start, uint32_t* d_rec,
+                         uint64_t n_edges, const int32_t* d_degree, gs_graph** out) {
+    *out = nullptr;
+    gs_graph* g = nullptr;
+    gs_status st = new_graph(ctx, V, &g);
+    if (st != GS_OK) {
+        gs_dev_free(d_rec);
+        return st;
+    }
+    g->d_rec = d_rec;
+    g->E = n_edges;
+    g->h_start.resize(n_start);
+    cudaError_t e = cudaMemcpyAsync(g->h_start.data(), d_start, n_start * 8, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "copy start");
+    if (st == GS_OK) st = check_start(g, n_start, n_edges);
+    if (st == GS_OK) st = finish_upload(g, d_degree, true);
+    if (st != GS_OK) {
+        free_graph_arrays(g);
+        delete g;
+        return st;
+    }
+    *out = g;
+    return GS_OK;
+}
+
+extern "C" {
+
+gs_status gs_upload_graph(gs_ctx* ctx, const uint64_t* start, uint64_t n_start,
+                          const uint32_t* grid, uint64_t n_edges, const int32_t* degree,
+                          uint64_t V, gs_graph** out) {
+    if (!ctx || !start || !out || (n_edges && !grid)) return gs_fail(ctx, GS_ERR_ARG, "null argument");
+    *out = nullptr;
+    gs_graph* g = nullptr;
+    GS_TRY(new_graph(ctx, V, &g));
+    g->h_start.assign(start, start + std::min<uint64_t>(n_start, g->T_all + 1));
+    gs_status st = check_start(g, n_start, n_edges);
+    if (st == GS_OK && ctx->budget && n_edges * 4 > ctx->budget)
+        st = gs_fail(ctx, GS_ERR_OOM, "grid exceeds the HBM tile budget; use the streamed sweep");
+    if (st == GS_OK) {
+        g->E = n_edges;
+        st = gs_dev_alloc(ctx, (void**)&g->d_rec, std::max<uint64_t>(1, n_edges) * 4);
+        if (st == GS_OK && n_edges) {
+            cudaError_t e = cudaMemcpyAsync(g->d_rec, grid, n_edges * 4, cudaMemcpyHostToDevice, ctx->stream);
+            if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "cudaMemcpyAsync(grid)");
+        }
+    }
+    if (st == GS_OK) st = finish_upload(g, degree, false);
+    if (st != GS_OK) {
+        free_graph_arrays(g);
+        delete g;
+        return st;
+    }
+    *out = g;
+    return GS_OK;
+}
+
+gs_status gs_upload_graph_device(gs_ctx* ctx, const uint64_t* d_start, uint64_t n_start,
+                                 const uint32_t* d_grid, uint64_t n_edges,
+                                 const int32_t* d_degree, uint64_t V, gs_graph** out) {
+    if (!ctx || !d_start || !out || (n_edges && !d_grid)) return gs_fail(ctx, GS_ERR_ARG, "null argument");
+    *out = nullptr;
+    gs_graph* g = nullptr;
+    GS_TRY(new_graph(ctx, V, &g));
+    gs_status st = GS_OK;
+    if (n_start != g->T_all + 1) st = check_start(g, n_start, n_edges);
+    if (st == GS_OK) {
+        g->h_start.resize(n_start);
+        cudaError_t e = cudaMemcpyAsync(g->h_start.data(), d_start, n_start * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "copy start");
+    }
+    if (st == GS_OK) st = check_start(g, n_start, n_edges);
+    if (st == GS_OK) {
+        g->E = n_edges;
+        st = gs_dev_alloc(ctx, (void**)&g->d_rec, std::max<uint64_t>(1, n_edges) * 4);
+        if (st == GS_OK && n_edges) {
+            cudaError_t e = cudaMemcpyAsync(g->d_rec, d_grid, n_edges * 4, cudaMemcpyDeviceToDevice, ctx->stream);
+            if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "cudaMemcpyAsync(grid)");
+        }
+    }
+    if (st == GS_OK) st = finish_upload(g, d_degree, true);
+    if (st != GS_OK) {
+        free_graph_arrays(g);
+        delete g;
+        return st;
+    }
+    *out = g;
+    return GS_OK;
+}
+
+gs_status gs_graph_free(gs_graph* g) {
+    if (!g) return GS_OK;
+    cudaStreamSynchronize(g->ctx->stream);
+    free_graph_arrays(g);
+    delete g;
+    return GS_OK;
+}
+
+gs_status gs_graph_info(const gs_graph* g, uint64_t* n_edges, uint64_t* n_tiles, uint64_t* n_items,
+                        uint64_t* V) {
+    if (!g) return GS_ERR_ARG;
+    if (n_edges) *n_edges = g->E;
+    if (n_tiles) *n_tiles = g->T;
+    if (n_items) *n_items = g->I;
+    if (V) *V = g->V;
+    return GS_OK;
+}
+
+gs_status gs_graph_degree(const gs_graph* g, int32_t* host_degree) {
+    if (!g || !host_degree) return GS_ERR_ARG;
+    GS_CHECK_CUDA(g->ctx, cudaMemcpyAsync(host_degree, g->d_degree, g->V * 4, cudaMemcpyDeviceToHost,
+                                          g->ctx->stream));
+    GS_CHECK_CUDA(g->ctx, cudaStreamSynchronize(g->ctx->stream));
+    return GS_OK;
+}
+
+gs_status gs_graph_download(const gs_graph* g, uint64_t* host_start, uint32_t* host_grid,
+                            int32_t* host_degree) {
+    if (!g) return GS_ERR_ARG;
+    gs_ctx* ctx = g->ctx;
+    if (host_start) std::memcpy(host_start, g->h_start.data(), g->h_start.size() * 8);
+    if (host_grid && g->E)
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(host_grid, g->d_rec, g->E * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (host_degree)
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(host_degree, g->d_degree, g->V * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return GS_OK;
+}
+
+// ------------------------------------------------------------------ state --
+gs_status gs_state_create(gs_graph* g, gs_algo algo, int64_t arg, gs_state** out) {
+    if (!g || !out) return GS_ERR_ARG;
+    *out = nullptr;
+    gs_ctx* ctx = g->ctx;
+    if (algo == GS_ALGO_KCORE && g->directed)
+        return gs_fail(ctx, GS_ERR_UNSUPPORTED, "Kcore not applicable for directed graphs");
+    if (algo == GS_ALGO_BFS && (arg < 0 || (uint64_t)arg >= g->V))
+        return gs_fail(ctx, GS_ERR_ARG, "BFS root out of range");
+    if (algo == GS_ALGO_PAGERANK && arg < 1) return gs_fail(ctx, GS_ERR_ARG, "iterations < 1");
+    gs_state* s = new (std::nothrow) gs_state();
+    if (!s) return GS_ERR_OOM;
+    s->g = g;
+    s->algo = algo;
+    s->arg = arg;
+    gs_status st = GS_ERR_ARG;
+    switch (algo) {
+        case GS_ALGO_BFS: st = bfs_init(s); break;
+        case GS_ALGO_PAGERANK: st = pr_init(s); break;
+        case GS_ALGO_WCC: st = wcc_init(s); break;
+        case GS_ALGO_KCORE: st = kcore_init(s); break;
+    }
+    if (st != GS_OK) {
+        gs_state_free(s);
+        return st;
+    }
+    *out = s;
+    return GS_OK;
+}
+
+gs_status gs_state_reset(gs_state* s, int64_t arg) {
+    if (!s) return GS_ERR_ARG;
+    gs_graph* g = s->g;
+    if (s->algo == GS_ALGO_BFS && (arg < 0 || (uint64_t)arg >= g->V))
+        return gs_fail(g->ctx, GS_ERR_ARG, "BFS root out of range");
+    if (s->algo == GS_ALGO_PAGERANK && arg < 1) return gs_fail(g->ctx, GS_ERR_ARG, "iterations < 1");
+    s->arg = arg;
+    s->step = 0;
+    s->done = false;
+    s->last_count = 0;
+    switch (s->algo) {
+        case GS_ALGO_BFS: return bfs_init(s);
+        case GS_ALGO_PAGERANK: return pr_init(s);
+        case GS_ALGO_WCC: return wcc_init(s);
+        case GS_ALGO_KCORE: return kcore_init(s);
+    }
+    return GS_ERR_ARG;
+}
+
+gs_status gs_state_free(gs_state* s) {
+    if (!s) return GS_OK;
+    cudaStreamSynchronize(s->g->ctx->stream);
+    gs_dev_free(s->d_depth);
+    gs_dev_free(s->d_front);
+    gs_dev_free(s->d_visited);
+    gs_dev_free(s->d_act);
+    gs_dev_free(s->d_act_next);
+    gs_dev_free(s->d_x);
+    gs_dev_free(s->d_y);
+    gs_dev_free(s->d_r);
+    gs_dev_free(s->d_parent);
+    gs_dev_free(s->d_touched);
+    gs_dev_free(s->d_deg);
+    gs_dev_free(s->d_kactive);
+    delete s;
+    return GS_OK;
+}
+
+gs_status gs_pagerank_compat(gs_state* s, int enable) {
+    if (!s || s->algo != GS_ALGO_PAGERANK) return GS_ERR_ARG;
+    if (s->step != 0) return gs_fail(s->g->ctx, GS_ERR_STATE, "compat must precede the first sweep");
+    s->compat = enable != 0;
+    return GS_OK;
+}
+
+gs_status gs_sweep(gs_state* s, const gs_segment* segs, int n_segs) {
+    if (!s) return GS_ERR_ARG;
+    if (segs || n_segs) return gs_fail(s->g->ctx, GS_ERR_UNSUPPORTED, "segment sweeps need a streamed graph");
+    if (s->done) return gs_fail(s->g->ctx, GS_ERR_STATE, "algorithm already finished");
+    switch (s->algo) {
+        case GS_ALGO_BFS: return bfs_sweep(s);
+        case GS_ALGO_PAGERANK: return pr_sweep(s);
+        case GS_ALGO_WCC: return wcc_sweep(s);
+        case GS_ALGO_KCORE: return kcore_sweep(s);
+    }
+    return GS_ERR_ARG;
+}
+
+gs_status gs_finalize(gs_state* s, int64_t* frontier_out, int* done_out) {
+    if (!s) return GS_ERR_ARG;
+    int64_t f = 0;
+    int d = 0;
+    gs_status st = GS_ERR_ARG;
+    switch (s->algo) {
+        case GS_ALGO_BFS: st = bfs_finalize(s, &f, &d); break;
+        case GS_ALGO_PAGERANK: st = pr_finalize(s, &f, &d); break;
+        case GS_ALGO_WCC: st = wcc_finalize(s, &f, &d); break;
+        case GS_ALGO_KCORE: st = kcore_finalize(s, &f, &d); break;
+    }
+    if (st != GS_OK) return st;
+    s->last_count = f;
+    s->done = d != 0;
+    if (frontier_out) *frontier_out = f;
+    if (done_out) *done_out = d;
+    return GS_OK;
+}
+
+gs_status gs_run(gs_state* s, int64_t* steps_out) {
+    if (!s) return GS_ERR_ARG;
+    int64_t steps = 0;
+    if (s->algo == GS_ALGO_KCORE && s->step == 0 && !s->done) {
+        // kcore_mmap runs one iteration_finalize before the first sweep
+        // (gstore.cpp:2725-2726).
+        int64_t f;
+        int d;
+        GS_TRY(gs_finalize(s, &f, &d));
+    }
+    while (!s->done) {
+        GS_TRY(gs_sweep(s, nullptr, 0));
+        ++steps;
+        int64_t f;
+        int d;
+        GS_TRY(gs_finalize(s, &f, &d));
+    }
+    if (steps_out) *steps_out = steps;
+    return GS_OK;
+}
+
+gs_status gs_download(gs_state* s, int what, void* host_dst, uint64_t bytes) {
+    if (!s || !host_dst) return GS_ERR_ARG;
+    gs_graph* g = s->g;
+    gs_ctx* ctx = g->ctx;
+    const void* src = nullptr;
+    uint64_t need = 0;
+    uint32_t* tmp = nullptr;
+    switch (s->algo) {
+        case GS_ALGO_BFS: src = s->d_depth; need = g->V; break;
+        case GS_ALGO_PAGERANK: src = what == 1 ? s->d_x : s->d_r; need = g->V * 4; break;
+        case GS_ALGO_KCORE: src = s->d_deg; need = g->V * 4; break;
+        case GS_ALGO_WCC: {
+            GS_TRY(gs_dev_alloc(ctx, (void**)&tmp, g->N * 4));
+            uint64_t cnt;
+            gs_status st = gs_wcc_labels(s, tmp, &cnt);
+            if (st != GS_OK) {
+                gs_dev_free(tmp);
+                return st;
+            }
+            src = tmp;
+            need = g->V * 4;
+            break;
+        }
+    }
+    if (bytes < need) {
+        gs_dev_free(tmp);
+        return gs_fail(ctx, GS_ERR_ARG, "destination too small: need " + std::to_string(need));
+    }
+    cudaError_t e = cudaMemcpyAsync(host_dst, src, need, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    gs_dev_free(tmp);
+    if (e != cudaSuccess) return gs_cuda_fail(ctx, e, "download");
+    return GS_OK;
+}
+
+gs_status gs_result_count(gs_state* s, uint64_t* count) {
+    if (!s || !count) return GS_ERR_ARG;
+    switch (s->algo) {
+        case GS_ALGO_BFS: {
+            uint64_t e;
+            return gs_count_reached(s, count, &e);
+        }
+        case GS_ALGO_KCORE: return gs_count_kcore(s, count);
+        case GS_ALGO_WCC: {
+            uint32_t* tmp = nullptr;
+            GS_TRY(gs_dev_alloc(s->g->ctx, (void**)&tmp, s->g->N * 4));
+            gs_status st = gs_wcc_labels(s, tmp, count);
+            gs_dev_free(tmp);
+            return st;
+        }
+        case GS_ALGO_PAGERANK: *count = (uint64_t)s->step; return GS_OK;
+    }
+    return GS_ERR_ARG;
+}
+
+gs_status gs_bfs_stats(gs_state* s, uint64_t* edges_in_component, uint64_t* swept_records,
+                       int max_levels, int* n_levels, uint64_t* level_counts) {
+    if (!s || s->algo != GS_ALGO_BFS) return GS_ERR_ARG;
+    if (edges_in_component) {
+        uint64_t reached;
+        GS_TRY(gs_count_reached(s, &reached, edges_in_component));
+    }
+    int nl = (int)s->level_counts.size();
+    if (n_levels) *n_levels = nl;
+    if (level_counts)
+        for (int l = 0; l < nl && l < max_levels; ++l) level_counts[l] = s->level_counts[l];
+    if (swept_records) {
+        for (int l = 0; l < nl && l < max_levels; ++l) {
+            uint64_t sw = 0;
+            GS_TRY(gs_swept_records(s, s->level_act[l].data(), &sw));
+            swept_records[l] = sw;
+        }
+    }
+    return GS_OK;
+}
+
+}  // extern "C"

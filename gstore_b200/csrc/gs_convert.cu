@@ -1,0 +1,180 @@
+// In-memory converter "-c 1" on the device (grid::pre_grid + grid::proc_grid,
+// gstore.cpp:1245-1458): edge pairs -> .start offsets, .grid records and
+// .degree counts, as a resident graph.
+//
+//  1. count:   per non-self-loop edge, order (min, max) for the half grid,
+//              find its tile, count it, count both endpoint degrees
+//              (out-degree only for the directed grid) — gstore.cpp:1270-1312
+//  2. scan:    exclusive prefix sum of the tile counts -> .start (:1316-1324)
+//  3. scatter: each edge takes the next slot of its tile (:1403-1447); the
+//              in-tile order is the order the atomics resolve, as in the
+//              reference (thread order).
+#include "gs_internal.cuh"
+
+#include <cub/device/device_scan.cuh>
+
+namespace {
+
+__device__ __forceinline__ uint64_t dev_calc_index_half(uint64_t i, uint64_t j, uint64_t pc) {
+    return ((i * ((pc << 1) - i - 1)) >> 1) + j;
+}
+
+// .start index of the tile holding (a, b), a <= b for the half grid.
+__device__ __forceinline__ uint64_t tile_of(uint64_t a, uint64_t b, uint64_t p, int directed) {
+    const uint64_t gi = a >> kGroupBits, gj = b >> kGroupBits;
+    const uint64_t si = (a >> kTileBits) & 255, sj = (b >> kTileBits) & 255;
+    if (directed) return ((gi * p + gj) << 16) + si * 256 + sj;
+    if (gi == gj)
+        return ((dev_calc_index_half(gi, gi, p) - gi) << 16) + ((gi * 257) << 7) +
+               dev_calc_index_half(si, sj, 256);
+    return ((dev_calc_index_half(gi, gj, p) - gi - 1) << 16) + (((gi + 1) * 257) << 7) + si * 256 + sj;
+}
+
+__global__ void count_kernel(const uint2* __restrict__ pairs, uint64_t n, uint64_t V, uint64_t p,
+                             int directed, unsigned long long* __restrict__ counts, int32_t* __restrict__ deg,
+                             int* bad) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t k = tid; k < n; k += nth) {
+        const uint2 e = pairs[k];
+        if (e.x == e.y) continue;  // is_self_loop
+        if (e.x >= V || e.y >= V) {
+            *bad = 1;
+            continue;
+        }
+        uint64_t a = e.x, b = e.y;
+        if (!directed && a > b) {
+            a = e.y;
+            b = e.x;
+        }
+        atomicAdd(counts + tile_of(a, b, p, directed), 1ull);
+        atomicAdd(deg + e.x, 1);
+        if (!directed) atomicAdd(deg + e.y, 1);
+    }
+}
+
+__global__ void scatter_kernel(const uint2* __restrict__ pairs, uint64_t n, uint64_t p, int directed,
+                               const uint64_t* __restrict__ start, unsigned int* __restrict__ cursor,
+                               uint32_t* __restrict__ rec) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t k = tid; k < n; k += nth) {
+        const uint2 e = pairs[k];
+        if (e.x == e.y) continue;
+        uint64_t a = e.x, b = e.y;
+        if (!directed && a > b) {
+            a = e.y;
+            b = e.x;
+        }
+        const uint64_t t = tile_of(a, b, p, directed);
+        const unsigned slot = atomicAdd(cursor + t, 1u);
+        rec[start[t] + slot] = (uint32_t)(a & 0xFFFF) | ((uint32_t)(b & 0xFFFF) << 16);
+    }
+}
+
+}  // namespace
+
+gs_status gs_convert_launch(gs_ctx* ctx, const uint32_t* d_pairs, uint64_t n_pairs, uint64_t V, int directed,
+                            uint64_t** d_start_out, uint32_t** d_grid_out, int32_t** d_degree_out,
+                            uint64_t* n_start, uint64_t* n_rec) {
+    uint32_t p, ps;
+    uint64_t T;
+    gs_geometry_of(V, directed, &p, &ps, &T);
+    uint64_t* d_start = nullptr;
+    unsigned int* d_cursor = nullptr;
+    int32_t* d_deg = nullptr;
+    uint32_t* d_rec = nullptr;
+    void* d_tmp = nullptr;
+    size_t tmp_bytes = 0;
+    int* d_bad = (int*)ctx->d_scalars;
+    gs_status st = GS_OK;
+    const uint2* pairs = reinterpret_cast<const uint2*>(d_pairs);
+    const uint32_t blocks = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>((n_pairs + 255) / 256, gs_grid_size(ctx, 16)));
+    uint64_t total = 0;
+    int bad = 0;
+#define CV_CHECK(call)                                   \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) {                         \
+            st = gs_cuda_fail(ctx, e_, #call);           \
+            goto fail;                                   \
+        }                                                \
+    } while (0)
+    if ((st = gs_dev_alloc(ctx, (void**)&d_start, (T + 1) * 8)) != GS_OK) goto fail;
+    if ((st = gs_dev_alloc(ctx, (void**)&d_deg, std::max<uint64_t>(V, 1) * 4)) != GS_OK) goto fail;
+    CV_CHECK(cudaMemsetAsync(d_start, 0, (T + 1) * 8, ctx->stream));
+    CV_CHECK(cudaMemsetAsync(d_deg, 0, V * 4, ctx->stream));
+    CV_CHECK(cudaMemsetAsync(d_bad, 0, sizeof(int), ctx->stream));
+    if (n_pairs) {
+        count_kernel<<<blocks, 256, 0, ctx->stream>>>(pairs, n_pairs, V, p, directed,
+                                                      (unsigned long long*)d_start, d_deg, d_bad);
+        CV_CHECK(cudaGetLastError());
+        ctx->launches++;
+    }
+    CV_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_start, d_start, T + 1, ctx->stream));
+    if ((st = gs_dev_alloc(ctx, &d_tmp, tmp_bytes)) != GS_OK) goto fail;
+    CV_CHECK(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_start, d_start, T + 1, ctx->stream));
+    CV_CHECK(cudaMemcpyAsync(&total, d_start + T, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CV_CHECK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CV_CHECK(cudaStreamSynchronize(ctx->stream));
+    if (bad) {
+        st = gs_fail(ctx, GS_ERR_FORMAT, "an edge endpoint is >= the vertex count");
+        goto fail;
+    }
+    if ((st = gs_dev_alloc(ctx, (void**)&d_rec, std::max<uint64_t>(total, 1) * 4)) != GS_OK) goto fail;
+    if ((st = gs_dev_alloc(ctx, (void**)&d_cursor, T * 4)) != GS_OK) goto fail;
+    CV_CHECK(cudaMemsetAsync(d_cursor, 0, T * 4, ctx->stream));
+    if (n_pairs) {
+        scatter_kernel<<<blocks, 256, 0, ctx->stream>>>(pairs, n_pairs, p, directed, d_start, d_cursor, d_rec);
+        CV_CHECK(cudaGetLastError());
+        ctx->launches++;
+    }
+    CV_CHECK(cudaStreamSynchronize(ctx->stream));
+    gs_dev_free(d_cursor);
+    gs_dev_free(d_tmp);
+    *d_start_out = d_start;
+    *d_grid_out = d_rec;
+    *d_degree_out = d_deg;
+    *n_start = T + 1;
+    *n_rec = total;
+    return GS_OK;
+fail:
+#undef CV_CHECK
+    cudaStreamSynchronize(ctx->stream);
+    gs_dev_free(d_start);
+    gs_dev_free(d_cursor);
+    gs_dev_free(d_deg);
+    gs_dev_free(d_rec);
+    gs_dev_free(d_tmp);
+    return st;
+}
+
+extern "C" gs_status gs_convert(gs_ctx* ctx, const uint32_t* pairs, uint64_t n_pairs, int is_device,
+                                uint64_t V, gs_graph** out) {
+    if (!ctx || !out || (n_pairs && !pairs) || V == 0 || V > (1ull << 32)) return GS_ERR_ARG;
+    *out = nullptr;
+    const uint32_t* d_pairs = pairs;
+    uint32_t* d_copy = nullptr;
+    if (!is_device && n_pairs) {
+        GS_TRY(gs_dev_alloc(ctx, (void**)&d_copy, n_pairs * 8));
+        cudaError_t e = cudaMemcpyAsync(d_copy, pairs, n_pairs * 8, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) {
+            gs_dev_free(d_copy);
+            return gs_cuda_fail(ctx, e, "copy pairs");
+        }
+        d_pairs = d_copy;
+    }
+    uint64_t* d_start = nullptr;
+    uint32_t* d_rec = nullptr;
+    int32_t* d_deg = nullptr;
+    uint64_t n_start = 0, n_rec = 0;
+    gs_status st = gs_convert_launch(ctx, d_pairs, n_pairs, V, ctx->directed, &d_start, &d_rec, &d_deg,
+                                     &n_start, &n_rec);
+    gs_dev_free(d_copy);
+    if (st != GS_OK) return st;
+    st = gs_graph_adopt(ctx, V, d_start, n_start, d_rec, n_rec, d_deg, out);
+    gs_dev_free(d_start);
+    gs_dev_free(d_deg);
+    return st;
+}

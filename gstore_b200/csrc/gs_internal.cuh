@@ -1,0 +1,168 @@
+// Internal declarations of libgstore_cuda.so (not part of the C ABI).
+#pragma once
+
+#include "gstore_cuda.h"
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+// Tile geometry constants of the reference (gstore.h:77-104).
+constexpr int kTileBits = 16;          // bit_shift2: a tile spans 2^16 vertices
+constexpr uint32_t kGroupTiles = 256;  // p_p: tiles per physical group side
+constexpr int kGroupBits = 24;         // bit_shift1: a group spans 2^24 vertices
+// Upper bound of records per work item (a slice of one tile).
+constexpr uint32_t kItemRecords = 4096;
+
+// One work item: records [beg, beg + cnt) of the tile at global tile row
+// `row`, column `col` (every record of an item lies in that one tile).
+struct alignas(16) gs_item {
+    uint64_t beg;
+    uint32_t cnt;
+    uint32_t rc;  // row << 16 | col
+};
+
+struct KernelTimes {
+    uint64_t launches = 0;
+    double ms = 0.0;
+    uint64_t bytes = 0;
+};
+
+struct gs_ctx {
+    int device = 0;
+    int directed = 0;
+    uint64_t budget = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    bool profile = false;
+    KernelTimes ktime[4];
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint64_t* d_scalars = nullptr;   // small device scratch for counters/flags
+    uint64_t* h_scalars = nullptr;   // pinned mirror
+    int num_sms = 148;
+    uint64_t launches = 0;           // kernels launched on this context
+};
+
+struct gs_graph {
+    gs_ctx* ctx = nullptr;
+    int directed = 0;
+    uint64_t V = 0;      // vertex count given by the caller
+    uint64_t N = 0;      // padded vertex count: nw * 2^16
+    uint32_t p = 0, p_s = 0, nw = 0;
+    uint64_t T_all = 0;  // stored tiles (.start entries - 1)
+    uint64_t E = 0;      // records
+    uint64_t T = 0;      // non-empty tiles
+    uint64_t I = 0;      // work items
+    uint32_t* d_rec = nullptr;
+    gs_item* d_items = nullptr;
+    uint64_t* d_tile_off = nullptr;   // T + 1 record offsets of non-empty tiles
+    uint32_t* d_tile_rc = nullptr;    // T packed (row << 16 | col)
+    int32_t* d_degree = nullptr;      // N
+    bool degree_from_records = false;
+    std::vector<uint64_t> h_start;    // full .start copy (host), for planners
+    std::vector<uint64_t> h_tile_off; // host copy of d_tile_off
+    std::vector<uint32_t> h_tile_rc;  // host copy of d_tile_rc
+};
+
+struct gs_state {
+    gs_graph* g = nullptr;
+    gs_algo algo = GS_ALGO_BFS;
+    int64_t arg = 0;
+    int step = 0;          // sweeps done
+    bool done = false;
+    bool compat = false;   // PageRank int32 inverse-degree truncation
+    // BFS
+    uint8_t level = 1;
+    uint8_t* d_depth = nullptr;      // N
+    uint32_t* d_front = nullptr;     // N/32 frontier bitmap
+    uint32_t* d_visited = nullptr;   // N/32
+    uint8_t* d_act = nullptr;        // nw window flags (current)
+    uint8_t* d_act_next = nullptr;   // nw
+    std::vector<uint64_t> level_counts;
+    std::vector<std::vector<uint8_t>> level_act;  // per level window flags (host)
+    // PageRank
+    float* d_x = nullptr;            // N
+    float* d_y = nullptr;            // N
+    float* d_r = nullptr;            // N
+    // WCC
+    uint32_t* d_parent = nullptr;    // N
+    uint8_t* d_touched = nullptr;    // N
+    // k-core
+    int32_t* d_deg = nullptr;        // N
+    uint32_t* d_kactive = nullptr;   // N/32
+    int64_t last_count = 0;
+};
+
+// ---------------------------------------------------------------- errors --
+gs_status gs_fail(gs_ctx* ctx, gs_status code, const std::string& msg);
+gs_status gs_cuda_fail(gs_ctx* ctx, cudaError_t e, const char* what);
+
+#define GS_CHECK_CUDA(ctx, call)                                  \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) return gs_cuda_fail((ctx), e_, #call); \
+    } while (0)
+
+#define GS_TRY(call)                          \
+    do {                                      \
+        gs_status s_ = (call);                \
+        if (s_ != GS_OK) return s_;           \
+    } while (0)
+
+// --------------------------------------------------------------- geometry --
+inline uint64_t gs_calc_index_half(uint64_t i, uint64_t j, uint64_t pc) {
+    return ((i * ((pc << 1) - i - 1)) >> 1) + j;   // calc_index, gstore.h:109-113
+}
+// First .start index of group (gi, gj): beg_edge_offset1/2 (gstore.h:128-178).
+inline uint64_t gs_group_base(uint64_t gi, uint64_t gj, uint64_t p, int directed) {
+    if (directed) return (gi * p + gj) << 16;
+    if (gi == gj) return ((gs_calc_index_half(gi, gi, p) - gi) << 16) + ((gi * 257) << 7);
+    return ((gs_calc_index_half(gi, gj, p) - gi - 1) << 16) + (((gi + 1) * 257) << 7);
+}
+void gs_geometry_of(uint64_t V, int directed, uint32_t* p, uint32_t* p_s, uint64_t* n_tiles);
+
+// ------------------------------------------------------- device launchers --
+gs_status gs_dev_alloc(gs_ctx* ctx, void** ptr, size_t bytes);
+void gs_dev_free(void* ptr);
+
+gs_status launch_validate_records(gs_graph* g, int* d_flag);
+gs_status launch_degree_from_records(gs_graph* g);
+
+gs_status bfs_init(gs_state* s);
+gs_status bfs_sweep(gs_state* s);
+gs_status bfs_finalize(gs_state* s, int64_t* frontier, int* done);
+
+gs_status pr_init(gs_state* s);
+gs_status pr_sweep(gs_state* s);
+gs_status pr_finalize(gs_state* s, int64_t* frontier, int* done);
+
+gs_status wcc_init(gs_state* s);
+gs_status wcc_sweep(gs_state* s);
+gs_status wcc_finalize(gs_state* s, int64_t* frontier, int* done);
+
+gs_status kcore_init(gs_state* s);
+gs_status kcore_sweep(gs_state* s);
+gs_status kcore_finalize(gs_state* s, int64_t* frontier, int* done);
+
+gs_status gs_count_reached(gs_state* s, uint64_t* reached, uint64_t* edges_in_component);
+gs_status gs_count_kcore(gs_state* s, uint64_t* members);
+gs_status gs_wcc_labels(gs_state* s, uint32_t* d_out, uint64_t* count);
+gs_status gs_swept_records(gs_state* s, const uint8_t* h_act, uint64_t* swept);
+
+gs_status gs_kron_gen_launch(gs_ctx* ctx, int scale, int64_t ef, uint64_t s1, uint64_t s2,
+                             uint32_t* d_pairs);
+gs_status gs_convert_launch(gs_ctx* ctx, const uint32_t* d_pairs, uint64_t n_pairs, uint64_t V,
+                            int directed, uint64_t** d_start_out, uint32_t** d_grid_out,
+                            int32_t** d_degree_out, uint64_t* n_start, uint64_t* n_rec);
+
+gs_status gs_graph_adopt(gs_ctx* ctx, uint64_t V, const uint64_t* d_start, uint64_t n_start, uint32_t* d_rec,
+                         uint64_t n_edges, const int32_t* d_degree, gs_graph** out);
+
+// Timing helpers around the main sweep kernel of an algorithm.
+void gs_timer_begin(gs_ctx* ctx);
+void gs_timer_end(gs_ctx* ctx, int algo, uint64_t bytes);
+
+inline uint32_t gs_grid_size(const gs_ctx* ctx, int per_sm) { return (uint32_t)ctx->num_sms * per_sm; }

@@ -1,0 +1,266 @@
+// gstoreu / gstored: the reference's command line (grid::init,
+// gstore.cpp:132-348) driving the B200 engine through libgstore_cuda.so.
+//
+// Built twice, like the reference (Makefile:41-45): with -DHALF_GRID as
+// gstoreu (undirected, upper-triangle tiles) and without as gstored
+// (directed, full grid).  Flags keep their meaning:
+//   -s scale | -v vertex count   geometry (p, p_s)
+//   -i input prefix / edge list, -o output prefix (converter)
+//   -j job, -a job argument, -m memory budget in MB (HBM tile budget),
+//   -c converter mode
+// and the jobs print the reference's lines (level/frontier counts, "WCC
+// count = ", ">= k vertices count = ", "<job> time = ").
+//
+// Differences, by design: "-s" below 24 maps to one tile group instead of
+// wrapping to 2^32 groups (gstore.cpp:145-146 computes 1 << (scale - 24) in
+// unsigned arithmetic); jobs 4, 30, 100 and converter modes other than 1/6
+// are not part of this engine.
+#include <getopt.h>
+#include <sys/time.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "algo.h"
+#include "gstore_cuda.h"
+#include "tilefile.h"
+
+#ifdef HALF_GRID
+static const int kDirected = 0;
+#else
+static const int kDirected = 1;
+#endif
+
+static double mywtime() {   // wtime.h:188-199
+    timeval t;
+    gettimeofday(&t, nullptr);
+    return t.tv_sec + t.tv_usec / 1e6;
+}
+
+static int fail(gs_ctx* ctx, const std::string& what) {
+    std::cerr << "gstore: " << what;
+    if (ctx && gs_last_error(ctx)[0]) std::cerr << ": " << gs_last_error(ctx);
+    std::cerr << std::endl;
+    return 1;
+}
+
+struct options {
+    uint64_t vert_count = 0;
+    std::string edgefile, part_file;
+    int job = 0, convert = 0, arg = -1;
+    uint64_t total_size = 8192ull << 20;   // -m default, gstore.cpp:79
+};
+
+static int read_graph_files(const options& o, bool want_degree, tile_files* tf) {
+    uint32_t p, ps;
+    uint64_t n_start;
+    gs_geometry(o.vert_count, kDirected, &p, &ps, &n_start);
+    std::string err = read_tile_files(o.edgefile, n_start, o.vert_count, want_degree, tf);
+    if (!err.empty()) return fail(nullptr, err);
+    return 0;
+}
+
+static int upload_graph(gs_ctx* ctx, const options& o, const tile_files& tf, bool want_degree, gs_graph** g) {
+    gs_status st = gs_upload_graph(ctx, tf.start.data(), tf.start.size(), tf.grid.data(), tf.grid.size(),
+                                   want_degree ? tf.degree.data() : nullptr, o.vert_count, g);
+    if (st != GS_OK) return fail(ctx, "loading " + o.edgefile);
+    return 0;
+}
+
+static int run_bfs(gs_ctx* ctx, gs_graph* g, uint64_t root) {
+    bfs_t bf;
+    bf.init(ctx, g, root);
+    if (bf.status() != GS_OK) return fail(ctx, "bfs init");
+    while (true) {
+        double start = mywtime();
+        bf.algo_mem_part(nullptr);
+        int done = bf.iteration_finalize();
+        std::cout << "iteration time = " << mywtime() - start << std::endl;
+        if (bf.status() != GS_OK) return fail(ctx, "bfs");
+        if (done) break;
+    }
+    uint64_t edges = 0;
+    uint64_t reached = 0;
+    gs_bfs_stats(bf.state(), &edges, nullptr, 0, nullptr, nullptr);
+    gs_result_count(bf.state(), &reached);
+    std::cout << "reached vertices = " << reached << ", component edge records = " << edges << std::endl;
+    return 0;
+}
+
+static int run_pagerank(gs_ctx* ctx, gs_graph* g, int iters) {
+    pr_t pr;
+    pr.init(ctx, g, iters, getenv("GS_PR_COMPAT") != nullptr);
+    for (int it = 0; it < iters && pr.status() == GS_OK; ++it) {
+        pr.algo_mem_part(nullptr);
+        pr.iteration_finalize(it);
+    }
+    if (pr.status() != GS_OK) return fail(ctx, "pagerank");
+    return 0;
+}
+
+static int run_kcore(gs_ctx* ctx, gs_graph* g, int kc) {
+    if (kDirected) {
+        std::cout << "Kcore not applicable for directed graphs" << std::endl;   // gstore.cpp:2718-2720
+        return 0;
+    }
+    if (kc == -1) kc = 10;
+    kcore_t kcorep;
+    kcorep.init(ctx, g, kc);
+    if (kcorep.status() != GS_OK) return fail(ctx, "kcore init");
+    if (0 == kcorep.iteration_finalize()) return kcorep.status() == GS_OK ? 0 : fail(ctx, "kcore");
+    while (true) {
+        double start = mywtime();
+        kcorep.algo_mem_part(nullptr);
+        int removed = kcorep.iteration_finalize();
+        std::cout << "iteration time = " << mywtime() - start << std::endl;
+        if (kcorep.status() != GS_OK) return fail(ctx, "kcore");
+        if (0 == removed) break;
+    }
+    uint64_t total = 0;
+    gs_result_count(kcorep.state(), &total);
+    std::cout << ">= " << kc << "vertices count = " << total << std::endl;   // gstore.cpp:2803
+    return 0;
+}
+
+static int run_wcc(gs_ctx* ctx, gs_graph* g) {
+    wcc2_t w;
+    w.init(ctx, g);
+    if (w.status() != GS_OK) return fail(ctx, "wcc init");
+    while (true) {
+        double start = mywtime();
+        w.algo_mem_part(nullptr);
+        int more = w.iteration_finalize();
+        std::cout << "iteration time = " << mywtime() - start << std::endl;
+        if (w.status() != GS_OK) return fail(ctx, "wcc");
+        if (0 == more) break;
+    }
+    return 0;
+}
+
+static int convert(gs_ctx* ctx, const options& o, const std::vector<uint32_t>& pairs) {
+    std::string err;
+    double start = mywtime();
+    gs_graph* g = nullptr;
+    if (gs_convert(ctx, pairs.data(), pairs.size() / 2, 0, o.vert_count, &g) != GS_OK)
+        return fail(ctx, "convert");
+    double end = mywtime();
+    uint64_t E, T, I, V;
+    gs_graph_info(g, &E, &T, &I, &V);
+    std::cout << "Total edges = " << E << std::endl;   // gstore.cpp:1325
+    uint32_t p, ps;
+    uint64_t n_start;
+    gs_geometry(o.vert_count, kDirected, &p, &ps, &n_start);
+    tile_files tf;
+    tf.start.resize(n_start);
+    tf.grid.resize(E);
+    tf.degree.resize(o.vert_count);
+    if (gs_graph_download(g, tf.start.data(), tf.grid.data(), tf.degree.data()) != GS_OK)
+        return fail(ctx, "download");
+    gs_graph_free(g);
+    if (o.convert == 1) {
+        err = write_tile_files(o.part_file, tf);
+        if (!err.empty()) return fail(nullptr, err);
+        std::cout << "Total Edges again = " << tf.start.back() << std::endl;   // gstore.cpp:2907
+    }
+    std::cout << "GStore Time = " << end - start << std::endl;
+    return 0;
+}
+
+int main(int argc, char* argv[]) {
+    options o;
+    int c;
+    bool have_geometry = false;
+    while ((c = getopt(argc, argv, "s:o:hi:j:c:m:v:a:")) != -1) {   // gstore.cpp:140
+        switch (c) {
+            case 's': {
+                int scale = atoi(optarg);
+                if (scale < 1 || scale > 32) return fail(nullptr, "-s must be in 1..32");
+                o.vert_count = 1ull << scale;
+                have_geometry = true;
+                break;
+            }
+            case 'v':
+                o.vert_count = strtoull(optarg, nullptr, 10);
+                have_geometry = true;
+                break;
+            case 'i': o.edgefile = optarg; break;
+            case 'o': o.part_file = optarg; break;
+            case 'j': o.job = atoi(optarg); break;
+            case 'h': std::cout << "Coming soon" << std::endl; return 0;
+            case 'c': o.convert = atoi(optarg); break;
+            case 'm': o.total_size = (uint64_t)atoi(optarg) << 20; break;
+            case 'a': o.arg = atoi(optarg); break;
+            default: std::cout << "Unknown argument" << std::endl;
+        }
+    }
+    if (!have_geometry || o.vert_count == 0) return fail(nullptr, "give the vertex count with -s or -v");
+    uint32_t p, ps;
+    uint64_t n_start;
+    gs_geometry(o.vert_count, kDirected, &p, &ps, &n_start);
+    std::cout << "Total Physcial Group Count (in One Direction) = " << p << std::endl;
+    std::cout << "Total Tiles Count (in One Direction) = " << ps << std::endl;
+
+    // Host-side checks (file formats, job numbers) come before any device
+    // work, so malformed input is reported the same way with or without a GPU.
+    if (o.convert) {
+        if (o.convert != 1 && o.convert != 6)
+            return fail(nullptr, "converter mode " + std::to_string(o.convert) + " is not provided by this engine");
+        std::vector<uint32_t> pairs;
+        std::string err = read_edge_list(o.edgefile, &pairs);
+        if (!err.empty()) return fail(nullptr, err);
+        gs_ctx* ctx = nullptr;
+        if (gs_create(&ctx, 0, 0, kDirected) != GS_OK) return fail(nullptr, "no usable CUDA device");
+        int rc = convert(ctx, o, pairs);
+        gs_destroy(ctx);
+        return rc;
+    }
+
+    const int job = o.job;
+    const bool bfs = job == 0 || job == 10 || job == 20;
+    const bool pr = job == 1 || job == 11 || job == 21;
+    const bool kc = job == 2 || job == 12 || job == 22;
+    const bool wcc = job == 3 || job == 13 || job == 23;
+    if (!(bfs || pr || kc || wcc)) {
+        if (job == 4 || job == 30 || job == 100) std::cout << "job " << job << " is not provided by this engine" << std::endl;
+        else std::cout << "Wrong value for -j argument" << std::endl;
+        return 1;
+    }
+    // Jobs 2x exclude file loading from the printed time (gstore.cpp:250-333).
+    const bool exclude_load = job >= 20;
+    const bool want_degree = pr || kc;
+    double start = mywtime();
+    tile_files tf;
+    int rc = read_graph_files(o, want_degree, &tf);
+    if (rc) return rc;
+    gs_ctx* ctx = nullptr;
+    if (gs_create(&ctx, 0, 0, kDirected) != GS_OK) return fail(nullptr, "no usable CUDA device");
+    gs_graph* g = nullptr;
+    rc = upload_graph(ctx, o, tf, want_degree, &g);
+    if (rc == 0) {
+        if (exclude_load) start = mywtime();
+        const char* label = "";
+        if (bfs) {
+            // job 0 takes the root from -a (default 0); 10/20 fix it to 1
+            // (gstore.cpp:2306-2307, 2634).
+            uint64_t root = job == 0 ? (o.arg == -1 ? 0 : (uint64_t)o.arg) : 1;
+            rc = run_bfs(ctx, g, root);
+            label = "Half BFS time = ";
+        } else if (pr) {
+            rc = run_pagerank(ctx, g, o.arg == -1 ? 5 : o.arg);
+            label = job == 1 ? "Page-rank time = " : "Page-rank_mmap time = ";
+        } else if (kc) {
+            rc = run_kcore(ctx, g, o.arg);
+            label = "Kcore time = ";
+        } else {
+            rc = run_wcc(ctx, g);
+            label = "WCC time = ";
+        }
+        if (rc == 0) std::cout << label << mywtime() - start << std::endl;
+        gs_graph_free(g);
+    }
+    gs_destroy(ctx);
+    return rc;
+}

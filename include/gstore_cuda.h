@@ -1,0 +1,180 @@
+/*
+ * gstore_cuda.h — C ABI of libgstore_cuda.so, the B200 (sm_100a) engine for
+ * G-Store's tile-grid edge scan.
+ *
+ * The library replaces the hot path of the G-Store reference: the per-level /
+ * per-iteration sweep over the 2D grid of SNB tiles that drives BFS, PageRank,
+ * WCC and k-core.  Host code (the gstoreu/gstored CLI, the algo_t adapters, or
+ * any FFI caller) drives it through the plain-C entry points below: plain
+ * pointers and sizes, no C++ or framework types.
+ *
+ * Formats (identical to the reference's files):
+ *   start  : uint64 edge offsets, one per stored tile plus one
+ *            (grid::save_start_files, gstore.cpp:2899-2908)
+ *   grid   : uint32 records, v0 | v1 << 16, tile after tile
+ *            (edge_t, gstore.h:311-334; grid::save_grid, gstore.cpp:2818-2829)
+ *   degree : int32 per vertex (grid::save_degree_files, gstore.cpp:2911-2917)
+ * Geometry (grid::init -v, gstore.cpp:152-161): p = ceil(V / 2^24) groups per
+ * dimension, p_s = 256 p tiles per dimension; the undirected layout ("gstoreu",
+ * HALF_GRID) stores the upper triangle, p_s (p_s + 1) / 2 tiles; the directed
+ * one ("gstored") stores p_s^2 tiles.
+ *
+ * Ownership: the library owns every device allocation and pinned staging
+ * buffer it makes.  The caller owns host arrays and keeps them alive until the
+ * call that takes them returns.  All calls are synchronous unless named
+ * otherwise.
+ * Errors: every call returns gs_status; no call exits or asserts (unlike the
+ * reference's handle_error, gstore.h:43-44).  gs_last_error() gives the text
+ * of the last failure on a context.
+ * Threading: a gs_ctx and everything made from it is single-threaded.
+ */
+#ifndef GSTORE_CUDA_H
+#define GSTORE_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t gs_status;
+#define GS_OK 0
+#define GS_ERR_CUDA 1      /* a CUDA runtime call failed                     */
+#define GS_ERR_OOM 2       /* device or pinned memory exhausted / over budget */
+#define GS_ERR_FORMAT 3    /* start/grid/degree inconsistent or out of range  */
+#define GS_ERR_TIMEOUT 4   /* a bounded device-side wait gave up              */
+#define GS_ERR_ARG 5       /* invalid argument                                */
+#define GS_ERR_RANGE 6     /* BFS would exceed 254 levels (u8 depth_t)        */
+#define GS_ERR_STATE 7     /* call out of order for this object              */
+#define GS_ERR_UNSUPPORTED 8 /* e.g. k-core on a directed grid               */
+
+typedef enum gs_algo {
+    GS_ALGO_BFS = 0,      /* bfs_t   (bfs.cpp)   arg = root                 */
+    GS_ALGO_PAGERANK = 1, /* pr_t    (pr.cpp)    arg = iterations           */
+    GS_ALGO_KCORE = 2,    /* kcore_t (kcore.cpp) arg = k                    */
+    GS_ALGO_WCC = 3       /* wcc2_t  (wcc.cpp)   arg unused                 */
+} gs_algo;
+
+typedef struct gs_ctx gs_ctx;
+typedef struct gs_graph gs_graph;
+typedef struct gs_state gs_state;
+
+/* A run of consecutive stored tiles, mirroring part_meta_t (gstore.h:563-568):
+ * part ids use the reference's encoding (group_full_index << 16 | i << 8 | j,
+ * gstore.h:199-220) and start..end is inclusive in file order.  Used by the
+ * streamed (semi-external) sweep. */
+typedef struct gs_segment {
+    uint64_t part_start;
+    uint64_t part_end;
+} gs_segment;
+
+/* ------------------------------------------------------------ context --- */
+/* Replaces: grid::init / read_aio_init set-up (gstore.cpp:132-186, 3044-3119).
+ * hbm_budget_bytes bounds the tile bytes kept resident (0 = no bound); it is
+ * the "-m" memory budget of the reference reused for HBM. */
+gs_status gs_create(gs_ctx** out, int device, uint64_t hbm_budget_bytes, int directed);
+gs_status gs_destroy(gs_ctx* ctx);
+const char* gs_last_error(const gs_ctx* ctx);
+/* Launch all work of this context on an existing cudaStream_t (NULL = the
+ * context's own stream). */
+gs_status gs_set_stream(gs_ctx* ctx, void* cuda_stream);
+/* Enable per-kernel CUDA-event timing (kind: 0 = main sweep kernel). */
+gs_status gs_profile(gs_ctx* ctx, int enable);
+gs_status gs_kernel_time(gs_ctx* ctx, int algo, uint64_t* launches, double* total_ms,
+                         uint64_t* bytes);
+
+/* Number of kernels this context has launched so far (all entry points). */
+gs_status gs_launch_count(const gs_ctx* ctx, uint64_t* launches);
+
+/* Geometry of the tile files for vertex count V (grid::init -v). */
+gs_status gs_geometry(uint64_t V, int directed, uint32_t* p, uint32_t* p_s,
+                      uint64_t* n_start_entries);
+
+/* -------------------------------------------------------------- graph --- */
+/* Replaces: read_grid_in_mem + read_degree_in_mem (gstore.cpp:2953-3011).
+ * Copies host start[n_start], grid[n_edges] and degree[V] (degree may be NULL:
+ * it is then counted on the device from the records) into HBM and builds the
+ * tile tables.  Checks: n_start matches the geometry, start is monotone,
+ * start[last] == n_edges, every record addresses a vertex below V. */
+gs_status gs_upload_graph(gs_ctx* ctx, const uint64_t* start, uint64_t n_start,
+                          const uint32_t* grid, uint64_t n_edges,
+                          const int32_t* degree, uint64_t V, gs_graph** out);
+/* The same from device pointers (e.g. produced by gs_convert_device); the
+ * library copies them, the caller keeps ownership. */
+gs_status gs_upload_graph_device(gs_ctx* ctx, const uint64_t* d_start, uint64_t n_start,
+                                 const uint32_t* d_grid, uint64_t n_edges,
+                                 const int32_t* d_degree, uint64_t V, gs_graph** out);
+gs_status gs_graph_free(gs_graph* g);
+/* Counts: records, non-empty tiles, work items, vertex count. */
+gs_status gs_graph_info(const gs_graph* g, uint64_t* n_edges, uint64_t* n_tiles,
+                        uint64_t* n_items, uint64_t* V);
+/* Copy the graph's degree array (V int32) to the host. */
+gs_status gs_graph_degree(const gs_graph* g, int32_t* host_degree);
+
+/* ------------------------------------------------- algo_t plug-in layer --- */
+/* Replaces: bfs_t/pr_t/kcore_t/wcc2_t ::init (bfs.cpp:56-75, pr.cpp:82-117,
+ * kcore.cpp:55-61, wcc.cpp:57-83).  arg: BFS root, PageRank iterations,
+ * k-core k; unused for WCC.  The state lives in HBM. */
+gs_status gs_state_create(gs_graph* g, gs_algo algo, int64_t arg, gs_state** out);
+gs_status gs_state_free(gs_state* s);
+/* Re-initialise a state for a new run (new root / iterations / k) without
+ * reallocating its device arrays. */
+gs_status gs_state_reset(gs_state* s, int64_t arg);
+/* Replaces: algo_t::algo_mem_part(segment*) (algo.h:40): sweeps the tiles of
+ * the given runs (segs, n_segs), or every resident tile when segs == NULL,
+ * applying the algorithm's own tile-skip rule. */
+gs_status gs_sweep(gs_state* s, const gs_segment* segs, int n_segs);
+/* Replaces: iteration_finalize() (bfs.cpp:187-224, pr.cpp:229-303,
+ * kcore.cpp:179-217, wcc.cpp:281-395).  frontier_out: BFS vertices found in
+ * the last sweep, k-core vertices removed, WCC labels changed, PageRank the
+ * iteration just finished.  done_out: 1 when the algorithm has finished. */
+gs_status gs_finalize(gs_state* s, int64_t* frontier_out, int* done_out);
+/* Sweep + finalize until done, all on the device (one 8-byte read per step).
+ * steps_out: number of sweeps. */
+gs_status gs_run(gs_state* s, int64_t* steps_out);
+
+/* Results.  BFS: uint8 depth[V] (root 1, unreached 0, bfs.cpp:54).
+ * PageRank: float rank[V] = 0.15 + 0.85 s after the last iteration
+ * (what = 0) or float x[V] = rank * inv_degree (what = 1, the reference's
+ * vert_rank_prior after its final swap).  k-core: int32 degree[V] (final,
+ * removed vertices 0 or negative, kcore.cpp:179-217).  WCC: uint32 label[V],
+ * the smallest vertex id of the component, 0xFFFFFFFF for vertices without
+ * records (wcc.cpp:54). */
+gs_status gs_download(gs_state* s, int what, void* host_dst, uint64_t bytes);
+/* Scalar summary: BFS reached vertices, k-core members (deg != 0,
+ * gstore.cpp:2796-2803), WCC component count (wcc.cpp:324-336). */
+gs_status gs_result_count(gs_state* s, uint64_t* count);
+/* BFS: records with both endpoints reached (the GTEPS numerator) and the
+ * records swept per level under the reference's tile-skip rule. */
+gs_status gs_bfs_stats(gs_state* s, uint64_t* edges_in_component, uint64_t* swept_records,
+                       int max_levels, int* n_levels, uint64_t* level_counts);
+
+/* PageRank with the reference's int32 inverse-degree truncation
+ * (pr.cpp:112-114) instead of the real inverse; must precede gs_run. */
+gs_status gs_pagerank_compat(gs_state* s, int enable);
+
+/* ------------------------------------------- generator and converter --- */
+/* Graph500 Kronecker generator (graph500-generator/graph_generator.c,
+ * make_graph.c), byte-identical output: 2 * (edgefactor << scale) uint32
+ * written to device memory d_pairs (caller-allocated). */
+gs_status gs_kron_generate_device(gs_ctx* ctx, int scale, int64_t edgefactor,
+                                  uint64_t seed1, uint64_t seed2, uint32_t* d_pairs);
+/* The same into host memory. */
+gs_status gs_kron_generate(gs_ctx* ctx, int scale, int64_t edgefactor, uint64_t seed1,
+                           uint64_t seed2, uint32_t* host_pairs);
+/* Converter "-c 1" (grid::pre_grid + proc_grid, gstore.cpp:1245-1458) on the
+ * device: edge pairs (host or device pointer, is_device) -> a resident graph.
+ * Self-loops dropped, duplicates kept, (min,max) order for the half grid.
+ * In-tile record order is not specified (the reference's is thread order). */
+gs_status gs_convert(gs_ctx* ctx, const uint32_t* pairs, uint64_t n_pairs, int is_device,
+                     uint64_t V, gs_graph** out);
+/* Copy a resident graph back into host start/grid/degree arrays (sizes from
+ * gs_graph_info / gs_geometry), e.g. to write .start/.grid/.degree files. */
+gs_status gs_graph_download(const gs_graph* g, uint64_t* host_start, uint32_t* host_grid,
+                            int32_t* host_degree);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
