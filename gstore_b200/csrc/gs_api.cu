@@ -36,6 +36,12 @@ void gs_dev_free(void* ptr) {
     if (ptr) cudaFree(ptr);
 }
 
+gs_status gs_alloc_records(gs_ctx* ctx, uint32_t** ptr, uint64_t n_records) {
+    GS_TRY(gs_dev_alloc(ctx, (void**)ptr, (n_records + kRecPad) * 4));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(*ptr + n_records, 0, kRecPad * 4, ctx->stream));
+    return GS_OK;
+}
+
 void gs_geometry_of(uint64_t V, int directed, uint32_t* p, uint32_t* p_s, uint64_t* n_tiles) {
     // grid::init "-v" (gstore.cpp:152-161): p = ceil(V / 2^24), p_s = 256 p.
     uint64_t pp = (V >> kGroupBits) + ((V & ((1ull << kGroupBits) - 1)) != 0);
@@ -157,6 +163,10 @@ static void free_graph_arrays(gs_graph* g) {
     gs_dev_free(g->d_tile_off);
     gs_dev_free(g->d_tile_rc);
     gs_dev_free(g->d_degree);
+    gs_dev_free(g->d_runs);
+    gs_dev_free(g->d_units);
+    g->d_runs = nullptr;
+    g->d_units = nullptr;
     g->d_rec = nullptr;
     g->d_items = nullptr;
     g->d_tile_off = nullptr;
@@ -173,15 +183,24 @@ static gs_status build_tables(gs_graph* g) {
     std::vector<uint64_t>& tile_off = g->h_tile_off;
     std::vector<uint32_t>& tile_rc = g->h_tile_rc;
     std::vector<gs_item> items;
+    std::vector<gs_tile_run> runs;
+    std::vector<gs_unit> units;
     tile_off.clear();
     tile_rc.clear();
     tile_off.reserve(1024);
     uint64_t t = 0;
     const uint64_t p = g->p;
+    gs_tile_run open{0, 0, 0, 0, 0, 0};
+    bool is_open = false;
+    auto close_run = [&]() {
+        if (is_open) runs.push_back(open);
+        is_open = false;
+    };
     for (uint64_t gi = 0; gi < p; ++gi) {
         for (uint64_t gj = g->directed ? 0 : gi; gj < p; ++gj) {
             for (uint64_t m = 0; m < kGroupTiles; ++m) {
                 uint64_t n0 = (!g->directed && gi == gj) ? m : 0;
+                close_run();  // a run never leaves the row segment of its group
                 for (uint64_t n = n0; n < kGroupTiles; ++n, ++t) {
                     uint64_t b = st[t], e = st[t + 1];
                     if (e == b) continue;
@@ -192,6 +211,28 @@ static gs_status build_tables(gs_graph* g) {
                                        "tile (" + std::to_string(row) + "," + std::to_string(col) +
                                            ") holds records beyond the vertex count");
                     uint32_t rc = (row << 16) | col;
+                    const uint32_t k = (uint32_t)tile_rc.size();
+                    const uint32_t u0 = (uint32_t)units.size();
+                    for (uint64_t x = b; x < e; x += kUnitRecords)
+                        units.push_back(gs_unit{x, (uint32_t)std::min<uint64_t>(kUnitRecords, e - x), rc});
+                    const uint32_t u1 = (uint32_t)units.size();
+                    // kRunRecords is a multiple of kUnitRecords: units never straddle runs
+                    if (e - b > kRunRecords) {
+                        close_run();
+                        for (uint64_t x = b; x < e; x += kRunRecords) {
+                            const uint64_t xe = std::min<uint64_t>(e, x + kRunRecords);
+                            runs.push_back(gs_tile_run{x, xe, k, k + 1, u0 + (uint32_t)((x - b) / kUnitRecords),
+                                                       u0 + (uint32_t)((xe - b + kUnitRecords - 1) / kUnitRecords)});
+                        }
+                    } else if (is_open && e - open.rec_beg <= kRunRecords) {
+                        open.rec_end = e;
+                        open.tile_end = k + 1;
+                        open.unit_end = u1;
+                    } else {
+                        close_run();
+                        open = gs_tile_run{b, e, k, k + 1, u0, u1};
+                        is_open = true;
+                    }
                     tile_off.push_back(b);
                     tile_rc.push_back(rc);
                     for (uint64_t x = b; x < e; x += kItemRecords) {
@@ -205,9 +246,20 @@ static gs_status build_tables(gs_graph* g) {
             }
         }
     }
+    close_run();
     tile_off.push_back(st[t]);
     g->T = tile_rc.size();
     g->I = items.size();
+    g->R = runs.size();
+    g->U = units.size();
+    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_units, std::max<size_t>(1, units.size()) * sizeof(gs_unit)));
+    if (!units.empty())
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_units, units.data(), units.size() * sizeof(gs_unit),
+                                           cudaMemcpyHostToDevice, ctx->stream));
+    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_runs, std::max<size_t>(1, runs.size()) * sizeof(gs_tile_run)));
+    if (!runs.empty())
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_runs, runs.data(), runs.size() * sizeof(gs_tile_run),
+                                           cudaMemcpyHostToDevice, ctx->stream));
     GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_tile_off, tile_off.size() * sizeof(uint64_t)));
     GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_tile_rc, std::max<size_t>(1, tile_rc.size()) * sizeof(uint32_t)));
     GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_items, std::max<size_t>(1, items.size()) * sizeof(gs_item)));
@@ -328,7 +380,7 @@ gs_status gs_upload_graph(gs_ctx* ctx, const uint64_t* start, uint64_t n_start,
         st = gs_fail(ctx, GS_ERR_OOM, "grid exceeds the HBM tile budget; use the streamed sweep");
     if (st == GS_OK) {
         g->E = n_edges;
-        st = gs_dev_alloc(ctx, (void**)&g->d_rec, std::max<uint64_t>(1, n_edges) * 4);
+        st = gs_alloc_records(ctx, &g->d_rec, n_edges);
         if (st == GS_OK && n_edges) {
             cudaError_t e = cudaMemcpyAsync(g->d_rec, grid, n_edges * 4, cudaMemcpyHostToDevice, ctx->stream);
             if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "cudaMemcpyAsync(grid)");
@@ -362,7 +414,7 @@ gs_status gs_upload_graph_device(gs_ctx* ctx, const uint64_t* d_start, uint64_t 
     if (st == GS_OK) st = check_start(g, n_start, n_edges);
     if (st == GS_OK) {
         g->E = n_edges;
-        st = gs_dev_alloc(ctx, (void**)&g->d_rec, std::max<uint64_t>(1, n_edges) * 4);
+        st = gs_alloc_records(ctx, &g->d_rec, n_edges);
         if (st == GS_OK && n_edges) {
             cudaError_t e = cudaMemcpyAsync(g->d_rec, d_grid, n_edges * 4, cudaMemcpyDeviceToDevice, ctx->stream);
             if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "cudaMemcpyAsync(grid)");
@@ -481,6 +533,11 @@ gs_status gs_state_free(gs_state* s) {
     gs_dev_free(s->d_touched);
     gs_dev_free(s->d_deg);
     gs_dev_free(s->d_kactive);
+    gs_dev_free(s->d_error);
+    gs_dev_free(s->d_fv);
+    gs_dev_free(s->d_uflags);
+    gs_dev_free(s->d_sel);
+    gs_dev_free(s->d_cub);
     delete s;
     return GS_OK;
 }

@@ -1,0 +1,338 @@
+// BFS sweep and finalize (sm_100a): the level sweep of bfs.cpp:138-185.
+//
+// Per-vertex state in HBM (L2-resident for the graph sizes of interest):
+//   st[v >> 4]  2 bits per vertex, bit 0 frontier (depth == level), bit 1
+//               visited (depth != 0); 16 KB per 2^16-vertex window
+//   next[v>>5]  discovered during this sweep
+//   depth[v]    u8, written by the finalize for new vertices
+//
+// A CTA sweeps one run at a time (consecutive tiles of one tile row inside
+// a group, <= kRunRecords records).  The row window's state (16 KB) is
+// brought into shared memory once per run with one cp.async.bulk copy; the
+// run's units (tile slices of <= kUnitRecords records) are spread over the
+// warps, each warp streaming its unit's records with 128-bit evict-first
+// loads.  Per record: the row end's state comes from shared memory, the
+// column end's from global memory through L1 — tiles written by the device
+// converter are sorted by column offset, so the 32 lookups of a warp fall
+// on a few neighbouring lines.  A discovered row end sets a bit in a
+// shared bitmap OR-ed into `next` once per run (its dirty words only); a
+// discovered column end goes straight to `next`.  No barrier between tiles.
+//
+// Reference rule kept: a tile is swept when its row window (or, half grid,
+// its column window) holds a frontier vertex (grid::bfs_mmap,
+// gstore.cpp:2671-2698); a record discovers its unvisited end from its
+// frontier end (bfs.cpp:158-177).  Depth values do not depend on the order
+// in which records are visited, so the result is the reference's.
+#include "gs_internal.cuh"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr uint32_t kStWords = 4096;           // 2-bit state words per window
+constexpr uint32_t kStBytes = kStWords * 4;   // 16 KB
+constexpr uint32_t kNxWords = 2048;           // 1-bit words per window
+constexpr long long kWaitLimit = 1ll << 24;   // bounded mbarrier waits
+
+struct __align__(128) BfsSmem {
+    uint32_t strow[kStWords];
+    uint32_t nx[kNxWords];
+    uint32_t dirty[kNxWords / 32];
+    unsigned long long bar;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Bounded wait for the phase with the given parity; false on timeout.
+__device__ __forceinline__ bool bar_wait(unsigned long long* bar, uint32_t parity) {
+    const uint32_t a = smem_addr(bar);
+    for (long long i = 0; i < kWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+struct RunArgs {
+    const gs_tile_run* runs;
+    uint64_t n_runs;
+    const gs_unit* units;
+    const uint32_t* rec;
+    const uint32_t* st;
+    uint32_t* next;
+    const uint8_t* act;
+    uint8_t* act_next;
+    int directed;
+    int* error;
+};
+
+__global__ void __launch_bounds__(kThreads) bfs_run_kernel(RunArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    BfsSmem& m = *reinterpret_cast<BfsSmem*>(smem_raw);
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&m.bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (uint32_t w = tid; w < kNxWords; w += kThreads) m.nx[w] = 0;
+    if (tid < kNxWords / 32) m.dirty[tid] = 0;
+    __syncthreads();
+    uint32_t parity = 0;
+
+    for (uint64_t ri = blockIdx.x; ri < a.n_runs; ri += gridDim.x) {
+        const gs_tile_run run = a.runs[ri];
+        const uint32_t row = a.units[run.unit_beg].rc >> 16;
+        const bool ar = a.act[row] != 0;
+        // the run is swept when its row window or any column window is active
+        int any = ar ? 1 : 0;
+        if (!ar && !a.directed)
+            for (uint32_t ui = run.unit_beg + tid; ui < run.unit_end; ui += kThreads)
+                any |= a.act[a.units[ui].rc & 0xFFFFu] != 0;
+        if (!__syncthreads_or(any)) continue;
+
+        if (tid == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&m.bar)),
+                         "r"(kStBytes)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_addr(m.strow)),
+                "l"(a.st + ((size_t)row << 12)), "r"(kStBytes), "r"(smem_addr(&m.bar))
+                : "memory");
+        }
+        const bool got = bar_wait(&m.bar, parity);
+        parity ^= 1;
+        if (!__syncthreads_and(got)) {
+            if (tid == 0) atomicExch(a.error, 1);
+            return;   // uniform; nothing else in flight
+        }
+        const uint32_t mr = ar ? 1u : 0u;
+        for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps) {
+            const gs_unit d = a.units[ui];
+            const uint32_t col = d.rc & 0xFFFFu;
+            const uint32_t mc = (!a.directed && a.act[col]) ? 2u : 0u;
+            if (!mr && !mc) continue;                       // warp-uniform
+            const uint32_t* colst = a.st + ((size_t)col << 12);
+            uint32_t* next_col = a.next + ((size_t)col << 11);
+            bool hit = false;
+            // bit 0: the column end is discovered (row end in the frontier,
+            // column end unvisited, bfs.cpp:158-164); bit 1: the row end
+            // (bfs.cpp:166-172)
+            auto visit = [&](uint32_t r) {
+                const uint32_t v0 = r & 0xFFFFu, v1 = r >> 16;
+                const uint32_t s0 = m.strow[v0 >> 4] >> ((v0 & 15) << 1);
+                const uint32_t s1 = __ldg(colst + (v1 >> 4)) >> ((v1 & 15) << 1);
+                const uint32_t c = (s0 & ~(s1 >> 1) & mr) | (((s1 & ~(s0 >> 1)) << 1) & mc);
+                if (c & 1u) {
+                    atomicOr(next_col + (v1 >> 5), 1u << (v1 & 31));
+                    hit = true;
+                }
+                if (c & 2u) {
+                    const uint32_t w = v0 >> 5, bit = 1u << (v0 & 31);
+                    if (!(m.nx[w] & bit) && atomicOr(m.nx + w, bit) == 0)
+                        atomicOr(m.dirty + (w >> 5), 1u << (w & 31));
+                }
+            };
+            const uint64_t b = d.rec_beg, e = d.rec_beg + d.n;
+            uint64_t ab = (b + 3) & ~3ull;
+            if (ab > e) ab = e;
+            uint64_t ae = e & ~3ull;
+            if (ae < ab) ae = ab;
+            if (b + lane < ab) visit(__ldcs(a.rec + b + lane));
+            if (ae + lane < e) visit(__ldcs(a.rec + ae + lane));
+            const uint4* r4 = reinterpret_cast<const uint4*>(a.rec + ab);
+            const uint32_t n4 = (uint32_t)((ae - ab) >> 2);
+            for (uint32_t k = lane; k < n4; k += 64) {
+                const uint4 q0 = __ldcs(r4 + k);
+                const bool two = k + 32 < n4;
+                uint4 q1 = make_uint4(0, 0, 0, 0);
+                if (two) q1 = __ldcs(r4 + k + 32);
+                visit(q0.x);
+                visit(q0.y);
+                visit(q0.z);
+                visit(q0.w);
+                if (two) {
+                    visit(q1.x);
+                    visit(q1.y);
+                    visit(q1.z);
+                    visit(q1.w);
+                }
+            }
+            if (__any_sync(0xFFFFFFFFu, hit) && lane == 0) a.act_next[col] = 1;   // read_part_next->set_bit_atomic(j)
+        }
+        __syncthreads();
+        // row side: OR the dirty words into next, clear them
+        bool any_row = false;
+        if (tid < kNxWords / 32) {
+            uint32_t dw = m.dirty[tid];
+            if (dw) {
+                any_row = true;
+                m.dirty[tid] = 0;
+                uint32_t* dst = a.next + ((size_t)row << 11) + tid * 32;
+                uint32_t* src = m.nx + tid * 32;
+                while (dw) {
+                    const int k = __ffs(dw) - 1;
+                    atomicOr(dst + k, src[k]);
+                    src[k] = 0;
+                    dw &= dw - 1;
+                }
+            }
+        }
+        if (__syncthreads_or(any_row) && tid == 0) a.act_next[row] = 1;        // read_part_next->set_bit_atomic(i)
+    }
+}
+
+// Bits 1,3,5,... of x gathered into bits 0..15.
+__device__ __forceinline__ uint32_t odd_bits(uint32_t x) {
+    x = (x >> 1) & 0x55555555u;
+    x = (x | (x >> 1)) & 0x33333333u;
+    x = (x | (x >> 2)) & 0x0F0F0F0Fu;
+    x = (x | (x >> 4)) & 0x00FF00FFu;
+    return (x | (x >> 8)) & 0x0000FFFFu;
+}
+// Bits 0..15 of x spread to bits 0,2,4,...
+__device__ __forceinline__ uint32_t spread_bits(uint32_t x) {
+    x &= 0xFFFFu;
+    x = (x | (x << 8)) & 0x00FF00FFu;
+    x = (x | (x << 4)) & 0x0F0F0F0Fu;
+    x = (x | (x << 2)) & 0x33333333u;
+    return (x | (x << 1)) & 0x55555555u;
+}
+
+// Per 32 vertices: new = next & ~visited; frontier := new; visited |= new;
+// depth[v] = level + 1 for new vertices; next := 0 (iteration_finalize,
+// bfs.cpp:187-224 — the level count is exact here).
+__global__ void bfs_finalize_kernel(uint32_t* __restrict__ st, uint32_t* __restrict__ next,
+                                    uint8_t* __restrict__ depth, uint64_t n_words, uint8_t next_level,
+                                    unsigned long long* count) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t local = 0;
+    for (uint64_t w = tid; w < n_words; w += nth) {
+        const uint32_t nx = next[w];
+        const uint2 s = reinterpret_cast<const uint2*>(st)[w];
+        if (nx) next[w] = 0;
+        const uint32_t vis = odd_bits(s.x) | (odd_bits(s.y) << 16);
+        const uint32_t fresh = nx & ~vis;
+        if (fresh == 0 && ((s.x | s.y) & 0x55555555u) == 0) continue;
+        const uint32_t e0 = spread_bits(fresh), e1 = spread_bits(fresh >> 16);
+        reinterpret_cast<uint2*>(st)[w] =
+            make_uint2((s.x & 0xAAAAAAAAu) | e0 | (e0 << 1), (s.y & 0xAAAAAAAAu) | e1 | (e1 << 1));
+        uint32_t x = fresh;
+        while (x) {
+            const int k = __ffs(x) - 1;
+            depth[w * 32 + k] = next_level;
+            x &= x - 1;
+        }
+        local += __popc(fresh);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xFFFFFFFFu, local, o);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, (unsigned long long)local);
+}
+
+__global__ void bfs_seed_kernel(uint8_t* depth, uint32_t* st, uint8_t* act, uint64_t root) {
+    depth[root] = 1;                                 // bfs.cpp:70
+    st[root >> 4] = 3u << ((root & 15) << 1);        // frontier + visited
+    act[root >> 16] = 1;                             // calc_part_needed, bfs.cpp:324-338
+}
+
+inline uint32_t blocks_for(uint64_t n, const gs_ctx* ctx) {
+    uint64_t b = (n + 255) / 256;
+    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(b, gs_grid_size(ctx, 16)));
+}
+
+}  // namespace
+
+gs_status bfs_init(gs_state* s) {
+    gs_graph* g = s->g;
+    gs_ctx* ctx = g->ctx;
+    const uint64_t words = g->N / 32;
+    if (!s->d_depth) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_depth, g->N));
+    if (!s->d_front) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_front, words * 8));    // 2-bit state
+    if (!s->d_visited) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_visited, words * 4)); // next bitmap
+    if (!s->d_act) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_act, g->nw));
+    if (!s->d_act_next) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_act_next, g->nw));
+    if (!s->d_error) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_error, sizeof(uint64_t)));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_depth, 0, g->N, ctx->stream));   // INFTY = 0
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_front, 0, words * 8, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_visited, 0, words * 4, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_act, 0, g->nw, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_act_next, 0, g->nw, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_error, 0, sizeof(uint64_t), ctx->stream));
+    bfs_seed_kernel<<<1, 1, 0, ctx->stream>>>(s->d_depth, s->d_front, s->d_act, (uint64_t)s->arg);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    ctx->launches++;
+    s->level = 1;
+    s->level_counts.clear();
+    s->level_act.clear();
+    return GS_OK;
+}
+
+gs_status bfs_sweep(gs_state* s) {
+    gs_graph* g = s->g;
+    gs_ctx* ctx = g->ctx;
+    // Window flags of this sweep, kept for the swept-record statistics.
+    s->level_act.emplace_back(g->nw);
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(s->level_act.back().data(), s->d_act, g->nw, cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+    if (g->R == 0) {
+        s->step += 1;
+        return GS_OK;
+    }
+    static bool attr_set[64] = {false};
+    if (!attr_set[ctx->device & 63]) {
+        GS_CHECK_CUDA(ctx, cudaFuncSetAttribute(bfs_run_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)sizeof(BfsSmem)));
+        attr_set[ctx->device & 63] = true;
+    }
+    RunArgs a{g->d_runs, g->R, g->d_units, g->d_rec, s->d_front, s->d_visited, s->d_act, s->d_act_next,
+              g->directed, (int*)s->d_error};
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(g->R, gs_grid_size(ctx, 6));
+    gs_timer_begin(ctx);
+    bfs_run_kernel<<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    ctx->launches++;
+    gs_timer_end(ctx, GS_ALGO_BFS, 0);
+    s->step += 1;
+    return GS_OK;
+}
+
+gs_status bfs_finalize(gs_state* s, int64_t* frontier, int* done) {
+    gs_graph* g = s->g;
+    gs_ctx* ctx = g->ctx;
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_scalars, 0, sizeof(uint64_t), ctx->stream));
+    const uint64_t words = g->N / 32;
+    bfs_finalize_kernel<<<blocks_for(words, ctx), 256, 0, ctx->stream>>>(
+        s->d_front, s->d_visited, s->d_depth, words, (uint8_t)(s->level + 1), (unsigned long long*)ctx->d_scalars);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    ctx->launches++;
+    // swap(read_part, read_part_next); read_part_next->reset() (bfs.cpp:322-324)
+    std::swap(s->d_act, s->d_act_next);
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_act_next, 0, g->nw, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->h_scalars, ctx->d_scalars, sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->h_scalars + 1, s->d_error, sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const uint64_t count = ctx->h_scalars[0];
+    if (ctx->h_scalars[1] != 0) return gs_fail(ctx, GS_ERR_TIMEOUT, "BFS sweep: a bounded wait gave up");
+    s->level_counts.push_back(count);
+    *frontier = (int64_t)count;
+    if (count == 0) {
+        *done = 1;
+        return GS_OK;
+    }
+    if (s->level == 254) return gs_fail(ctx, GS_ERR_RANGE, "BFS exceeds 254 levels (u8 depth_t)");
+    s->level += 1;
+    *done = 0;
+    return GS_OK;
+}

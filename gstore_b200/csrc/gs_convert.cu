@@ -6,12 +6,15 @@
 //              find its tile, count it, count both endpoint degrees
 //              (out-degree only for the directed grid) — gstore.cpp:1270-1312
 //  2. scan:    exclusive prefix sum of the tile counts -> .start (:1316-1324)
-//  3. scatter: each edge takes the next slot of its tile (:1403-1447); the
-//              in-tile order is the order the atomics resolve, as in the
-//              reference (thread order).
+//  3. scatter: each edge takes the next slot of its tile (:1403-1447)
+//  4. sort:    records inside each tile are sorted by value (v1, then v0).
+//              The reference leaves them in thread order, so any in-tile
+//              order is a valid .grid; a sorted one is deterministic and lets
+//              a warp's consecutive records touch neighbouring state words.
 #include "gs_internal.cuh"
 
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_segmented_sort.cuh>
 
 namespace {
 
@@ -72,7 +75,73 @@ __global__ void scatter_kernel(const uint2* __restrict__ pairs, uint64_t n, uint
     }
 }
 
+__global__ void rebase_offsets_kernel(const uint64_t* __restrict__ start, uint64_t t0, uint64_t n,
+                                      int* __restrict__ out) {
+    const uint64_t base = start[t0];
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = (int)(start[t0 + i] - base);
+}
+
 }  // namespace
+
+// Sorts the records of every tile in place (segments = tiles of `start`).
+gs_status gs_sort_tiles(gs_ctx* ctx, const uint64_t* d_start, uint64_t n_tiles, uint32_t* d_rec, uint64_t n_rec) {
+    if (n_rec < 2 || n_tiles == 0) return GS_OK;
+    std::vector<uint64_t> h(n_tiles + 1);
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(h.data(), d_start, (n_tiles + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    // chunks of whole tiles with at most 2^30 records and 2^24 tiles each
+    const uint64_t kMaxRec = 1ull << 30, kMaxTiles = 1ull << 24;
+    uint32_t* d_out = nullptr;
+    int* d_off = nullptr;
+    void* d_tmp = nullptr;
+    size_t tmp_bytes = 0;
+    gs_status st = gs_alloc_records(ctx, &d_out, n_rec);
+    if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&d_off, (std::min(n_tiles, kMaxTiles) + 1) * sizeof(int));
+    uint64_t t0 = 0;
+    while (st == GS_OK && t0 < n_tiles) {
+        uint64_t t1 = t0;
+        while (t1 < n_tiles && t1 - t0 < kMaxTiles && h[t1 + 1] - h[t0] <= kMaxRec) ++t1;
+        if (t1 == t0) {
+            st = gs_fail(ctx, GS_ERR_FORMAT, "a tile holds more than 2^30 records");
+            break;
+        }
+        const uint64_t nr = h[t1] - h[t0];
+        if (nr > 1) {
+            rebase_offsets_kernel<<<256, 256, 0, ctx->stream>>>(d_start, t0, t1 - t0, d_off);
+            ctx->launches++;
+            size_t need = 0;
+            cudaError_t e = cub::DeviceSegmentedSort::SortKeys(nullptr, need, d_rec + h[t0], d_out + h[t0], (int)nr,
+                                                               (int)(t1 - t0), d_off, d_off + 1, ctx->stream);
+            if (e == cudaSuccess && need > tmp_bytes) {
+                gs_dev_free(d_tmp);
+                d_tmp = nullptr;
+                tmp_bytes = need;
+                st = gs_dev_alloc(ctx, &d_tmp, tmp_bytes);
+            }
+            if (e == cudaSuccess && st == GS_OK)
+                e = cub::DeviceSegmentedSort::SortKeys(d_tmp, need, d_rec + h[t0], d_out + h[t0], (int)nr,
+                                                       (int)(t1 - t0), d_off, d_off + 1, ctx->stream);
+            if (e != cudaSuccess && st == GS_OK) st = gs_cuda_fail(ctx, e, "segmented sort");
+            ctx->launches++;
+        } else if (nr == 1) {
+            cudaError_t e = cudaMemcpyAsync(d_out + h[t0], d_rec + h[t0], 4, cudaMemcpyDeviceToDevice, ctx->stream);
+            if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "copy");
+        }
+        t0 = t1;
+    }
+    if (st == GS_OK) {
+        cudaError_t e = cudaMemcpyAsync(d_rec, d_out, n_rec * 4, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "copy sorted records");
+    } else {
+        cudaStreamSynchronize(ctx->stream);
+    }
+    gs_dev_free(d_out);
+    gs_dev_free(d_off);
+    gs_dev_free(d_tmp);
+    return st;
+}
 
 gs_status gs_convert_launch(gs_ctx* ctx, const uint32_t* d_pairs, uint64_t n_pairs, uint64_t V, int directed,
                             uint64_t** d_start_out, uint32_t** d_grid_out, int32_t** d_degree_out,
@@ -122,7 +191,7 @@ gs_status gs_convert_launch(gs_ctx* ctx, const uint32_t* d_pairs, uint64_t n_pai
         st = gs_fail(ctx, GS_ERR_FORMAT, "an edge endpoint is >= the vertex count");
         goto fail;
     }
-    if ((st = gs_dev_alloc(ctx, (void**)&d_rec, std::max<uint64_t>(total, 1) * 4)) != GS_OK) goto fail;
+    if ((st = gs_alloc_records(ctx, &d_rec, total)) != GS_OK) goto fail;
     if ((st = gs_dev_alloc(ctx, (void**)&d_cursor, T * 4)) != GS_OK) goto fail;
     CV_CHECK(cudaMemsetAsync(d_cursor, 0, T * 4, ctx->stream));
     if (n_pairs) {
@@ -132,6 +201,8 @@ gs_status gs_convert_launch(gs_ctx* ctx, const uint32_t* d_pairs, uint64_t n_pai
     }
     CV_CHECK(cudaStreamSynchronize(ctx->stream));
     gs_dev_free(d_cursor);
+    d_cursor = nullptr;
+    if ((st = gs_sort_tiles(ctx, d_start, T, d_rec, total)) != GS_OK) goto fail;
     gs_dev_free(d_tmp);
     *d_start_out = d_start;
     *d_grid_out = d_rec;

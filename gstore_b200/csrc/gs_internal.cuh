@@ -24,6 +24,36 @@ struct alignas(16) gs_item {
     uint32_t rc;  // row << 16 | col
 };
 
+// Upper bound of records per run.
+constexpr uint64_t kRunRecords = 131072;
+// Zeroed records after the last one, so 16-byte-rounded bulk copies of a
+// record range stay inside the allocation.
+constexpr uint64_t kRecPad = 4;
+
+// One run: consecutive non-empty tiles [tile_beg, tile_end) of the tile table
+// that share a tile row and a group (contiguous in the file), restricted to
+// records [rec_beg, rec_end).  A tile larger than kRunRecords is cut into
+// several single-tile runs.
+struct alignas(8) gs_tile_run {
+    uint64_t rec_beg;
+    uint64_t rec_end;
+    uint32_t tile_beg;
+    uint32_t tile_end;
+    uint32_t unit_beg;   // the run's units [unit_beg, unit_end) of the unit table
+    uint32_t unit_end;
+};
+
+// Records per BFS unit.
+constexpr uint32_t kUnitRecords = 2048;
+
+// One unit: records [rec_beg, rec_beg + n) of the tile at row rc >> 16,
+// column rc & 0xFFFF (n <= kUnitRecords; units follow the file order).
+struct alignas(16) gs_unit {
+    uint64_t rec_beg;
+    uint32_t n;
+    uint32_t rc;
+};
+
 struct KernelTimes {
     uint64_t launches = 0;
     double ms = 0.0;
@@ -56,8 +86,12 @@ struct gs_graph {
     uint64_t E = 0;      // records
     uint64_t T = 0;      // non-empty tiles
     uint64_t I = 0;      // work items
+    uint64_t R = 0;      // runs
+    uint64_t U = 0;      // units
     uint32_t* d_rec = nullptr;
     gs_item* d_items = nullptr;
+    gs_tile_run* d_runs = nullptr;
+    gs_unit* d_units = nullptr;
     uint64_t* d_tile_off = nullptr;   // T + 1 record offsets of non-empty tiles
     uint32_t* d_tile_rc = nullptr;    // T packed (row << 16 | col)
     int32_t* d_degree = nullptr;      // N
@@ -77,8 +111,14 @@ struct gs_state {
     // BFS
     uint8_t level = 1;
     uint8_t* d_depth = nullptr;      // N
-    uint32_t* d_front = nullptr;     // N/32 frontier bitmap
-    uint32_t* d_visited = nullptr;   // N/32
+    uint32_t* d_front = nullptr;     // N/32 frontier words
+    uint32_t* d_visited = nullptr;   // N/32 words: discovered-this-sweep bitmap
+    uint64_t* d_error = nullptr;     // bounded-wait failure flag
+    uint2* d_fv = nullptr;           // N/32 {frontier, visited} word pairs
+    uint8_t* d_uflags = nullptr;     // 2 x U: per-unit activity flags, selection flags
+    uint32_t* d_sel = nullptr;       // U + 1: selected unit indices, then their count
+    void* d_cub = nullptr;           // compaction scratch
+    size_t cub_bytes = 0;
     uint8_t* d_act = nullptr;        // nw window flags (current)
     uint8_t* d_act_next = nullptr;   // nw
     std::vector<uint64_t> level_counts;
@@ -126,6 +166,7 @@ void gs_geometry_of(uint64_t V, int directed, uint32_t* p, uint32_t* p_s, uint64
 
 // ------------------------------------------------------- device launchers --
 gs_status gs_dev_alloc(gs_ctx* ctx, void** ptr, size_t bytes);
+gs_status gs_alloc_records(gs_ctx* ctx, uint32_t** ptr, uint64_t n_records);
 void gs_dev_free(void* ptr);
 
 gs_status launch_validate_records(gs_graph* g, int* d_flag);
@@ -158,6 +199,7 @@ gs_status gs_convert_launch(gs_ctx* ctx, const uint32_t* d_pairs, uint64_t n_pai
                             int directed, uint64_t** d_start_out, uint32_t** d_grid_out,
                             int32_t** d_degree_out, uint64_t* n_start, uint64_t* n_rec);
 
+gs_status gs_sort_tiles(gs_ctx* ctx, const uint64_t* d_start, uint64_t n_tiles, uint32_t* d_rec, uint64_t n_rec);
 gs_status gs_graph_adopt(gs_ctx* ctx, uint64_t V, const uint64_t* d_start, uint64_t n_start, uint32_t* d_rec,
                          uint64_t n_edges, const int32_t* d_degree, gs_graph** out);
 

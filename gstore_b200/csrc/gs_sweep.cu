@@ -136,76 +136,6 @@ struct DegreeOp {
 };
 
 // -------------------------------------------------------------------- BFS --
-struct BfsOp {
-    const uint32_t* front;
-    const uint32_t* visited;
-    uint8_t* depth;
-    const uint8_t* act;
-    uint8_t* act_next;
-    uint8_t next_level;
-    int directed;
-    struct Item {
-        uint32_t rb, cb;
-        bool fr, fc, hit_r, hit_c;
-    };
-    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
-        // tile-skip rule of bfs_mmap (gstore.cpp:2671-2698): a tile is swept
-        // when its row window (or, half grid, its column window) holds a
-        // frontier vertex.
-        c.fr = act[row] != 0;
-        c.fc = !directed && act[col] != 0;
-        c.rb = row << 16;
-        c.cb = col << 16;
-        c.hit_r = c.hit_c = false;
-        return c.fr || c.fc;
-    }
-    __device__ void record(uint32_t r, Item& c) const {
-        const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
-        if (c.fr && bit_of(front, a) && !bit_of(visited, b)) {  // bfs.cpp:158-164
-            depth[b] = next_level;
-            c.hit_c = true;
-        }
-        if (c.fc && bit_of(front, b) && !bit_of(visited, a)) {  // bfs.cpp:166-172
-            depth[a] = next_level;
-            c.hit_r = true;
-        }
-    }
-    __device__ void end(uint32_t row, uint32_t col, Item& c) const {
-        const bool hc = __any_sync(kFull, c.hit_c), hr = __any_sync(kFull, c.hit_r);
-        if ((threadIdx.x & 31) == 0) {
-            if (hc) act_next[col] = 1;  // read_part_next->set_bit_atomic(j)
-            if (hr) act_next[row] = 1;  // read_part_next->set_bit_atomic(i)
-        }
-    }
-};
-
-// One warp per 32-vertex word: the new frontier is depth == next_level.
-__global__ void bfs_finalize_kernel(const uint8_t* __restrict__ depth, uint32_t* __restrict__ front,
-                                    uint32_t* __restrict__ visited, uint64_t n_words,
-                                    uint8_t next_level, unsigned long long* count) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    uint64_t local = 0;
-    for (uint64_t w = warp; w < n_words; w += nwarps) {
-        const uint32_t bits = __ballot_sync(kFull, depth[w * 32 + lane] == next_level);
-        if (lane == 0) {
-            front[w] = bits;
-            visited[w] |= bits;
-            local += __popc(bits);
-        }
-    }
-    if (lane == 0 && local) atomicAdd(count, (unsigned long long)local);
-}
-
-__global__ void bfs_seed_kernel(uint8_t* depth, uint32_t* front, uint32_t* visited, uint8_t* act,
-                                uint64_t root) {
-    depth[root] = 1;                                   // bfs.cpp:70
-    front[root >> 5] = 1u << (root & 31);
-    visited[root >> 5] = 1u << (root & 31);
-    act[root >> 16] = 1;                               // calc_part_needed, bfs.cpp:324-338
-}
-
 __global__ void count_reached_kernel(const uint8_t* __restrict__ depth, uint64_t n,
                                      unsigned long long* out) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -445,69 +375,6 @@ gs_status launch_degree_from_records(gs_graph* g) {
 }
 
 // ------------------------------------------------------------------- BFS ----
-gs_status bfs_init(gs_state* s) {
-    gs_graph* g = s->g;
-    gs_ctx* ctx = g->ctx;
-    if (!s->d_depth) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_depth, g->N));
-    if (!s->d_front) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_front, g->N / 8));
-    if (!s->d_visited) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_visited, g->N / 8));
-    if (!s->d_act) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_act, g->nw));
-    if (!s->d_act_next) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_act_next, g->nw));
-    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_depth, 0, g->N, ctx->stream));   // INFTY = 0
-    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_front, 0, g->N / 8, ctx->stream));
-    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_visited, 0, g->N / 8, ctx->stream));
-    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_act, 0, g->nw, ctx->stream));
-    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_act_next, 0, g->nw, ctx->stream));
-    bfs_seed_kernel<<<1, 1, 0, ctx->stream>>>(s->d_depth, s->d_front, s->d_visited, s->d_act,
-                                              (uint64_t)s->arg);
-    GS_CHECK_CUDA(ctx, cudaGetLastError());
-    ctx->launches++;
-    s->level = 1;
-    s->level_counts.clear();
-    s->level_act.clear();
-    return GS_OK;
-}
-
-gs_status bfs_sweep(gs_state* s) {
-    gs_graph* g = s->g;
-    BfsOp op{s->d_front, s->d_visited, s->d_depth, s->d_act, s->d_act_next,
-             (uint8_t)(s->level + 1), g->directed};
-    // Window flags of this sweep, kept for the swept-record statistics.
-    s->level_act.emplace_back(g->nw);
-    GS_CHECK_CUDA(g->ctx, cudaMemcpyAsync(s->level_act.back().data(), s->d_act, g->nw,
-                                          cudaMemcpyDeviceToHost, g->ctx->stream));
-    GS_TRY(launch_sweep(g, op, GS_ALGO_BFS, 0));
-    s->step += 1;
-    return GS_OK;
-}
-
-gs_status bfs_finalize(gs_state* s, int64_t* frontier, int* done) {
-    gs_graph* g = s->g;
-    gs_ctx* ctx = g->ctx;
-    GS_TRY(zero_scalar(ctx));
-    const uint64_t words = g->N / 32;
-    bfs_finalize_kernel<<<blocks_for(words * 32, ctx), kThreads, 0, ctx->stream>>>(
-        s->d_depth, s->d_front, s->d_visited, words, (uint8_t)(s->level + 1),
-        (unsigned long long*)ctx->d_scalars);
-    GS_CHECK_CUDA(ctx, cudaGetLastError());
-    ctx->launches++;
-    // swap(read_part, read_part_next); read_part_next->reset() (bfs.cpp:322-324)
-    std::swap(s->d_act, s->d_act_next);
-    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_act_next, 0, g->nw, ctx->stream));
-    uint64_t count = 0;
-    GS_TRY(read_scalar(ctx, &count));
-    s->level_counts.push_back(count);
-    *frontier = (int64_t)count;
-    if (count == 0) {
-        *done = 1;
-        return GS_OK;
-    }
-    if (s->level == 254) return gs_fail(ctx, GS_ERR_RANGE, "BFS exceeds 254 levels (u8 depth_t)");
-    s->level += 1;
-    *done = 0;
-    return GS_OK;
-}
-
 gs_status gs_count_reached(gs_state* s, uint64_t* reached, uint64_t* edges_in_component) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
