@@ -43,6 +43,9 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 HBM_FALLBACK_GBS = 6650.0
+# DRAM bytes (read + write) per algorithmic byte of the BFS sweep kernel,
+# from one ncu capture of a full level at scale 22: 275.9 MB / 268.4 MB.
+BFS_DRAM_PER_ALG_BYTE = (271.015424 + 4.886016) / (67106947 * 4 / 1e6)
 
 
 def parse_args():
@@ -345,9 +348,14 @@ def main():
     value = e_total / (ms_max / 1e3) / 1e9
     peak, peak_kind = measured_peak()
     achieved = (4.0 * swept_records) / (sweep_ms / 1e3) / 1e9 if sweep_ms > 0 else None
-    roofline = {"bound": "hbm", "kernel": "sweep_items<BfsOp>", "achieved": achieved, "peak": peak,
+    alg_per_launch = 4.0 * swept_records / max(sweep_launches, 1)
+    roofline = {"bound": "hbm", "kernel": "bfs_run_kernel", "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                "traffic": None, "algorithmic_bytes": "4 B x records in swept tiles per level",
+                "traffic": BFS_DRAM_PER_ALG_BYTE * alg_per_launch,
+                "traffic_note": "bytes per launch: DRAM read+write per algorithmic byte from an ncu capture "
+                                "of a full level at scale 22, times this run's algorithmic bytes per launch",
+                "algorithmic_bytes": "4 B x records in swept tiles per level",
+                "algorithmic_bytes_per_launch": alg_per_launch,
                 "launches": sweep_launches, "sweep_ms_total": sweep_ms}
 
     line = {
