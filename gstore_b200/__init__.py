@@ -40,6 +40,7 @@ ABI_SYMBOLS = [
     "gs_graph_degree", "gs_state_create", "gs_state_free", "gs_state_reset", "gs_sweep", "gs_finalize", "gs_run",
     "gs_download", "gs_result_count", "gs_bfs_stats", "gs_pagerank_compat",
     "gs_kron_generate_device", "gs_kron_generate", "gs_convert", "gs_graph_download",
+    "gs_bfs_noalloc",
 ]
 
 
@@ -90,6 +91,7 @@ def lib():
             "gs_kron_generate": [vp, i32, i64, u64, u64, vp],
             "gs_convert": [vp, vp, u64, i32, u64, pvp],
             "gs_graph_download": [vp, vp, vp, vp],
+            "gs_bfs_noalloc": [vp, u64, vp, C.POINTER(C.c_int64)],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -262,6 +264,13 @@ class Graph:
         h = C.c_void_p()
         self.ctx._check(lib().gs_state_create(self._h, a, arg, C.byref(h)))
         return State(self, h, a)
+
+    def bfs_noalloc(self, root: int, d_depth: int) -> int:
+        """BFS into a caller-owned device buffer (uint8, V bytes) without any
+        allocation by the library; returns the number of sweeps."""
+        n = C.c_int64()
+        self.ctx._check(lib().gs_bfs_noalloc(self._h, root, C.c_void_p(d_depth), C.byref(n)))
+        return n.value
 
     # convenience: whole runs ------------------------------------------------
     def bfs(self, root: int) -> np.ndarray:

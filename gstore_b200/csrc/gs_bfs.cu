@@ -336,3 +336,36 @@ gs_status bfs_finalize(gs_state* s, int64_t* frontier, int* done) {
     *done = 0;
     return GS_OK;
 }
+
+// ------------------------------------------------- caller-provided buffers --
+// Launchers over explicit buffers for gs_bfs_noalloc (gs_noalloc.cu): the
+// same kernels as above, with the state living wherever the caller says.
+gs_status bfs_seed_into(gs_ctx* ctx, uint8_t* depth, uint32_t* st, uint8_t* act, uint64_t root) {
+    bfs_seed_kernel<<<1, 1, 0, ctx->stream>>>(depth, st, act, root);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    ctx->launches++;
+    return GS_OK;
+}
+
+gs_status bfs_level_into(gs_ctx* ctx, const gs_graph* g, uint8_t* depth, uint32_t* st, uint32_t* next,
+                         uint8_t* act, uint8_t* act_next, unsigned long long* count, int* error,
+                         uint8_t next_level) {
+    if (g->R) {
+        static bool attr_set[64] = {false};
+        if (!attr_set[ctx->device & 63]) {
+            GS_CHECK_CUDA(ctx, cudaFuncSetAttribute(bfs_run_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    (int)sizeof(BfsSmem)));
+            attr_set[ctx->device & 63] = true;
+        }
+        RunArgs a{g->d_runs, g->R, g->d_units, g->d_rec, st, next, act, act_next, g->directed, error};
+        const uint32_t grid = (uint32_t)std::min<uint64_t>(g->R, gs_grid_size(ctx, 6));
+        bfs_run_kernel<<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
+        GS_CHECK_CUDA(ctx, cudaGetLastError());
+        ctx->launches++;
+    }
+    const uint64_t words = g->N / 32;
+    bfs_finalize_kernel<<<blocks_for(words, ctx), 256, 0, ctx->stream>>>(st, next, depth, words, next_level, count);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    ctx->launches++;
+    return GS_OK;
+}

@@ -203,6 +203,11 @@ gs_status gs_sort_tiles(gs_ctx* ctx, const uint64_t* d_start, uint64_t n_tiles, 
 gs_status gs_graph_adopt(gs_ctx* ctx, uint64_t V, const uint64_t* d_start, uint64_t n_start, uint32_t* d_rec,
                          uint64_t n_edges, const int32_t* d_degree, gs_graph** out);
 
+gs_status bfs_seed_into(gs_ctx* ctx, uint8_t* depth, uint32_t* st, uint8_t* act, uint64_t root);
+gs_status bfs_level_into(gs_ctx* ctx, const gs_graph* g, uint8_t* depth, uint32_t* st, uint32_t* next,
+                         uint8_t* act, uint8_t* act_next, unsigned long long* count, int* error,
+                         uint8_t next_level);
+
 // Timing helpers around the main sweep kernel of an algorithm.
 void gs_timer_begin(gs_ctx* ctx);
 void gs_timer_end(gs_ctx* ctx, int algo, uint64_t bytes);

@@ -150,6 +150,20 @@ gs_status gs_result_count(gs_state* s, uint64_t* count);
 gs_status gs_bfs_stats(gs_state* s, uint64_t* edges_in_component, uint64_t* swept_records,
                        int max_levels, int* n_levels, uint64_t* level_counts);
 
+/* BFS without any allocation (no counterpart in the reference; added for
+ * callers that may not allocate device memory while they run queries, such
+ * as a host framework whose memory pool already owns the GPU, or a serving
+ * loop that cannot take the device-wide synchronisation of cudaMalloc).
+ * Runs the same sweep kernels as gs_run on a BFS state, keeps its scratch
+ * state in a fixed array inside the library (about 6 MiB per GPU, for the
+ * life of the process) and writes uint8 depth[V] (root 1, unreached 0) into
+ * the caller's device buffer d_depth.  Limit: V <= 16777216 (else
+ * GS_ERR_RANGE).  The first call on a device looks the array up; make it
+ * before any stream capture.  Calls overlapping on one GPU share the array
+ * and race: issue them one after another.  levels_out (may be NULL): sweeps
+ * done. */
+gs_status gs_bfs_noalloc(gs_graph* g, uint64_t root, uint8_t* d_depth, int64_t* levels_out);
+
 /* PageRank with the reference's int32 inverse-degree truncation
  * (pr.cpp:112-114) instead of the real inverse; must precede gs_run. */
 gs_status gs_pagerank_compat(gs_state* s, int enable);
