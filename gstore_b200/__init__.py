@@ -40,7 +40,7 @@ ABI_SYMBOLS = [
     "gs_graph_degree", "gs_state_create", "gs_state_free", "gs_state_reset", "gs_sweep", "gs_finalize", "gs_run",
     "gs_download", "gs_result_count", "gs_bfs_stats", "gs_pagerank_compat",
     "gs_kron_generate_device", "gs_kron_generate", "gs_convert", "gs_graph_download",
-    "gs_bfs_noalloc",
+    "gs_bfs_noalloc", "gs_upload_graph_streamed", "gs_stream_stats",
 ]
 
 
@@ -92,6 +92,8 @@ def lib():
             "gs_convert": [vp, vp, u64, i32, u64, pvp],
             "gs_graph_download": [vp, vp, vp, vp],
             "gs_bfs_noalloc": [vp, u64, vp, C.POINTER(C.c_int64)],
+            "gs_upload_graph_streamed": [vp, vp, u64, vp, u64, vp, u64, u64, pvp],
+            "gs_stream_stats": [vp, pu64, pu64, pu64, pu64],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -115,6 +117,12 @@ def geometry(V: int, directed: bool = False):
     p, ps, n = C.c_uint32(), C.c_uint32(), C.c_uint64()
     lib().gs_geometry(V, int(directed), C.byref(p), C.byref(ps), C.byref(n))
     return p.value, ps.value, n.value
+
+
+def part_id(gi: int, gj: int, si: int, sj: int, p: int) -> int:
+    """The reference's part id of tile (si, sj) in group (gi, gj):
+    group_full_index << 16 | si << 8 | sj (get_ij, gstore.h:199-220)."""
+    return ((gi * p + gj) << 16) | (si << 8) | sj
 
 
 def read_tile_files(prefix, V: int | None = None, with_degree: bool = True):
@@ -194,7 +202,23 @@ class Context:
         h = C.c_void_p()
         self._check(lib().gs_upload_graph(self._h, _ptr(start), start.size, _ptr(grid), grid.size,
                                           _ptr(degree), V, C.byref(h)))
-        return Graph(self, h)
+        # over the HBM budget the graph streams from `grid`: keep it alive
+        return Graph(self, h, keep=grid)
+
+    def upload_streamed(self, start, grid, degree, V: int, segment_bytes: int) -> "Graph":
+        """A graph whose records stay in host memory (`grid`, pinned by the
+        library unless it already is) and stream through two HBM segments of
+        segment_bytes each on every sweep."""
+        start = np.ascontiguousarray(start, np.uint64)
+        if not (isinstance(grid, np.ndarray) and grid.dtype == np.uint32 and grid.flags["C_CONTIGUOUS"]):
+            grid = np.ascontiguousarray(grid, np.uint32)
+        if degree is not None:
+            degree = np.ascontiguousarray(degree, np.int32)
+            assert degree.size >= V, "degree array shorter than V"
+        h = C.c_void_p()
+        self._check(lib().gs_upload_graph_streamed(self._h, _ptr(start), start.size, _ptr(grid), grid.size,
+                                                   _ptr(degree), V, segment_bytes, C.byref(h)))
+        return Graph(self, h, keep=grid)
 
     def upload_device(self, d_start: int, n_start: int, d_grid: int, n_edges: int, d_degree: int | None,
                       V: int) -> "Graph":
@@ -227,9 +251,10 @@ class Context:
 class Graph:
     """A resident tile grid (gs_graph)."""
 
-    def __init__(self, ctx: Context, handle):
+    def __init__(self, ctx: Context, handle, keep=None):
         self.ctx = ctx
         self._h = handle
+        self._keep = keep        # host records of a streamed graph
         e, t, i, v = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
         ctx._check(lib().gs_graph_info(self._h, C.byref(e), C.byref(t), C.byref(i), C.byref(v)))
         self.n_edges, self.n_tiles, self.n_items, self.V = e.value, t.value, i.value, v.value
@@ -239,12 +264,19 @@ class Graph:
         if self._h:
             lib().gs_graph_free(self._h)
             self._h = None
+        self._keep = None
 
     def __del__(self):
         try:
             self.free()
         except Exception:
             pass
+
+    def stream_stats(self) -> dict:
+        """Host-to-device traffic of a streamed graph since upload."""
+        b, c, sg, r = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+        self.ctx._check(lib().gs_stream_stats(self._h, C.byref(b), C.byref(c), C.byref(sg), C.byref(r)))
+        return {"bytes": b.value, "copies": c.value, "segments": sg.value, "reused": r.value}
 
     def degree(self) -> np.ndarray:
         out = np.empty(self.V, np.int32)
@@ -331,9 +363,15 @@ class State:
     def compat(self, enable: bool = True):
         self._check(lib().gs_pagerank_compat(self._h, int(enable)))
 
-    def sweep(self):
-        """algo_mem_part over every resident tile (algo.h:40)."""
-        self._check(lib().gs_sweep(self._h, None, 0))
+    def sweep(self, parts=None):
+        """algo_mem_part (algo.h:40) over every tile, or over the tiles of
+        the given part ranges [(part_start, part_end), ...] (inclusive, in
+        file order; ids from part_id)."""
+        if not parts:
+            self._check(lib().gs_sweep(self._h, None, 0))
+            return
+        arr = np.ascontiguousarray(np.asarray(parts, np.uint64).reshape(-1, 2))
+        self._check(lib().gs_sweep(self._h, _ptr(arr), arr.shape[0]))
 
     def finalize(self):
         """iteration_finalize(): returns (frontier, done)."""

@@ -158,6 +158,7 @@ gs_status gs_kernel_time(gs_ctx* ctx, int algo, uint64_t* launches, double* tota
 
 // ------------------------------------------------------------------ graph --
 static void free_graph_arrays(gs_graph* g) {
+    gs_stream_close(g);
     gs_dev_free(g->d_rec);
     gs_dev_free(g->d_items);
     gs_dev_free(g->d_tile_off);
@@ -182,9 +183,11 @@ static gs_status build_tables(gs_graph* g) {
     const std::vector<uint64_t>& st = g->h_start;
     std::vector<uint64_t>& tile_off = g->h_tile_off;
     std::vector<uint32_t>& tile_rc = g->h_tile_rc;
-    std::vector<gs_item> items;
-    std::vector<gs_tile_run> runs;
-    std::vector<gs_unit> units;
+    std::vector<gs_tile_run>& runs = g->h_runs;
+    std::vector<gs_unit>& units = g->h_units;
+    uint64_t n_items = 0;
+    runs.clear();
+    units.clear();
     tile_off.clear();
     tile_rc.clear();
     tile_off.reserve(1024);
@@ -235,13 +238,7 @@ static gs_status build_tables(gs_graph* g) {
                     }
                     tile_off.push_back(b);
                     tile_rc.push_back(rc);
-                    for (uint64_t x = b; x < e; x += kItemRecords) {
-                        gs_item it;
-                        it.beg = x;
-                        it.cnt = (uint32_t)std::min<uint64_t>(kItemRecords, e - x);
-                        it.rc = rc;
-                        items.push_back(it);
-                    }
+                    n_items += (e - b + kItemRecords - 1) / kItemRecords;
                 }
             }
         }
@@ -249,7 +246,7 @@ static gs_status build_tables(gs_graph* g) {
     close_run();
     tile_off.push_back(st[t]);
     g->T = tile_rc.size();
-    g->I = items.size();
+    g->I = n_items;
     g->R = runs.size();
     g->U = units.size();
     GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_units, std::max<size_t>(1, units.size()) * sizeof(gs_unit)));
@@ -262,14 +259,10 @@ static gs_status build_tables(gs_graph* g) {
                                            cudaMemcpyHostToDevice, ctx->stream));
     GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_tile_off, tile_off.size() * sizeof(uint64_t)));
     GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_tile_rc, std::max<size_t>(1, tile_rc.size()) * sizeof(uint32_t)));
-    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_items, std::max<size_t>(1, items.size()) * sizeof(gs_item)));
     GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_tile_off, tile_off.data(), tile_off.size() * sizeof(uint64_t),
                                        cudaMemcpyHostToDevice, ctx->stream));
     if (!tile_rc.empty())
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_tile_rc, tile_rc.data(), tile_rc.size() * sizeof(uint32_t),
-                                           cudaMemcpyHostToDevice, ctx->stream));
-    if (!items.empty())
-        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_items, items.data(), items.size() * sizeof(gs_item),
                                            cudaMemcpyHostToDevice, ctx->stream));
     // The host vectors die at return: wait for the copies.
     GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -376,8 +369,20 @@ gs_status gs_upload_graph(gs_ctx* ctx, const uint64_t* start, uint64_t n_start,
     GS_TRY(new_graph(ctx, V, &g));
     g->h_start.assign(start, start + std::min<uint64_t>(n_start, g->T_all + 1));
     gs_status st = check_start(g, n_start, n_edges);
-    if (st == GS_OK && ctx->budget && n_edges * 4 > ctx->budget)
-        st = gs_fail(ctx, GS_ERR_OOM, "grid exceeds the HBM tile budget; use the streamed sweep");
+    if (st == GS_OK && ctx->budget && n_edges * 4 > ctx->budget) {
+        // over the tile budget: stream the grid through two segments of half
+        // the budget each (the reference's -m semi-external mode)
+        g->E = n_edges;
+        st = gs_stream_open(g, grid, (ctx->budget / 2) & ~15ull);
+        if (st == GS_OK) st = finish_upload(g, degree, false);
+        if (st != GS_OK) {
+            free_graph_arrays(g);
+            delete g;
+            return st;
+        }
+        *out = g;
+        return GS_OK;
+    }
     if (st == GS_OK) {
         g->E = n_edges;
         st = gs_alloc_records(ctx, &g->d_rec, n_edges);
@@ -386,6 +391,27 @@ gs_status gs_upload_graph(gs_ctx* ctx, const uint64_t* start, uint64_t n_start,
             if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "cudaMemcpyAsync(grid)");
         }
     }
+    if (st == GS_OK) st = finish_upload(g, degree, false);
+    if (st != GS_OK) {
+        free_graph_arrays(g);
+        delete g;
+        return st;
+    }
+    *out = g;
+    return GS_OK;
+}
+
+gs_status gs_upload_graph_streamed(gs_ctx* ctx, const uint64_t* start, uint64_t n_start,
+                                   const uint32_t* grid, uint64_t n_edges, const int32_t* degree,
+                                   uint64_t V, uint64_t segment_bytes, gs_graph** out) {
+    if (!ctx || !start || !out || (n_edges && !grid)) return gs_fail(ctx, GS_ERR_ARG, "null argument");
+    *out = nullptr;
+    gs_graph* g = nullptr;
+    GS_TRY(new_graph(ctx, V, &g));
+    g->h_start.assign(start, start + std::min<uint64_t>(n_start, g->T_all + 1));
+    gs_status st = check_start(g, n_start, n_edges);
+    g->E = n_edges;
+    if (st == GS_OK) st = gs_stream_open(g, grid, segment_bytes);
     if (st == GS_OK) st = finish_upload(g, degree, false);
     if (st != GS_OK) {
         free_graph_arrays(g);
@@ -461,8 +487,10 @@ gs_status gs_graph_download(const gs_graph* g, uint64_t* host_start, uint32_t* h
     if (!g) return GS_ERR_ARG;
     gs_ctx* ctx = g->ctx;
     if (host_start) std::memcpy(host_start, g->h_start.data(), g->h_start.size() * 8);
-    if (host_grid && g->E)
-        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(host_grid, g->d_rec, g->E * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (host_grid && g->E) {
+        if (g->stream) std::memcpy(host_grid, gs_stream_records(g), g->E * 4);
+        else GS_CHECK_CUDA(ctx, cudaMemcpyAsync(host_grid, g->d_rec, g->E * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    }
     if (host_degree)
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(host_degree, g->d_degree, g->V * 4, cudaMemcpyDeviceToHost, ctx->stream));
     GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -507,6 +535,7 @@ gs_status gs_state_reset(gs_state* s, int64_t arg) {
     if (s->algo == GS_ALGO_PAGERANK && arg < 1) return gs_fail(g->ctx, GS_ERR_ARG, "iterations < 1");
     s->arg = arg;
     s->step = 0;
+    s->swept = false;
     s->done = false;
     s->last_count = 0;
     switch (s->algo) {
@@ -549,21 +578,55 @@ gs_status gs_pagerank_compat(gs_state* s, int enable) {
     return GS_OK;
 }
 
-gs_status gs_sweep(gs_state* s, const gs_segment* segs, int n_segs) {
-    if (!s) return GS_ERR_ARG;
-    if (segs || n_segs) return gs_fail(s->g->ctx, GS_ERR_UNSUPPORTED, "segment sweeps need a streamed graph");
-    if (s->done) return gs_fail(s->g->ctx, GS_ERR_STATE, "algorithm already finished");
+}  // extern "C"
+
+static gs_status sweep_launch(gs_state* s) {
     switch (s->algo) {
-        case GS_ALGO_BFS: return bfs_sweep(s);
-        case GS_ALGO_PAGERANK: return pr_sweep(s);
-        case GS_ALGO_WCC: return wcc_sweep(s);
-        case GS_ALGO_KCORE: return kcore_sweep(s);
+        case GS_ALGO_BFS: return bfs_sweep_launch(s);
+        case GS_ALGO_PAGERANK: return pr_sweep_launch(s);
+        case GS_ALGO_WCC: return wcc_sweep_launch(s);
+        case GS_ALGO_KCORE: return kcore_sweep_launch(s);
     }
     return GS_ERR_ARG;
 }
 
+extern "C" {
+
+gs_status gs_sweep(gs_state* s, const gs_segment* segs, int n_segs) {
+    if (!s) return GS_ERR_ARG;
+    gs_graph* g = s->g;
+    gs_ctx* ctx = g->ctx;
+    if (n_segs < 0 || (n_segs > 0 && !segs)) return gs_fail(ctx, GS_ERR_ARG, "bad segment list");
+    if (s->done) return gs_fail(ctx, GS_ERR_STATE, "algorithm already finished");
+    if (!s->swept) {
+        // once per sweep, however many segment calls make it up
+        if (s->algo == GS_ALGO_BFS) GS_TRY(bfs_sweep_begin(s));
+        if (s->algo == GS_ALGO_WCC) GS_TRY(wcc_sweep_begin(s));
+        s->swept = true;
+    }
+    auto launch = [s]() { return sweep_launch(s); };
+    if (n_segs > 0) return gs_each_part(g, segs, n_segs, launch);
+    gs_need need;
+    std::vector<uint8_t> act;
+    if (g->stream && (s->algo == GS_ALGO_BFS || s->algo == GS_ALGO_KCORE)) {
+        // the window flags the skip rule reads: BFS frontier windows
+        // (bfs.cpp:290-312), k-core windows of removed vertices
+        // (gstore.cpp:2773-2782)
+        act.resize(g->nw);
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(act.data(), s->d_act, g->nw, cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        need.act = act.data();
+        need.by_col = !g->directed;
+    }
+    return gs_each_segment(g, need, s->step & 1, launch);
+}
+
 gs_status gs_finalize(gs_state* s, int64_t* frontier_out, int* done_out) {
     if (!s) return GS_ERR_ARG;
+    if (s->swept) {
+        s->step += 1;
+        s->swept = false;
+    }
     int64_t f = 0;
     int d = 0;
     gs_status st = GS_ERR_ARG;

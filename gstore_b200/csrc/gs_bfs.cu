@@ -71,6 +71,7 @@ struct RunArgs {
     uint8_t* act_next;
     int directed;
     int* error;
+    const gs_seg_run* seg;   // segment sweep: entries to sweep (records at rec + delta), else null
 };
 
 __global__ void __launch_bounds__(kThreads) bfs_run_kernel(RunArgs a) {
@@ -86,14 +87,24 @@ __global__ void __launch_bounds__(kThreads) bfs_run_kernel(RunArgs a) {
     __syncthreads();
     uint32_t parity = 0;
 
-    for (uint64_t ri = blockIdx.x; ri < a.n_runs; ri += gridDim.x) {
-        const gs_tile_run run = a.runs[ri];
-        const uint32_t row = a.units[run.unit_beg].rc >> 16;
+    for (uint64_t i = blockIdx.x; i < a.n_runs; i += gridDim.x) {
+        uint32_t ub, ue;
+        const uint32_t* rec = a.rec;
+        if (a.seg) {
+            const gs_seg_run e = a.seg[i];
+            ub = e.unit_beg;
+            ue = e.unit_end;
+            rec = a.rec + e.delta;
+        } else {
+            ub = a.runs[i].unit_beg;
+            ue = a.runs[i].unit_end;
+        }
+        const uint32_t row = a.units[ub].rc >> 16;
         const bool ar = a.act[row] != 0;
         // the run is swept when its row window or any column window is active
         int any = ar ? 1 : 0;
         if (!ar && !a.directed)
-            for (uint32_t ui = run.unit_beg + tid; ui < run.unit_end; ui += kThreads)
+            for (uint32_t ui = ub + tid; ui < ue; ui += kThreads)
                 any |= a.act[a.units[ui].rc & 0xFFFFu] != 0;
         if (!__syncthreads_or(any)) continue;
 
@@ -115,7 +126,7 @@ __global__ void __launch_bounds__(kThreads) bfs_run_kernel(RunArgs a) {
             return;   // uniform; nothing else in flight
         }
         const uint32_t mr = ar ? 1u : 0u;
-        for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps) {
+        for (uint32_t ui = ub + warp; ui < ue; ui += kWarps) {
             const gs_unit d = a.units[ui];
             const uint32_t col = d.rc & 0xFFFFu;
             const uint32_t mc = (!a.directed && a.act[col]) ? 2u : 0u;
@@ -146,9 +157,9 @@ __global__ void __launch_bounds__(kThreads) bfs_run_kernel(RunArgs a) {
             if (ab > e) ab = e;
             uint64_t ae = e & ~3ull;
             if (ae < ab) ae = ab;
-            if (b + lane < ab) visit(__ldcs(a.rec + b + lane));
-            if (ae + lane < e) visit(__ldcs(a.rec + ae + lane));
-            const uint4* r4 = reinterpret_cast<const uint4*>(a.rec + ab);
+            if (b + lane < ab) visit(__ldcs(rec + b + lane));
+            if (ae + lane < e) visit(__ldcs(rec + ae + lane));
+            const uint4* r4 = reinterpret_cast<const uint4*>(rec + ab);
             const uint32_t n4 = (uint32_t)((ae - ab) >> 2);
             for (uint32_t k = lane; k < n4; k += 64) {
                 const uint4 q0 = __ldcs(r4 + k);
@@ -277,32 +288,36 @@ gs_status bfs_init(gs_state* s) {
     return GS_OK;
 }
 
-gs_status bfs_sweep(gs_state* s) {
+gs_status bfs_sweep_begin(gs_state* s) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
     // Window flags of this sweep, kept for the swept-record statistics.
     s->level_act.emplace_back(g->nw);
     GS_CHECK_CUDA(ctx, cudaMemcpyAsync(s->level_act.back().data(), s->d_act, g->nw, cudaMemcpyDeviceToHost,
                                        ctx->stream));
-    if (g->R == 0) {
-        s->step += 1;
-        return GS_OK;
-    }
     static bool attr_set[64] = {false};
     if (!attr_set[ctx->device & 63]) {
         GS_CHECK_CUDA(ctx, cudaFuncSetAttribute(bfs_run_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 (int)sizeof(BfsSmem)));
         attr_set[ctx->device & 63] = true;
     }
-    RunArgs a{g->d_runs, g->R, g->d_units, g->d_rec, s->d_front, s->d_visited, s->d_act, s->d_act_next,
-              g->directed, (int*)s->d_error};
-    const uint32_t grid = (uint32_t)std::min<uint64_t>(g->R, gs_grid_size(ctx, 6));
+    return GS_OK;
+}
+
+gs_status bfs_sweep_launch(gs_state* s) {
+    gs_graph* g = s->g;
+    gs_ctx* ctx = g->ctx;
+    // every run of the resident graph, or the entries of the current segment
+    const uint64_t n_runs = g->seg.list ? g->seg.n : g->R;
+    if (n_runs == 0) return GS_OK;
+    RunArgs a{g->d_runs, n_runs, g->d_units, g->seg.list ? g->seg.buf : g->d_rec, s->d_front, s->d_visited,
+              s->d_act, s->d_act_next, g->directed, (int*)s->d_error, g->seg.list};
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(n_runs, gs_grid_size(ctx, 6));
     gs_timer_begin(ctx);
     bfs_run_kernel<<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
     gs_timer_end(ctx, GS_ALGO_BFS, 0);
-    s->step += 1;
     return GS_OK;
 }
 
@@ -357,7 +372,7 @@ gs_status bfs_level_into(gs_ctx* ctx, const gs_graph* g, uint8_t* depth, uint32_
                                                     (int)sizeof(BfsSmem)));
             attr_set[ctx->device & 63] = true;
         }
-        RunArgs a{g->d_runs, g->R, g->d_units, g->d_rec, st, next, act, act_next, g->directed, error};
+        RunArgs a{g->d_runs, g->R, g->d_units, g->d_rec, st, next, act, act_next, g->directed, error, nullptr};
         const uint32_t grid = (uint32_t)std::min<uint64_t>(g->R, gs_grid_size(ctx, 6));
         bfs_run_kernel<<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
         GS_CHECK_CUDA(ctx, cudaGetLastError());

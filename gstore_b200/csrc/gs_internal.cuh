@@ -54,6 +54,27 @@ struct alignas(16) gs_unit {
     uint32_t rc;
 };
 
+// One entry of a segment sweep: units [unit_beg, unit_end) of run `run`,
+// whose records sit in the segment buffer at (file record index + delta).
+// delta is a multiple of 4, so 16-byte record alignment carries over.
+struct alignas(8) gs_seg_run {
+    uint32_t run;
+    uint32_t unit_beg;
+    uint32_t unit_end;
+    uint32_t pad;
+    int64_t delta;
+};
+
+// The segment a sweep currently works on (list == nullptr: every run of the
+// resident graph).
+struct SegView {
+    const gs_seg_run* list = nullptr;
+    uint32_t n = 0;
+    const uint32_t* buf = nullptr;
+};
+
+struct gs_streamer;   // pinned-host record stream of a graph (gs_stream.cu)
+
 struct KernelTimes {
     uint64_t launches = 0;
     double ms = 0.0;
@@ -95,6 +116,15 @@ struct gs_graph {
     uint64_t* d_tile_off = nullptr;   // T + 1 record offsets of non-empty tiles
     uint32_t* d_tile_rc = nullptr;    // T packed (row << 16 | col)
     int32_t* d_degree = nullptr;      // N
+    SegView seg;                      // set during segment sweeps
+    gs_streamer* stream = nullptr;    // non-null: records stay in host memory
+    gs_seg_run* d_list = nullptr;     // segment entry lists (device, pinned host)
+    gs_seg_run* h_list = nullptr;
+    uint64_t list_cap = 0;
+    cudaEvent_t ev_list = nullptr;    // last upload of h_list
+    bool list_pending = false;
+    std::vector<gs_tile_run> h_runs;  // host copies of the run and unit tables
+    std::vector<gs_unit> h_units;
     bool degree_from_records = false;
     std::vector<uint64_t> h_start;    // full .start copy (host), for planners
     std::vector<uint64_t> h_tile_off; // host copy of d_tile_off
@@ -105,7 +135,8 @@ struct gs_state {
     gs_graph* g = nullptr;
     gs_algo algo = GS_ALGO_BFS;
     int64_t arg = 0;
-    int step = 0;          // sweeps done
+    int step = 0;          // sweeps done (counted at finalize)
+    bool swept = false;    // a sweep happened since the last finalize
     bool done = false;
     bool compat = false;   // PageRank int32 inverse-degree truncation
     // BFS
@@ -172,21 +203,56 @@ void gs_dev_free(void* ptr);
 gs_status launch_validate_records(gs_graph* g, int* d_flag);
 gs_status launch_degree_from_records(gs_graph* g);
 
+// Per algorithm: init, sweep_begin (once per sweep, before its launches),
+// sweep_launch (once per segment in g->seg, or once over the resident
+// graph), finalize.
 gs_status bfs_init(gs_state* s);
-gs_status bfs_sweep(gs_state* s);
+gs_status bfs_sweep_begin(gs_state* s);
+gs_status bfs_sweep_launch(gs_state* s);
 gs_status bfs_finalize(gs_state* s, int64_t* frontier, int* done);
 
 gs_status pr_init(gs_state* s);
-gs_status pr_sweep(gs_state* s);
+gs_status pr_sweep_launch(gs_state* s);
 gs_status pr_finalize(gs_state* s, int64_t* frontier, int* done);
 
 gs_status wcc_init(gs_state* s);
-gs_status wcc_sweep(gs_state* s);
+gs_status wcc_sweep_begin(gs_state* s);
+gs_status wcc_sweep_launch(gs_state* s);
 gs_status wcc_finalize(gs_state* s, int64_t* frontier, int* done);
 
 gs_status kcore_init(gs_state* s);
-gs_status kcore_sweep(gs_state* s);
+gs_status kcore_sweep_launch(gs_state* s);
 gs_status kcore_finalize(gs_state* s, int64_t* frontier, int* done);
+
+// ------------------------------------------------------- segment sweeps --
+// Which units a planned sweep needs (the algorithms' tile-skip rules).
+struct gs_need {
+    const uint8_t* act = nullptr;   // host window flags; null = every unit
+    bool by_col = true;             // a unit is needed when its row or column window is active
+};
+// Calls `launch` once per segment with g->seg set: for a streamed graph the
+// segments are planned from `need` and their records copied from pinned host
+// memory on a side stream, overlapped with the launches; for a resident
+// graph `launch` runs once over every run.  direction != 0 walks the
+// segments last to first (a streamed graph then reuses the segment that
+// the previous sweep left in HBM).
+gs_status gs_each_segment_fn(gs_graph* g, const gs_need& need, int direction,
+                             gs_status (*fn)(void*), void* arg);
+template <class F>
+gs_status gs_each_segment(gs_graph* g, const gs_need& need, int direction, F launch) {
+    return gs_each_segment_fn(g, need, direction,
+                              [](void* a) -> gs_status { return (*static_cast<F*>(a))(); }, &launch);
+}
+// The same for the tiles of reference part ranges (gs_segment list).
+gs_status gs_each_part_fn(gs_graph* g, const gs_segment* segs, int n_segs, gs_status (*fn)(void*), void* arg);
+template <class F>
+gs_status gs_each_part(gs_graph* g, const gs_segment* segs, int n_segs, F launch) {
+    return gs_each_part_fn(g, segs, n_segs,
+                           [](void* a) -> gs_status { return (*static_cast<F*>(a))(); }, &launch);
+}
+gs_status gs_stream_open(gs_graph* g, const uint32_t* host_grid, uint64_t segment_bytes);
+void gs_stream_close(gs_graph* g);
+const uint32_t* gs_stream_records(const gs_graph* g);   // host records of a streamed graph
 
 gs_status gs_count_reached(gs_state* s, uint64_t* reached, uint64_t* edges_in_component);
 gs_status gs_count_kcore(gs_state* s, uint64_t* members);

@@ -57,6 +57,7 @@ extern "C" gs_status gs_bfs_noalloc(gs_graph* g, uint64_t root, uint8_t* d_depth
                        "gs_bfs_noalloc handles at most 16777216 vertices (its scratch array is fixed); "
                        "use gs_state_create/gs_run for larger graphs");
     if (root >= g->V) return gs_fail(ctx, GS_ERR_ARG, "BFS root out of range");
+    if (g->stream) return gs_fail(ctx, GS_ERR_UNSUPPORTED, "gs_bfs_noalloc needs a graph resident in HBM");
     if (ctx->device < 0 || ctx->device >= 256) return gs_fail(ctx, GS_ERR_ARG, "device ordinal out of range");
     GS_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
     unsigned char* base = nullptr;

@@ -26,64 +26,85 @@ __device__ __forceinline__ uint32_t bit_of(const uint32_t* __restrict__ bm, uint
 
 __device__ __forceinline__ uint4 load_stream(const uint4* p) { return __ldcs(p); }
 
-// Generic warp-per-item sweep.  Op provides:
-//   struct Item;                         per-item warp-uniform context
-//   bool begin(uint32_t row, uint32_t col, Item&)   false = skip the item
-//   void record(uint32_t rec, Item&)     one record, any lane
+// Generic run sweep.  A CTA takes one run at a time (consecutive tiles of one
+// tile row inside a group), its warps take the run's units (tile slices of at
+// most kUnitRecords records) and stream their records with 128-bit
+// evict-first loads.  When `seg` lists runs, only those are swept and their
+// units are read from a segment buffer (file record r at rec[r + delta]).
+// Op provides:
+//   struct Item;                                    per-unit warp-uniform context
+//   bool begin(uint32_t row, uint32_t col, Item&)   false = skip the unit
+//   void record(uint32_t rec, Item&)                one record, any lane
 //   void end(uint32_t row, uint32_t col, Item&)     warp-collective epilogue
 template <class Op>
-__global__ void __launch_bounds__(kThreads) sweep_items(const gs_item* __restrict__ items,
-                                                        uint64_t n_items,
-                                                        const uint32_t* __restrict__ rec, Op op) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t w = warp; w < n_items; w += nwarps) {
-        const gs_item it = items[w];
-        const uint32_t row = it.rc >> 16, col = it.rc & 0xFFFFu;
-        typename Op::Item ic;
-        if (!op.begin(row, col, ic)) continue;
-        const uint64_t b = it.beg, e = it.beg + it.cnt;
-        uint64_t ab = (b + 3) & ~3ull;
-        if (ab > e) ab = e;
-        uint64_t ae = e & ~3ull;
-        if (ae < ab) ae = ab;
-        if (b + lane < ab) op.record(__ldcs(rec + b + lane), ic);
-        const uint4* r4 = reinterpret_cast<const uint4*>(rec + ab);
-        const uint32_t n4 = (uint32_t)((ae - ab) >> 2);
-        for (uint32_t k = lane; k < n4; k += 4 * 32) {
-            uint4 q[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const uint32_t kk = k + u * 32;
-                if (kk < n4) q[u] = load_stream(r4 + kk);
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (k + u * 32 < n4) {
-                    op.record(q[u].x, ic);
-                    op.record(q[u].y, ic);
-                    op.record(q[u].z, ic);
-                    op.record(q[u].w, ic);
+__global__ void __launch_bounds__(kThreads) sweep_runs(const gs_tile_run* __restrict__ runs, uint64_t n_runs,
+                                                       const gs_unit* __restrict__ units,
+                                                       const uint32_t* __restrict__ rec,
+                                                       const gs_seg_run* __restrict__ seg, Op op) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr uint32_t kWarps = kThreads / 32;
+    for (uint64_t i = blockIdx.x; i < n_runs; i += gridDim.x) {
+        uint32_t ub, ue;
+        const uint32_t* base = rec;
+        if (seg) {
+            const gs_seg_run e = seg[i];
+            ub = e.unit_beg;
+            ue = e.unit_end;
+            base = rec + e.delta;
+        } else {
+            ub = runs[i].unit_beg;
+            ue = runs[i].unit_end;
+        }
+        for (uint32_t ui = ub + warp; ui < ue; ui += kWarps) {
+            const gs_unit d = units[ui];
+            const uint32_t row = d.rc >> 16, col = d.rc & 0xFFFFu;
+            typename Op::Item ic;
+            if (!op.begin(row, col, ic)) continue;
+            const uint64_t b = d.rec_beg, e = d.rec_beg + d.n;
+            uint64_t ab = (b + 3) & ~3ull;
+            if (ab > e) ab = e;
+            uint64_t ae = e & ~3ull;
+            if (ae < ab) ae = ab;
+            if (b + lane < ab) op.record(__ldcs(base + b + lane), ic);
+            if (ae + lane < e) op.record(__ldcs(base + ae + lane), ic);
+            const uint4* r4 = reinterpret_cast<const uint4*>(base + ab);
+            const uint32_t n4 = (uint32_t)((ae - ab) >> 2);
+            for (uint32_t k = lane; k < n4; k += 2 * 32) {
+                const uint4 q0 = load_stream(r4 + k);
+                const bool two = k + 32 < n4;
+                uint4 q1 = make_uint4(0, 0, 0, 0);
+                if (two) q1 = load_stream(r4 + k + 32);
+                op.record(q0.x, ic);
+                op.record(q0.y, ic);
+                op.record(q0.z, ic);
+                op.record(q0.w, ic);
+                if (two) {
+                    op.record(q1.x, ic);
+                    op.record(q1.y, ic);
+                    op.record(q1.z, ic);
+                    op.record(q1.w, ic);
                 }
             }
+            op.end(row, col, ic);
         }
-        if (ae + lane < e) op.record(__ldcs(rec + ae + lane), ic);
-        op.end(row, col, ic);
     }
 }
 
+// Sweeps the whole resident graph, or, during a streamed sweep, the runs of
+// the segment the graph points at.
 template <class Op>
 gs_status launch_sweep(gs_graph* g, const Op& op, int algo, uint64_t bytes) {
     gs_ctx* ctx = g->ctx;
-    if (g->I == 0) return GS_OK;
-    uint64_t want = (g->I + (kThreads / 32) - 1) / (kThreads / 32);
-    uint32_t grid = (uint32_t)std::min<uint64_t>(want, gs_grid_size(ctx, 8));
+    const gs_seg_run* seg = g->seg.list;
+    const uint64_t n = seg ? g->seg.n : g->R;
+    const uint32_t* rec = seg ? g->seg.buf : g->d_rec;
+    if (n == 0) return GS_OK;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(n, gs_grid_size(ctx, 8));
     gs_timer_begin(ctx);
-    sweep_items<Op><<<grid, kThreads, 0, ctx->stream>>>(g->d_items, g->I, g->d_rec, op);
+    sweep_runs<Op><<<grid, kThreads, 0, ctx->stream>>>(g->d_runs, n, g->d_units, rec, seg, op);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
-    gs_timer_end(ctx, algo, bytes);
+    gs_timer_end(ctx, algo, seg ? 0 : bytes);
     return GS_OK;
 }
 
@@ -99,23 +120,24 @@ __device__ __forceinline__ void warp_add_u64(unsigned long long* dst, uint64_t v
 }
 
 // ---------------------------------------------------------- validation --
-__global__ void validate_records_kernel(const gs_item* __restrict__ items, uint64_t n_items,
-                                        const uint32_t* __restrict__ rec, uint32_t last_window,
-                                        uint64_t V, int* flag) {
-    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = tid; i < n_items; i += nth) {
-        const gs_item it = items[i];
-        const uint32_t row = it.rc >> 16, col = it.rc & 0xFFFFu;
-        if (row != last_window && col != last_window) continue;
-        for (uint64_t e = it.beg; e < it.beg + it.cnt; ++e) {
-            const uint32_t r = rec[e];
-            const uint64_t a = ((uint64_t)row << 16) + (r & 0xFFFFu);
-            const uint64_t b = ((uint64_t)col << 16) + (r >> 16);
-            if (a >= V || b >= V) *flag = 1;
-        }
+// Flags a record of the last (ragged) window that addresses a vertex >= V.
+struct ValidateOp {
+    uint32_t last_window;
+    uint64_t V;
+    int* flag;
+    struct Item {
+        uint64_t rb, cb;
+    };
+    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
+        c.rb = (uint64_t)row << 16;
+        c.cb = (uint64_t)col << 16;
+        return row == last_window || col == last_window;
     }
-}
+    __device__ void record(uint32_t r, Item& c) const {
+        if (c.rb + (r & 0xFFFFu) >= V || c.cb + (r >> 16) >= V) *flag = 1;
+    }
+    __device__ void end(uint32_t, uint32_t, Item&) const {}
+};
 
 struct DegreeOp {
     int32_t* deg;
@@ -360,18 +382,13 @@ gs_status zero_scalar(gs_ctx* ctx) {
 
 // ================================================================ launchers ==
 gs_status launch_validate_records(gs_graph* g, int* d_flag) {
-    gs_ctx* ctx = g->ctx;
-    if (g->I == 0) return GS_OK;
-    validate_records_kernel<<<blocks_for(g->I, ctx), kThreads, 0, ctx->stream>>>(
-        g->d_items, g->I, g->d_rec, g->nw - 1, g->V, d_flag);
-    GS_CHECK_CUDA(ctx, cudaGetLastError());
-    ctx->launches++;
-    return GS_OK;
+    ValidateOp op{g->nw - 1, g->V, d_flag};
+    return gs_each_segment(g, gs_need{}, 0, [&]() { return launch_sweep(g, op, 0, 0); });
 }
 
 gs_status launch_degree_from_records(gs_graph* g) {
     DegreeOp op{g->d_degree, g->directed};
-    return launch_sweep(g, op, 0, 0);
+    return gs_each_segment(g, gs_need{}, 0, [&]() { return launch_sweep(g, op, 0, 0); });
 }
 
 // ------------------------------------------------------------------- BFS ----
@@ -386,7 +403,7 @@ gs_status gs_count_reached(gs_state* s, uint64_t* reached, uint64_t* edges_in_co
     GS_TRY(read_scalar(ctx, reached));
     GS_TRY(zero_scalar(ctx));
     ComponentEdgesOp op{s->d_depth, (unsigned long long*)ctx->d_scalars};
-    GS_TRY(launch_sweep(g, op, 0, 0));
+    GS_TRY(gs_each_segment(g, gs_need{}, 0, [&]() { return launch_sweep(g, op, 0, 0); }));
     GS_TRY(read_scalar(ctx, edges_in_component));
     return GS_OK;
 }
@@ -417,13 +434,11 @@ gs_status pr_init(gs_state* s) {
     return GS_OK;
 }
 
-gs_status pr_sweep(gs_state* s) {
+gs_status pr_sweep_launch(gs_state* s) {
     gs_graph* g = s->g;
     PrOp op{s->d_x, s->d_y, g->directed};
     // algorithmic bytes per iteration: 4E + 12V (records, x, s, inv)
-    GS_TRY(launch_sweep(g, op, GS_ALGO_PAGERANK, 4 * g->E + 12 * g->V));
-    s->step += 1;
-    return GS_OK;
+    return launch_sweep(g, op, GS_ALGO_PAGERANK, 4 * g->E + 12 * g->V);
 }
 
 gs_status pr_finalize(gs_state* s, int64_t* frontier, int* done) {
@@ -452,14 +467,13 @@ gs_status wcc_init(gs_state* s) {
     return GS_OK;
 }
 
-gs_status wcc_sweep(gs_state* s) {
+gs_status wcc_sweep_begin(gs_state* s) { return zero_scalar(s->g->ctx); }
+
+gs_status wcc_sweep_launch(gs_state* s) {
     gs_graph* g = s->g;
-    GS_TRY(zero_scalar(g->ctx));
     WccOp op{s->d_parent, s->step == 0 ? s->d_touched : nullptr,
              (unsigned long long*)g->ctx->d_scalars};
-    GS_TRY(launch_sweep(g, op, GS_ALGO_WCC, 4 * g->E + 8 * g->V));
-    s->step += 1;
-    return GS_OK;
+    return launch_sweep(g, op, GS_ALGO_WCC, 4 * g->E + 8 * g->V);
 }
 
 gs_status wcc_finalize(gs_state* s, int64_t* frontier, int* done) {
@@ -499,12 +513,10 @@ gs_status kcore_init(gs_state* s) {
     return GS_OK;
 }
 
-gs_status kcore_sweep(gs_state* s) {
+gs_status kcore_sweep_launch(gs_state* s) {
     gs_graph* g = s->g;
     KcoreOp op{s->d_deg, s->d_kactive, s->d_act};
-    GS_TRY(launch_sweep(g, op, GS_ALGO_KCORE, 0));
-    s->step += 1;
-    return GS_OK;
+    return launch_sweep(g, op, GS_ALGO_KCORE, 0);
 }
 
 gs_status kcore_finalize(gs_state* s, int64_t* frontier, int* done) {

@@ -235,10 +235,15 @@ int main(int argc, char* argv[]) {
     tile_files tf;
     int rc = read_graph_files(o, want_degree, &tf);
     if (rc) return rc;
+    // Jobs 0-3 are the reference's semi-external jobs (budget -m, two IO
+    // segments, gstore.cpp:3044-3119): a grid above the budget streams from
+    // host memory through two HBM segments.  The mmap and in-memory jobs
+    // (1x, 2x) keep the grid resident.
+    const uint64_t budget = job < 10 ? o.total_size : 0;
     gs_ctx* ctx = nullptr;
-    if (gs_create(&ctx, 0, 0, kDirected) != GS_OK) return fail(nullptr, "no usable CUDA device");
+    if (gs_create(&ctx, 0, budget, kDirected) != GS_OK) return fail(nullptr, "no usable CUDA device");
     gs_graph* g = nullptr;
-    rc = upload_graph(ctx, o, tf, want_degree, &g);
+    rc = upload_graph(ctx, o, tf, want_degree, &g);   // tf outlives g: a streamed grid stays valid
     if (rc == 0) {
         if (exclude_load) start = mywtime();
         const char* label = "";

@@ -100,6 +100,26 @@ gs_status gs_geometry(uint64_t V, int directed, uint32_t* p, uint32_t* p_s,
 gs_status gs_upload_graph(gs_ctx* ctx, const uint64_t* start, uint64_t n_start,
                           const uint32_t* grid, uint64_t n_edges,
                           const int32_t* degree, uint64_t V, gs_graph** out);
+/* When the context's HBM budget is set and the grid is larger, the graph is
+ * streamed (gs_upload_graph_streamed with segment_bytes = budget / 2), and
+ * grid must then stay valid and unchanged until gs_graph_free. */
+
+/* Replaces: the semi-external mode of the reference (-m budget: two IO
+ * segments refilled by libaio, read_aio_init / fetch_mem_part,
+ * gstore.cpp:3044-3119, 3867-3918).  The records stay in host memory (grid
+ * is pinned with cudaHostRegister unless it already is; it must stay valid
+ * and unchanged until gs_graph_free); every sweep plans the tile runs its
+ * skip rule needs and copies them through two HBM buffers of segment_bytes
+ * each on a side stream, overlapped with the sweep kernels.  segment_bytes
+ * >= 1 MiB + 64 bytes. */
+gs_status gs_upload_graph_streamed(gs_ctx* ctx, const uint64_t* start, uint64_t n_start,
+                                   const uint32_t* grid, uint64_t n_edges, const int32_t* degree,
+                                   uint64_t V, uint64_t segment_bytes, gs_graph** out);
+/* Host-to-device traffic of a streamed graph since upload: bytes copied,
+ * cudaMemcpyAsync calls, segments swept, segments found already in HBM
+ * (all 0 for a resident graph). */
+gs_status gs_stream_stats(const gs_graph* g, uint64_t* bytes_copied, uint64_t* copies,
+                          uint64_t* segments, uint64_t* segments_reused);
 /* The same from device pointers (e.g. produced by gs_convert_device); the
  * library copies them, the caller keeps ownership. */
 gs_status gs_upload_graph_device(gs_ctx* ctx, const uint64_t* d_start, uint64_t n_start,
@@ -122,8 +142,11 @@ gs_status gs_state_free(gs_state* s);
  * reallocating its device arrays. */
 gs_status gs_state_reset(gs_state* s, int64_t arg);
 /* Replaces: algo_t::algo_mem_part(segment*) (algo.h:40): sweeps the tiles of
- * the given runs (segs, n_segs), or every resident tile when segs == NULL,
- * applying the algorithm's own tile-skip rule. */
+ * the given part ranges (segs, n_segs), or every tile when n_segs == 0,
+ * applying the algorithm's own tile-skip rule.  As in the reference, one
+ * level or iteration may be swept by several calls (one per segment); the
+ * next gs_finalize closes it.  With n_segs == 0 a streamed graph plans its
+ * own segments from the skip rule and streams them. */
 gs_status gs_sweep(gs_state* s, const gs_segment* segs, int n_segs);
 /* Replaces: iteration_finalize() (bfs.cpp:187-224, pr.cpp:229-303,
  * kcore.cpp:179-217, wcc.cpp:281-395).  frontier_out: BFS vertices found in

@@ -1,0 +1,198 @@
+"""Segment sweeps on the GPU: the streamed (semi-external) graph and sweeps
+over reference part ranges.
+
+A streamed graph keeps its records in host memory and copies the tile runs
+each sweep needs through two HBM segment buffers (the reference's -m mode,
+fetch_mem_part + libaio double buffering, gstore.cpp:3867-3918).  Every
+result must equal the resident graph's bit for bit (BFS depth, WCC labels,
+k-core degrees) or, for PageRank, be within PR_TOL relative L1 of the FP64
+oracle, whatever the segment size.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+PR_TOL = 1e-6   # relative L1, sum|gpu - fp64| / sum|fp64|
+MIN_SEG = 2 * (131072 + 8) * 4   # smallest segment the library takes
+
+
+def rel_l1(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def gs():
+    import gstore_b200
+
+    return gstore_b200
+
+
+@pytest.fixture(scope="module")
+def kron20(gpu_ctx_factory):
+    ctx = gpu_ctx_factory(False)
+    V = 1 << 20
+    graph = ctx.convert(ctx.kron_generate(20, 16), V)
+    start, grid, degree = graph.download()
+    return dict(V=V, graph=graph, start=start, grid=grid, degree=degree)
+
+
+def _roots(degree, n, seed):
+    nz = np.nonzero(degree)[0]
+    rng = np.random.default_rng(seed)
+    return [int(r) for r in rng.choice(nz, n, replace=False)]
+
+
+@pytest.mark.parametrize("seg_bytes", [MIN_SEG, 4 << 20])
+def test_streamed_kron20_matches_resident(seg_bytes, kron20, gpu_ctx_factory, oracle_lib):
+    k = kron20
+    ctx = gpu_ctx_factory(False)
+    sg = ctx.upload_streamed(k["start"], k["grid"], k["degree"], k["V"], seg_bytes)
+    res = k["graph"]
+    for root in [1, *_roots(k["degree"], 2, 11)]:
+        with sg.state("bfs", root) as s:
+            s.run()
+            depth = s.download()
+            st = s.bfs_stats()
+        with res.state("bfs", root) as s:
+            s.run()
+            want = s.download()
+            st_r = s.bfs_stats()
+        assert np.array_equal(depth, want), f"root {root}"
+        assert st["level_counts"].tolist() == st_r["level_counts"].tolist()
+        assert st["edges_in_component"] == st_r["edges_in_component"]
+    lab, n = sg.wcc()
+    lab_r, n_r = res.wcc()
+    assert np.array_equal(lab, lab_r) and n == n_r
+    for kk in (4, 8, 32):
+        deg, mem = sg.kcore(kk)
+        deg_r, mem_r = res.kcore(kk)
+        assert np.array_equal(deg, deg_r) and mem == mem_r, f"k={kk}"
+    p, _, _ = oracle_lib.geometry(k["V"])
+    r64, x64 = oracle_lib.pagerank(k["start"], k["grid"], k["degree"], p, False, k["V"], 5)
+    r, x = sg.pagerank(5)
+    assert rel_l1(r, r64) <= PR_TOL and rel_l1(x, x64) <= PR_TOL
+    stats = sg.stream_stats()
+    assert stats["segments"] > 0 and stats["bytes"] > 0
+    sg.free()
+
+
+def test_streamed_traffic_and_reuse(kron20, gpu_ctx_factory):
+    """A PageRank iteration copies every record once, less the segment the
+    previous iteration left in HBM; a BFS level copies only the runs its
+    skip rule needs."""
+    k = kron20
+    ctx = gpu_ctx_factory(False)
+    seg = 8 << 20
+    sg = ctx.upload_streamed(k["start"], k["grid"], k["degree"], k["V"], seg)
+    grid_bytes = k["grid"].size * 4
+    before = sg.stream_stats()
+    sg.pagerank(4)
+    after = sg.stream_stats()
+    copied = after["bytes"] - before["bytes"]
+    n_seg_iter = (after["segments"] - before["segments"]) // 4
+    assert n_seg_iter >= grid_bytes // seg
+    assert after["reused"] - before["reused"] >= 3           # iterations 2..4 start in HBM
+    assert grid_bytes * 4 - 3 * seg - 64 <= copied <= grid_bytes * 4 + 64 * n_seg_iter * 4
+    before = sg.stream_stats()
+    with sg.state("bfs", 1) as s:
+        s.run()
+        swept = int(s.bfs_stats()["swept"].sum())
+    copied = sg.stream_stats()["bytes"] - before["bytes"]
+    # every swept record was copied, plus small gaps and alignment
+    assert copied >= swept * 4
+    sg.free()
+
+
+@pytest.mark.parametrize("name", ["spread18", "spread18d", "handmade", "handmade_d"])
+def test_streamed_golden(name, gpu_ctx_factory):
+    g = load_golden(name)
+    ctx = gpu_ctx_factory(g["directed"])
+    sg = ctx.upload_streamed(g["start"], g["grid"], g["degree"], g["V"], MIN_SEG)
+    for r, root in enumerate(g["bfs_roots"]):
+        assert np.array_equal(sg.bfs(int(root)), g["bfs_depth"][r]), f"root {root}"
+    labels, count = sg.wcc()
+    assert np.array_equal(labels, g["wcc_label"]) and count == int(g["wcc_count"])
+    if not g["directed"]:
+        for i, kk in enumerate(g["kcore_k"]):
+            assert np.array_equal(sg.kcore(int(kk))[0], g["kcore_deg"][i])
+    sg.free()
+
+
+def test_budget_upload_streams(kron20, gs):
+    """A context whose HBM tile budget is below the grid streams it."""
+    k = kron20
+    ctx = gs.Context(0, hbm_budget=16 << 20)
+    try:
+        g = ctx.upload(k["start"], k["grid"], k["degree"], k["V"])
+        assert np.array_equal(g.bfs(1), k["graph"].bfs(1))
+        assert g.stream_stats()["segments"] > 0
+        g.free()
+    finally:
+        ctx.close()
+
+
+def test_streamed_degree_and_validation(kron20, gs, gpu_ctx_factory):
+    k = kron20
+    ctx = gpu_ctx_factory(False)
+    sg = ctx.upload_streamed(k["start"], k["grid"], None, k["V"], MIN_SEG)
+    assert np.array_equal(sg.degree(), k["degree"])
+    start, grid, degree = sg.download()
+    assert np.array_equal(grid, k["grid"]) and np.array_equal(start, k["start"])
+    sg.free()
+    h = load_golden("handmade")
+    with pytest.raises(gs.GStoreError, match="GS_ERR_FORMAT"):
+        ctx.upload_streamed(h["start"], h["grid"], h["degree"], h["V"] - 1, MIN_SEG)
+    with pytest.raises(gs.GStoreError, match="GS_ERR_ARG"):
+        ctx.upload_streamed(k["start"], k["grid"], k["degree"], k["V"], MIN_SEG - 16)
+    sg = ctx.upload_streamed(h["start"], h["grid"], h["degree"], h["V"], MIN_SEG)
+    out = np.zeros(1, np.uint8)
+    with pytest.raises(gs.GStoreError, match="GS_ERR_UNSUPPORTED"):
+        sg.bfs_noalloc(0, out.ctypes.data)
+    sg.free()
+
+
+def _thirds(gs):
+    """Three part ranges covering the one diagonal group of a p = 1 grid."""
+    P = lambda i, j: gs.part_id(0, 0, i, j, 1)   # noqa: E731
+    return [[(P(0, 0), P(84, 255))], [(P(85, 85), P(170, 255))], [(P(171, 171), P(255, 255))]]
+
+
+@pytest.mark.parametrize("streamed", [False, True])
+def test_part_sweeps_match_run(streamed, kron20, gs, gpu_ctx_factory):
+    """algo_mem_part called once per segment (three part ranges), then
+    iteration_finalize, equals the whole-grid run."""
+    k = kron20
+    ctx = gpu_ctx_factory(False)
+    g = (ctx.upload_streamed(k["start"], k["grid"], k["degree"], k["V"], 4 << 20) if streamed
+         else k["graph"])
+    parts = _thirds(gs)
+
+    def drive(state, first_finalize=False):
+        if first_finalize:
+            f, done = state.finalize()
+        else:
+            done = False
+        while not done:
+            for pr in parts:
+                state.sweep(pr)
+            f, done = state.finalize()
+
+    with g.state("bfs", 1) as s:
+        drive(s)
+        assert np.array_equal(s.download(), k["graph"].bfs(1))
+    with g.state("wcc") as s:
+        drive(s)
+        assert np.array_equal(s.download(), k["graph"].wcc()[0])
+    with g.state("kcore", 8) as s:
+        drive(s, first_finalize=True)
+        assert np.array_equal(s.download(), k["graph"].kcore(8)[0])
+    with g.state("bfs", 5) as s:          # a part range that is not a tile is an error
+        with pytest.raises(gs.GStoreError, match="GS_ERR_ARG"):
+            s.sweep([(gs.part_id(0, 0, 9, 3, 1), gs.part_id(0, 0, 9, 9, 1))])
+    if streamed:
+        g.free()
