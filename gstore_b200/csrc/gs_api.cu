@@ -166,13 +166,76 @@ static void free_graph_arrays(gs_graph* g) {
     gs_dev_free(g->d_degree);
     gs_dev_free(g->d_runs);
     gs_dev_free(g->d_units);
+    gs_dev_free(g->d_runs_blk);
+    gs_dev_free(g->d_units_blk);
     g->d_runs = nullptr;
     g->d_units = nullptr;
+    g->d_runs_blk = nullptr;
+    g->d_units_blk = nullptr;
     g->d_rec = nullptr;
     g->d_items = nullptr;
     g->d_tile_off = nullptr;
     g->d_tile_rc = nullptr;
     g->d_degree = nullptr;
+}
+
+// The L2-blocked sweep order: tiles grouped into blocks of kBlockWindows x
+// kBlockWindows windows (row-major inside a block), so the vertex state the
+// tiles in flight touch (2 kBlockWindows windows) stays in L2.  Runs are
+// short (one tile row, <= kBlockRunUnits units, one per warp of a CTA) so
+// the CTAs in flight work inside one or two blocks.  Used by the sweeps whose per-record state is large (PageRank,
+// WCC, k-core); their results do not depend on the order.
+static gs_status build_blocked_order(gs_graph* g) {
+    gs_ctx* ctx = g->ctx;
+    const uint64_t T = g->T;
+    std::vector<uint32_t> tile_unit(T + 1, 0);
+    {
+        uint64_t k = 0;
+        for (uint32_t u = 0; u < g->U; ++u) {
+            while (g->h_tile_off[k + 1] <= g->h_units[u].rec_beg) tile_unit[++k] = u;
+        }
+        while (k < T) tile_unit[++k] = (uint32_t)g->U;
+    }
+    std::vector<uint32_t> order(T);
+    for (uint32_t k = 0; k < T; ++k) order[k] = k;
+    auto block_of = [&](uint32_t k) {
+        const uint32_t rc = g->h_tile_rc[k];
+        return ((uint64_t)((rc >> 16) / kBlockWindows) << 32) | ((rc & 0xFFFFu) / kBlockWindows);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return block_of(a) < block_of(b); });
+    std::vector<gs_unit> units;
+    std::vector<gs_tile_run> runs;
+    units.reserve(g->U);
+    uint64_t open_block = ~0ull;
+    uint32_t open_row = ~0u;
+    bool is_open = false;
+    for (uint32_t k : order) {
+        const uint32_t row = g->h_tile_rc[k] >> 16;
+        const uint64_t blk = block_of(k);
+        for (uint32_t u = tile_unit[k]; u < tile_unit[k + 1]; ++u) {
+            const gs_unit& d = g->h_units[u];
+            if (!is_open || row != open_row || blk != open_block || runs.back().unit_end - runs.back().unit_beg >= kBlockRunUnits) {
+                runs.push_back(gs_tile_run{d.rec_beg, d.rec_beg, 0, 0, (uint32_t)units.size(), (uint32_t)units.size()});
+                open_row = row;
+                open_block = blk;
+                is_open = true;
+            }
+            units.push_back(d);
+            runs.back().rec_end = d.rec_beg + d.n;
+            runs.back().unit_end = (uint32_t)units.size();
+        }
+    }
+    g->R_blk = runs.size();
+    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_units_blk, std::max<size_t>(1, units.size()) * sizeof(gs_unit)));
+    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_runs_blk, std::max<size_t>(1, runs.size()) * sizeof(gs_tile_run)));
+    if (!units.empty())
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_units_blk, units.data(), units.size() * sizeof(gs_unit),
+                                           cudaMemcpyHostToDevice, ctx->stream));
+    if (!runs.empty())
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_runs_blk, runs.data(), runs.size() * sizeof(gs_tile_run),
+                                           cudaMemcpyHostToDevice, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return GS_OK;
 }
 
 // Builds the non-empty tile table and the work items from the host .start
@@ -249,6 +312,7 @@ static gs_status build_tables(gs_graph* g) {
     g->I = n_items;
     g->R = runs.size();
     g->U = units.size();
+    if (!g->stream) GS_TRY(build_blocked_order(g));
     GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_units, std::max<size_t>(1, units.size()) * sizeof(gs_unit)));
     if (!units.empty())
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_units, units.data(), units.size() * sizeof(gs_unit),

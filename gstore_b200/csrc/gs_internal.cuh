@@ -45,6 +45,10 @@ struct alignas(8) gs_tile_run {
 
 // Records per BFS unit.
 constexpr uint32_t kUnitRecords = 2048;
+// Side of a block of the L2-blocked sweep order, in windows.
+constexpr uint32_t kBlockWindows = 64;
+// Units per run of the L2-blocked order.
+constexpr uint32_t kBlockRunUnits = 8;
 
 // One unit: records [rec_beg, rec_beg + n) of the tile at row rc >> 16,
 // column rc & 0xFFFF (n <= kUnitRecords; units follow the file order).
@@ -74,6 +78,7 @@ struct SegView {
 };
 
 struct gs_streamer;   // pinned-host record stream of a graph (gs_stream.cu)
+struct gs_seglists;   // double-buffered entry lists of segment sweeps (gs_stream.cu)
 
 struct KernelTimes {
     uint64_t launches = 0;
@@ -113,16 +118,15 @@ struct gs_graph {
     gs_item* d_items = nullptr;
     gs_tile_run* d_runs = nullptr;
     gs_unit* d_units = nullptr;
+    uint64_t R_blk = 0;               // runs of the L2-blocked order (resident graphs)
+    gs_tile_run* d_runs_blk = nullptr;
+    gs_unit* d_units_blk = nullptr;
     uint64_t* d_tile_off = nullptr;   // T + 1 record offsets of non-empty tiles
     uint32_t* d_tile_rc = nullptr;    // T packed (row << 16 | col)
     int32_t* d_degree = nullptr;      // N
     SegView seg;                      // set during segment sweeps
     gs_streamer* stream = nullptr;    // non-null: records stay in host memory
-    gs_seg_run* d_list = nullptr;     // segment entry lists (device, pinned host)
-    gs_seg_run* h_list = nullptr;
-    uint64_t list_cap = 0;
-    cudaEvent_t ev_list = nullptr;    // last upload of h_list
-    bool list_pending = false;
+    gs_seglists* lists = nullptr;     // segment entry lists of segment sweeps
     std::vector<gs_tile_run> h_runs;  // host copies of the run and unit tables
     std::vector<gs_unit> h_units;
     bool degree_from_records = false;

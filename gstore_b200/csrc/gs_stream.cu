@@ -60,32 +60,82 @@ struct gs_streamer {
     cudaEvent_t ready[2] = {nullptr, nullptr};   // copies into the buffer done
     cudaEvent_t freed[2] = {nullptr, nullptr};   // last sweep reading the buffer done
     cudaStream_t copy = nullptr;
-    cudaEvent_t ev_start = nullptr;
     int last = 1;                  // buffer of the last segment swept
     uint64_t bytes = 0, copies = 0, segments = 0, reused = 0;
 };
 
+// Entry lists of consecutive segment sweeps alternate between two slots, so
+// the list of the next sweep uploads while the current one still runs.
+struct gs_seglists {
+    gs_seg_run* d[2] = {nullptr, nullptr};
+    gs_seg_run* h[2] = {nullptr, nullptr};      // pinned
+    uint64_t cap = 0;
+    cudaEvent_t uploaded[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};    // last sweep reading the slot
+    bool upload_pending[2] = {false, false};
+    bool done_recorded[2] = {false, false};
+    int slot = 0;
+};
+
 namespace {
 
-gs_status ensure_list(gs_graph* g, uint64_t n) {
-    gs_ctx* ctx = g->ctx;
-    if (!g->ev_list) GS_CHECK_CUDA(ctx, cudaEventCreateWithFlags(&g->ev_list, cudaEventDisableTiming));
-    if (g->list_pending) {
-        GS_CHECK_CUDA(ctx, cudaEventSynchronize(g->ev_list));
-        g->list_pending = false;
+void free_lists(gs_seglists* L) {
+    for (int k = 0; k < 2; ++k) {
+        gs_dev_free(L->d[k]);
+        if (L->h[k]) cudaFreeHost(L->h[k]);
+        L->d[k] = nullptr;
+        L->h[k] = nullptr;
     }
-    if (n <= g->list_cap) return GS_OK;
-    // the device list may still be read by queued sweeps
-    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    gs_dev_free(g->d_list);
-    if (g->h_list) cudaFreeHost(g->h_list);
-    g->d_list = nullptr;
-    g->h_list = nullptr;
-    g->list_cap = 0;
-    const uint64_t cap = std::max<uint64_t>(n, 1024);
-    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_list, cap * sizeof(gs_seg_run)));
-    GS_CHECK_CUDA(ctx, cudaHostAlloc((void**)&g->h_list, cap * sizeof(gs_seg_run), cudaHostAllocDefault));
-    g->list_cap = cap;
+    L->cap = 0;
+}
+
+// Uploads the entries of the next sweep on `stream` into the next slot and
+// makes the compute stream wait for them; returns the slot.
+gs_status upload_list(gs_graph* g, const std::vector<gs_seg_run>& ent, cudaStream_t stream, int* slot_out) {
+    gs_ctx* ctx = g->ctx;
+    if (!g->lists) {
+        g->lists = new (std::nothrow) gs_seglists();
+        if (!g->lists) return GS_ERR_OOM;
+        for (int k = 0; k < 2; ++k) {
+            GS_CHECK_CUDA(ctx, cudaEventCreateWithFlags(&g->lists->uploaded[k], cudaEventDisableTiming));
+            GS_CHECK_CUDA(ctx, cudaEventCreateWithFlags(&g->lists->done[k], cudaEventDisableTiming));
+        }
+    }
+    gs_seglists* L = g->lists;
+    if (ent.size() > L->cap) {
+        // queued sweeps may still read the old lists
+        GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        if (g->stream) GS_CHECK_CUDA(ctx, cudaStreamSynchronize(g->stream->copy));
+        free_lists(L);
+        const uint64_t cap = std::max<uint64_t>(ent.size(), 1024);
+        for (int k = 0; k < 2; ++k) {
+            GS_TRY(gs_dev_alloc(ctx, (void**)&L->d[k], cap * sizeof(gs_seg_run)));
+            GS_CHECK_CUDA(ctx, cudaHostAlloc((void**)&L->h[k], cap * sizeof(gs_seg_run), cudaHostAllocDefault));
+        }
+        L->cap = cap;
+        L->upload_pending[0] = L->upload_pending[1] = false;
+    }
+    const int k = L->slot;
+    L->slot ^= 1;
+    if (L->upload_pending[k]) {      // the host slot is free once its last upload finished
+        GS_CHECK_CUDA(ctx, cudaEventSynchronize(L->uploaded[k]));
+        L->upload_pending[k] = false;
+    }
+    std::memcpy(L->h[k], ent.data(), ent.size() * sizeof(gs_seg_run));
+    if (L->done_recorded[k]) GS_CHECK_CUDA(ctx, cudaStreamWaitEvent(stream, L->done[k], 0));
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(L->d[k], L->h[k], ent.size() * sizeof(gs_seg_run), cudaMemcpyHostToDevice,
+                                       stream));
+    GS_CHECK_CUDA(ctx, cudaEventRecord(L->uploaded[k], stream));
+    L->upload_pending[k] = true;
+    if (stream != ctx->stream) GS_CHECK_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, L->uploaded[k], 0));
+    *slot_out = k;
+    return GS_OK;
+}
+
+// Marks the end of the sweep that reads list slot k.
+gs_status list_done(gs_graph* g, int k) {
+    GS_CHECK_CUDA(g->ctx, cudaEventRecord(g->lists->done[k], g->ctx->stream));
+    g->lists->done_recorded[k] = true;
     return GS_OK;
 }
 
@@ -158,17 +208,6 @@ void pack(const gs_graph* g, std::vector<gs_seg_run>& ent, uint64_t cap, std::ve
     if (cur.list_n) segs.push_back(cur);
 }
 
-gs_status upload_list(gs_graph* g, const std::vector<gs_seg_run>& ent, cudaStream_t stream) {
-    gs_ctx* ctx = g->ctx;
-    GS_TRY(ensure_list(g, ent.size()));
-    std::memcpy(g->h_list, ent.data(), ent.size() * sizeof(gs_seg_run));
-    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_list, g->h_list, ent.size() * sizeof(gs_seg_run),
-                                       cudaMemcpyHostToDevice, stream));
-    GS_CHECK_CUDA(ctx, cudaEventRecord(g->ev_list, stream));
-    g->list_pending = true;
-    return GS_OK;
-}
-
 // Queues the copies of segment `sp` into a buffer and returns the buffer.
 gs_status stage(gs_graph* g, const SegPlan& sp, bool first, int prev, int* out) {
     gs_ctx* ctx = g->ctx;
@@ -206,11 +245,9 @@ gs_status run_streamed(gs_graph* g, std::vector<gs_seg_run>& ent, int direction,
     pack(g, ent, st->seg_records, segs);
     if (segs.empty()) return GS_OK;
     if (direction) std::reverse(segs.begin(), segs.end());
-    // the list and the buffers are rewritten only after the work queued so far
-    GS_CHECK_CUDA(ctx, cudaEventRecord(st->ev_start, ctx->stream));
-    GS_CHECK_CUDA(ctx, cudaStreamWaitEvent(st->copy, st->ev_start, 0));
-    GS_TRY(upload_list(g, ent, st->copy));
-    GS_CHECK_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, g->ev_list, 0));
+    int slot = 0;
+    GS_TRY(upload_list(g, ent, st->copy, &slot));
+    const gs_seg_run* list = g->lists->d[slot];
     int b = 0;
     GS_TRY(stage(g, segs[0], true, st->last, &b));
     gs_status status = GS_OK;
@@ -225,7 +262,7 @@ gs_status run_streamed(gs_graph* g, std::vector<gs_seg_run>& ent, int direction,
             status = gs_cuda_fail(ctx, e, "cudaStreamWaitEvent(ready)");
             break;
         }
-        g->seg.list = g->d_list + segs[k].list_beg;
+        g->seg.list = list + segs[k].list_beg;
         g->seg.n = (uint32_t)segs[k].list_n;
         g->seg.buf = st->d_buf[b];
         status = fn(arg);
@@ -240,7 +277,8 @@ gs_status run_streamed(gs_graph* g, std::vector<gs_seg_run>& ent, int direction,
         b = nb;
     }
     g->seg = SegView();
-    return status;
+    gs_status st2 = list_done(g, slot);
+    return status != GS_OK ? status : st2;
 }
 
 // Part id (group_full_index << 16 | i << 8 | j, get_ij in gstore.h:199-220)
@@ -301,13 +339,15 @@ gs_status gs_each_part_fn(gs_graph* g, const gs_segment* segs, int n_segs, gs_st
     }
     if (ent.empty()) return GS_OK;
     if (g->stream) return run_streamed(g, ent, 0, fn, arg);
-    GS_TRY(upload_list(g, ent, ctx->stream));
-    g->seg.list = g->d_list;
+    int slot = 0;
+    GS_TRY(upload_list(g, ent, ctx->stream, &slot));
+    g->seg.list = g->lists->d[slot];
     g->seg.n = (uint32_t)ent.size();
     g->seg.buf = g->d_rec;
     gs_status status = fn(arg);
     g->seg = SegView();
-    return status;
+    gs_status st2 = list_done(g, slot);
+    return status != GS_OK ? status : st2;
 }
 
 gs_status gs_stream_open(gs_graph* g, const uint32_t* host_grid, uint64_t segment_bytes) {
@@ -337,7 +377,6 @@ gs_status gs_stream_open(gs_graph* g, const uint32_t* host_grid, uint64_t segmen
         }
     }
     GS_CHECK_CUDA(ctx, cudaStreamCreateWithFlags(&st->copy, cudaStreamNonBlocking));
-    GS_CHECK_CUDA(ctx, cudaEventCreateWithFlags(&st->ev_start, cudaEventDisableTiming));
     for (int b = 0; b < 2; ++b) {
         GS_TRY(gs_dev_alloc(ctx, (void**)&st->d_buf[b], st->seg_records * 4 + 16));
         GS_CHECK_CUDA(ctx, cudaEventCreateWithFlags(&st->ready[b], cudaEventDisableTiming));
@@ -348,6 +387,7 @@ gs_status gs_stream_open(gs_graph* g, const uint32_t* host_grid, uint64_t segmen
 
 void gs_stream_close(gs_graph* g) {
     gs_streamer* st = g->stream;
+    if (st || g->lists) cudaStreamSynchronize(g->ctx->stream);   // sweeps reading buffers or lists
     if (st) {
         if (st->copy) cudaStreamSynchronize(st->copy);
         for (int b = 0; b < 2; ++b) {
@@ -355,20 +395,21 @@ void gs_stream_close(gs_graph* g) {
             if (st->ready[b]) cudaEventDestroy(st->ready[b]);
             if (st->freed[b]) cudaEventDestroy(st->freed[b]);
         }
-        if (st->ev_start) cudaEventDestroy(st->ev_start);
         if (st->copy) cudaStreamDestroy(st->copy);
         if (st->registered) cudaHostUnregister((void*)st->h_rec);
         delete st;
         g->stream = nullptr;
     }
-    gs_dev_free(g->d_list);
-    if (g->h_list) cudaFreeHost(g->h_list);
-    if (g->ev_list) cudaEventDestroy(g->ev_list);
-    g->d_list = nullptr;
-    g->h_list = nullptr;
-    g->ev_list = nullptr;
-    g->list_cap = 0;
-    g->list_pending = false;
+    if (g->lists) {
+        gs_seglists* L = g->lists;
+        free_lists(L);
+        for (int k = 0; k < 2; ++k) {
+            if (L->uploaded[k]) cudaEventDestroy(L->uploaded[k]);
+            if (L->done[k]) cudaEventDestroy(L->done[k]);
+        }
+        delete L;
+        g->lists = nullptr;
+    }
 }
 
 extern "C" gs_status gs_stream_stats(const gs_graph* g, uint64_t* bytes_copied, uint64_t* copies,

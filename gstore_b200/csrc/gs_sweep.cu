@@ -93,15 +93,17 @@ __global__ void __launch_bounds__(kThreads) sweep_runs(const gs_tile_run* __rest
 // Sweeps the whole resident graph, or, during a streamed sweep, the runs of
 // the segment the graph points at.
 template <class Op>
-gs_status launch_sweep(gs_graph* g, const Op& op, int algo, uint64_t bytes) {
+gs_status launch_sweep(gs_graph* g, const Op& op, int algo, uint64_t bytes, bool blocked = false) {
     gs_ctx* ctx = g->ctx;
     const gs_seg_run* seg = g->seg.list;
-    const uint64_t n = seg ? g->seg.n : g->R;
+    blocked = blocked && !seg && g->d_runs_blk;
+    const uint64_t n = seg ? g->seg.n : (blocked ? g->R_blk : g->R);
     const uint32_t* rec = seg ? g->seg.buf : g->d_rec;
     if (n == 0) return GS_OK;
     const uint32_t grid = (uint32_t)std::min<uint64_t>(n, gs_grid_size(ctx, 8));
     gs_timer_begin(ctx);
-    sweep_runs<Op><<<grid, kThreads, 0, ctx->stream>>>(g->d_runs, n, g->d_units, rec, seg, op);
+    sweep_runs<Op><<<grid, kThreads, 0, ctx->stream>>>(blocked ? g->d_runs_blk : g->d_runs, n,
+                                                        blocked ? g->d_units_blk : g->d_units, rec, seg, op);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
     gs_timer_end(ctx, algo, seg ? 0 : bytes);
@@ -438,7 +440,7 @@ gs_status pr_sweep_launch(gs_state* s) {
     gs_graph* g = s->g;
     PrOp op{s->d_x, s->d_y, g->directed};
     // algorithmic bytes per iteration: 4E + 12V (records, x, s, inv)
-    return launch_sweep(g, op, GS_ALGO_PAGERANK, 4 * g->E + 12 * g->V);
+    return launch_sweep(g, op, GS_ALGO_PAGERANK, 4 * g->E + 12 * g->V, true);
 }
 
 gs_status pr_finalize(gs_state* s, int64_t* frontier, int* done) {
@@ -473,7 +475,7 @@ gs_status wcc_sweep_launch(gs_state* s) {
     gs_graph* g = s->g;
     WccOp op{s->d_parent, s->step == 0 ? s->d_touched : nullptr,
              (unsigned long long*)g->ctx->d_scalars};
-    return launch_sweep(g, op, GS_ALGO_WCC, 4 * g->E + 8 * g->V);
+    return launch_sweep(g, op, GS_ALGO_WCC, 4 * g->E + 8 * g->V, true);
 }
 
 gs_status wcc_finalize(gs_state* s, int64_t* frontier, int* done) {
@@ -516,7 +518,7 @@ gs_status kcore_init(gs_state* s) {
 gs_status kcore_sweep_launch(gs_state* s) {
     gs_graph* g = s->g;
     KcoreOp op{s->d_deg, s->d_kactive, s->d_act};
-    return launch_sweep(g, op, GS_ALGO_KCORE, 0);
+    return launch_sweep(g, op, GS_ALGO_KCORE, 0, true);
 }
 
 gs_status kcore_finalize(gs_state* s, int64_t* frontier, int* done) {
