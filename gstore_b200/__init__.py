@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 from pathlib import Path
 
 import numpy as np
@@ -41,6 +42,8 @@ ABI_SYMBOLS = [
     "gs_download", "gs_result_count", "gs_bfs_stats", "gs_pagerank_compat",
     "gs_kron_generate_device", "gs_kron_generate", "gs_convert", "gs_graph_download",
     "gs_bfs_noalloc", "gs_upload_graph_streamed", "gs_stream_stats",
+    "gs_batch_create", "gs_batch_add", "gs_batch_run", "gs_batch_download", "gs_batch_result_count",
+    "gs_batch_bfs_levels", "gs_batch_stats", "gs_batch_free",
 ]
 
 
@@ -94,6 +97,14 @@ def lib():
             "gs_bfs_noalloc": [vp, u64, vp, C.POINTER(C.c_int64)],
             "gs_upload_graph_streamed": [vp, vp, u64, vp, u64, vp, u64, u64, pvp],
             "gs_stream_stats": [vp, pu64, pu64, pu64, pu64],
+            "gs_batch_create": [vp, pvp],
+            "gs_batch_add": [vp, vp, i32, i64, C.POINTER(C.c_int)],
+            "gs_batch_run": [vp],
+            "gs_batch_download": [vp, i32, i32, vp, u64],
+            "gs_batch_result_count": [vp, i32, pu64],
+            "gs_batch_bfs_levels": [vp, i32, vp, i32, C.POINTER(C.c_int)],
+            "gs_batch_stats": [vp, pu64, C.POINTER(C.c_double)],
+            "gs_batch_free": [vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -150,6 +161,7 @@ class Context:
 
     def __init__(self, device: int = 0, hbm_budget: int = 0, directed: bool = False):
         self._h = C.c_void_p()
+        self._children = weakref.WeakSet()   # graphs, states, batches made from this context
         st = lib().gs_create(C.byref(self._h), device, hbm_budget, int(directed))
         if st != 0:
             raise GStoreError(st, "gs_create failed (no usable CUDA device?)")
@@ -160,7 +172,14 @@ class Context:
             raise GStoreError(st, lib().gs_last_error(self._h).decode())
 
     def close(self):
+        """Free every object made from this context, then the context
+        (gs_destroy does not free graphs, states or batches)."""
         if self._h:
+            kids = list(self._children)
+            for kind in (State, Batch, Graph):
+                for k in kids:
+                    if isinstance(k, kind):
+                        k.free()
             lib().gs_destroy(self._h)
             self._h = C.c_void_p()
 
@@ -248,6 +267,69 @@ class Context:
         return Graph(self, h)
 
 
+class Batch:
+    """Queries run together (gs_batch): multi-source BFS groups, WCC and
+    k-core queries over several graphs in one persistent launch."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self._h = C.c_void_p()
+        ctx._check(lib().gs_batch_create(ctx._h, C.byref(self._h)))
+        self._graphs = {}
+        ctx._children.add(self)
+
+    def add(self, graph: "Graph", algo, arg: int = 0) -> int:
+        a = ALGOS[algo] if isinstance(algo, str) else int(algo)
+        qid = C.c_int()
+        self.ctx._check(lib().gs_batch_add(self._h, graph._h, a, arg, C.byref(qid)))
+        self._graphs[qid.value] = (graph, a)
+        return qid.value
+
+    def run(self):
+        self.ctx._check(lib().gs_batch_run(self._h))
+
+    def download(self, qid: int, what: int = 0) -> np.ndarray:
+        graph, a = self._graphs[qid]
+        dt = {GS_ALGO_BFS: np.uint8, GS_ALGO_PAGERANK: np.float32, GS_ALGO_KCORE: np.int32,
+              GS_ALGO_WCC: np.uint32}[a]
+        out = np.empty(graph.V, dt)
+        self.ctx._check(lib().gs_batch_download(self._h, qid, what, _ptr(out), out.nbytes))
+        return out
+
+    def count(self, qid: int) -> int:
+        c = C.c_uint64()
+        self.ctx._check(lib().gs_batch_result_count(self._h, qid, C.byref(c)))
+        return c.value
+
+    def bfs_levels(self, qid: int) -> np.ndarray:
+        out = np.zeros(256, np.uint64)
+        n = C.c_int()
+        self.ctx._check(lib().gs_batch_bfs_levels(self._h, qid, _ptr(out), 256, C.byref(n)))
+        return out[: n.value].copy()
+
+    def stats(self):
+        n, ms = C.c_uint64(), C.c_double()
+        self.ctx._check(lib().gs_batch_stats(self._h, C.byref(n), C.byref(ms)))
+        return {"launches": n.value, "kernel_ms": ms.value}
+
+    def free(self):
+        if self._h:
+            lib().gs_batch_free(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
 class Graph:
     """A resident tile grid (gs_graph)."""
 
@@ -255,6 +337,7 @@ class Graph:
         self.ctx = ctx
         self._h = handle
         self._keep = keep        # host records of a streamed graph
+        ctx._children.add(self)
         e, t, i, v = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
         ctx._check(lib().gs_graph_info(self._h, C.byref(e), C.byref(t), C.byref(i), C.byref(v)))
         self.n_edges, self.n_tiles, self.n_items, self.V = e.value, t.value, i.value, v.value
@@ -335,6 +418,7 @@ class State:
         self.graph = graph
         self._h = handle
         self.algo = algo
+        graph.ctx._children.add(self)
 
     def __enter__(self):
         return self

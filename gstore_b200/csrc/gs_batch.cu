@@ -1,0 +1,934 @@
+// Batched queries (sm_100a): many BFS, WCC and k-core queries per persistent
+// launch.
+//
+// Multi-source BFS.  Up to 64 BFS roots on one graph run together with one
+// bit per query in W-bit frontier words (W = 32 or 64): per vertex a pair
+// {frontier, visited} and a `next` word.  A record (v0, v1) of a swept tile
+// does, for all queries at once, what bfs_onepart does for one
+// (bfs.cpp:138-185):
+//     next[v1] |= frontier[v0] & ~visited[v1]
+//     next[v0] |= frontier[v1] & ~visited[v0]     (half grid)
+// and the finalize turns next into the new frontier and writes depth level+1
+// for each new (vertex, query) bit (iteration_finalize, bfs.cpp:187-224).  A
+// tile is swept when its row or column window holds a frontier vertex of any
+// query.  Per query the depths equal the single-root BFS bit for bit: a
+// vertex's depth is its level distance, whichever query shares the sweep.
+//
+// Batched WCC / k-core.  Any mix of WCC and k-core queries over any set of
+// resident graphs runs in one persistent launch: their runs and vertex
+// words are concatenated into one work list per phase (so graphs of uneven
+// size share the machine), each query keeping its own state.  The per-query
+// steps are the plain ones: k-core rounds (kcore.cpp:179-217) and
+// decrement sweeps (kcore.cpp:63-177), WCC hooking sweeps (wcc.cpp:177-278)
+// and pointer jumping (wcc.cpp:372-390).
+//
+// Persistent launches are cooperative (every CTA resident); phases are
+// separated by a grid barrier whose wait is bounded by kBarrierNs: a CTA that
+// waits longer sets the error flag and every CTA returns.
+//
+// Autotuning.  For the BFS groups of a graph the tuner tries each candidate
+// configuration once — frontier word width (32 or 64 queries per group) and
+// run order (file order, 64-unit runs; or L2-blocked, 8-unit runs) — timing
+// each launch with CUDA events per query, then keeps the fastest for that
+// graph.
+#include "gs_internal.cuh"
+#include "gs_ops.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+
+namespace {
+
+using namespace gsops;
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr uint64_t kBarrierNs = 4000000000ull;   // 4 s
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid-wide barrier of a cooperative launch.  bar[0] counts arrivals, bar[1]
+// is the generation.  False when the wait gave up or another CTA failed.
+__device__ bool grid_barrier(unsigned int* bar, int* err) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* vgen = bar + 1;
+        const unsigned int gen = *vgen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            const uint64_t t0 = global_ns();
+            while (*vgen == gen) {
+                if (*(volatile int*)err) break;
+                if (global_ns() - t0 > kBarrierNs) {
+                    atomicOr(err, 1);
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+        ok = *(volatile int*)err == 0;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// ------------------------------------------------------------ MS-BFS ----
+template <class W>
+struct FvPair;
+template <>
+struct alignas(8) FvPair<uint32_t> {
+    uint32_t f, vis;
+};
+template <>
+struct alignas(16) FvPair<unsigned long long> {
+    unsigned long long f, vis;
+};
+
+__device__ __forceinline__ FvPair<uint32_t> load_fv(const FvPair<uint32_t>* p) {
+    const uint2 x = __ldcg(reinterpret_cast<const uint2*>(p));
+    return FvPair<uint32_t>{x.x, x.y};
+}
+__device__ __forceinline__ FvPair<unsigned long long> load_fv(const FvPair<unsigned long long>* p) {
+    const ulonglong2 x = __ldcg(reinterpret_cast<const ulonglong2*>(p));
+    return FvPair<unsigned long long>{x.x, x.y};
+}
+__device__ __forceinline__ void store_fv(FvPair<uint32_t>* p, uint32_t f, uint32_t vis) {
+    __stcg(reinterpret_cast<uint2*>(p), make_uint2(f, vis));
+}
+__device__ __forceinline__ void store_fv(FvPair<unsigned long long>* p, unsigned long long f,
+                                         unsigned long long vis) {
+    ulonglong2 x;
+    x.x = f;
+    x.y = vis;
+    __stcg(reinterpret_cast<ulonglong2*>(p), x);
+}
+__device__ __forceinline__ int popc_w(uint32_t x) { return __popc(x); }
+__device__ __forceinline__ int popc_w(unsigned long long x) { return __popcll(x); }
+__device__ __forceinline__ int ffs_w(uint32_t x) { return __ffs(x); }
+__device__ __forceinline__ int ffs_w(unsigned long long x) { return __ffsll((long long)x); }
+
+template <class W>
+struct MsArgs {
+    const gs_tile_run* runs;
+    const gs_unit* units;
+    const uint32_t* rec;
+    uint64_t R;
+    uint64_t N;
+    uint32_t nw;
+    FvPair<W>* fv;
+    W* next;
+    uint8_t* depth;                  // [N][bits]
+    uint8_t* act;                    // 2 x nw, by level parity
+    unsigned long long* total;       // fresh (vertex, query) pairs per level, [256]
+    W* overflow;                     // queries that reached a depth over 254
+    unsigned int* bar;
+    int* err;
+    int* levels;
+    int directed;
+};
+
+template <class W>
+struct MsOp {
+    FvPair<W>* fv;
+    W* next;
+    int directed;
+    struct Item {
+        uint32_t rb, cb;
+    };
+    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
+        c.rb = row << 16;
+        c.cb = col << 16;
+        return true;
+    }
+    __device__ void record(uint32_t r, Item& c) const {
+        const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
+        const FvPair<W> sa = load_fv(fv + a), sb = load_fv(fv + b);
+        const W nb = sa.f & ~sb.vis;
+        if (nb) atomicOr(next + b, nb);
+        if (!directed) {            // the half grid stores each edge once
+            const W na = sb.f & ~sa.vis;
+            if (na) atomicOr(next + a, na);
+        }
+    }
+    __device__ void end(uint32_t, uint32_t, Item&) const {}
+};
+
+template <class W>
+__global__ void __launch_bounds__(kThreads) msbfs_kernel(MsArgs<W> a) {
+    constexpr int kBits = sizeof(W) * 8;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    const MsOp<W> op{a.fv, a.next, a.directed};
+    for (int level = 1; level < 255; ++level) {
+        const uint8_t* act = a.act + (level & 1) * a.nw;
+        uint8_t* act_next = a.act + ((level + 1) & 1) * a.nw;
+        // the flags of the next frontier start empty (last read one level ago)
+        for (uint64_t w = tid; w < a.nw; w += nth) act_next[w] = 0;
+        // sweep: a CTA per run, a warp per unit; a tile is swept when its row
+        // (or, half grid, column) window holds a frontier vertex of any query
+        // (grid::bfs_mmap, gstore.cpp:2671-2698)
+        for (uint64_t i = blockIdx.x; i < a.R; i += gridDim.x) {
+            const gs_tile_run run = a.runs[i];
+            const uint32_t row = a.units[run.unit_beg].rc >> 16;
+            const bool ar = __ldcg(act + row) != 0;
+            for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps) {
+                const gs_unit d = a.units[ui];
+                if (!ar && (a.directed || !__ldcg(act + (d.rc & 0xFFFFu)))) continue;
+                sweep_unit(d, a.rec, op, lane);
+            }
+        }
+        if (!grid_barrier(a.bar, a.err)) return;
+        // finalize: new = next & ~visited; frontier := new; visited |= new
+        uint64_t local = 0;
+        for (uint64_t v = tid; v < a.N; v += nth) {
+            const W nx = __ldcg(a.next + v);
+            const FvPair<W> s = load_fv(a.fv + v);
+            if (nx == 0 && s.f == 0) continue;
+            if (nx) __stcg(a.next + v, (W)0);
+            const W fresh = nx & ~s.vis;
+            store_fv(a.fv + v, fresh, s.vis | fresh);
+            if (fresh) {
+                local += popc_w(fresh);
+                act_next[v >> 16] = 1;
+                if (level == 254) atomicOr(a.overflow, fresh);
+                W x = fresh;
+                while (x) {
+                    const int q = ffs_w(x) - 1;
+                    a.depth[v * kBits + q] = (uint8_t)(level + 1);
+                    x &= x - 1;
+                }
+            }
+        }
+        warp_add_u64(a.total + level, local);
+        if (!grid_barrier(a.bar, a.err)) return;
+        if (__ldcg(a.total + level) == 0) {
+            if (tid == 0) *a.levels = level;
+            return;
+        }
+    }
+    if (tid == 0) *a.levels = 254;
+}
+
+// Root seeding: depth 1, frontier and visited bit of query q (bfs.cpp:70).
+// (one thread: several queries may share a root)
+template <class W>
+__global__ void msbfs_seed_kernel(const uint64_t* roots, int n, FvPair<W>* fv, uint8_t* depth, uint8_t* act1) {
+    constexpr int kBits = sizeof(W) * 8;
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int q = 0; q < n; ++q) {
+        const uint64_t r = roots[q];
+        fv[r].f |= (W)1 << q;
+        fv[r].vis |= (W)1 << q;
+        depth[r * kBits + q] = 1;
+        act1[r >> 16] = 1;   // calc_part_needed (bfs.cpp:324-338); level 1 has parity 1
+    }
+}
+
+// Per query: depth column q of [N][bits] into a contiguous V-byte array.
+__global__ void gather_depth_kernel(const uint8_t* __restrict__ depth, int bits, int q, uint8_t* __restrict__ out,
+                                    uint64_t V) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = tid; v < V; v += nth) out[v] = depth[v * bits + q];
+}
+
+// Per query and depth: vertex counts (the per-level frontier counts).
+__global__ void depth_histogram_kernel(const uint8_t* __restrict__ depth, int bits, int n_queries, uint64_t V,
+                                       unsigned long long* hist /* [n_queries][256] */) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = tid; i < V * bits; i += nth) {
+        const int q = (int)(i % bits);
+        if (q >= n_queries) continue;
+        const uint8_t d = depth[i];
+        if (d) atomicAdd(hist + q * 256 + d, 1ull);
+    }
+}
+
+// ----------------------------------------------------- WCC / k-core ----
+struct BQuery {
+    const gs_tile_run* runs;
+    const gs_unit* units;
+    const uint32_t* rec;
+    uint64_t R;
+    uint64_t words;              // N / 32
+    uint32_t nw;
+    int algo;
+    int k;
+    uint32_t* parent;            // WCC
+    uint8_t* touched;
+    int32_t* deg;                // k-core
+    uint32_t* removed;
+    uint8_t* act;                // 2 x nw, by iteration parity
+    unsigned long long* cnt;     // [4]: changes (WCC) / removals (k-core) by iteration
+    int* sweeps;
+};
+
+constexpr int kMaxBatch = 64;
+
+// KcoreOp for a persistent kernel: the removed bits and window flags change
+// between phases, so they are read through L2 (never the non-coherent path).
+struct KcoreOpL2 {
+    int32_t* deg;
+    const uint32_t* removed;
+    const uint8_t* act;
+    struct Item {
+        uint32_t rb, cb;
+        bool fr, fc;
+    };
+    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
+        c.fr = __ldcg(act + row) != 0;     // gstore.cpp:2773-2782
+        c.fc = __ldcg(act + col) != 0;
+        c.rb = row << 16;
+        c.cb = col << 16;
+        return c.fr || c.fc;
+    }
+    __device__ void record(uint32_t r, Item& c) const {
+        const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
+        if (c.fr && (__ldcg(removed + (a >> 5)) >> (a & 31) & 1u)) atomicSub(deg + b, 1);  // kcore.cpp:77-78
+        if (c.fc && (__ldcg(removed + (b >> 5)) >> (b & 31) & 1u)) atomicSub(deg + a, 1);  // kcore.cpp:90-91
+    }
+    __device__ void end(uint32_t, uint32_t, Item&) const {}
+};
+
+struct BatchArgs {
+    BQuery* q;
+    int nq;
+    unsigned int* bar;
+    int* err;
+};
+
+__device__ __forceinline__ int find_query(const uint64_t* pre, int nq, uint64_t x) {
+    int q = 0;
+    while (q + 1 < nq && pre[q + 1] <= x) ++q;
+    return q;
+}
+
+__global__ void __launch_bounds__(kThreads) wk_batch_kernel(BatchArgs a) {
+    __shared__ uint64_t run_pre[kMaxBatch + 1], word_pre[kMaxBatch + 1];
+    __shared__ unsigned long long done_mask;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t gwarp = (uint64_t)blockIdx.x * kWarps + warp;
+    const uint64_t nwarps = (uint64_t)gridDim.x * kWarps;
+    if (threadIdx.x == 0) {
+        run_pre[0] = word_pre[0] = 0;
+        for (int q = 0; q < a.nq; ++q) {
+            run_pre[q + 1] = run_pre[q] + a.q[q].R;
+            word_pre[q + 1] = word_pre[q] + a.q[q].words;
+        }
+        done_mask = 0;
+    }
+    __syncthreads();
+    for (int it = 0;; ++it) {
+        const int p = it & 1;
+        // phase A: k-core round / WCC pointer jumping, per 32-vertex word
+        for (uint64_t x = gwarp; x < word_pre[a.nq]; x += nwarps) {
+            const int qi = find_query(word_pre, a.nq, x);
+            if (done_mask >> qi & 1) continue;
+            const BQuery& q = a.q[qi];
+            const uint64_t w = x - word_pre[qi];
+            const uint32_t v = (uint32_t)(w * 32 + lane);
+            if (lane == 0 && w < 1) {
+                q.cnt[(it + 2) & 3] = 0;
+                for (uint32_t i = 0; i < q.nw; ++i) q.act[(p ^ 1) * q.nw + i] = 0;
+            }
+            if (q.algo == GS_ALGO_KCORE) {
+                const int32_t dv = __ldcg(q.deg + v);
+                const int16_t m = (int16_t)dv;           // kcore.cpp:189
+                const bool gone = m < q.k && m > 0;
+                if (gone) __stcg(q.deg + v, 0);
+                const uint32_t bits = __ballot_sync(kFull, gone);
+                if (lane == 0) {
+                    __stcg(q.removed + w, bits);
+                    if (bits) {
+                        q.act[p * q.nw + (w >> 11)] = 1;
+                        atomicAdd(q.cnt + (it & 3), (unsigned long long)__popc(bits));
+                    }
+                }
+            } else if (it > 0) {
+                const uint32_t r = find_root(q.parent, v);
+                if (r != v) __stcg(q.parent + v, r);
+            }
+        }
+        if (!grid_barrier(a.bar, a.err)) return;
+        // decisions, identical in every CTA (counters are final here)
+        if (threadIdx.x == 0) {
+            for (int qi = 0; qi < a.nq; ++qi) {
+                if (done_mask >> qi & 1) continue;
+                const BQuery& q = a.q[qi];
+                bool done;
+                if (q.algo == GS_ALGO_KCORE) done = __ldcg(q.cnt + (it & 3)) == 0;
+                else done = it > 0 && __ldcg(q.cnt + ((it - 1) & 3)) == 0;
+                if (done) {
+                    done_mask |= 1ull << qi;
+                    if (blockIdx.x == 0) *q.sweeps = it;
+                }
+            }
+        }
+        __syncthreads();
+        if (done_mask == (a.nq == 64 ? ~0ull : ((1ull << a.nq) - 1))) return;
+        // phase B: one sweep of every query still running
+        for (uint64_t x = blockIdx.x; x < run_pre[a.nq]; x += gridDim.x) {
+            const int qi = find_query(run_pre, a.nq, x);
+            if (done_mask >> qi & 1) continue;
+            const BQuery& q = a.q[qi];
+            const gs_tile_run run = q.runs[x - run_pre[qi]];
+            if (q.algo == GS_ALGO_KCORE) {
+                const KcoreOpL2 op{q.deg, q.removed, q.act + p * q.nw};
+                for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps)
+                    sweep_unit(q.units[ui], q.rec, op, lane);
+            } else {
+                const WccOp op{q.parent, it == 0 ? q.touched : nullptr, q.cnt + (it & 3)};
+                for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps)
+                    sweep_unit(q.units[ui], q.rec, op, lane);
+            }
+        }
+        if (!grid_barrier(a.bar, a.err)) return;
+    }
+}
+
+__global__ void wk_init_kernel(uint32_t* parent, uint64_t N) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = tid; v < N; v += nth) parent[v] = (uint32_t)v;
+}
+
+__global__ void wk_labels_kernel(const uint32_t* parent, const uint8_t* touched, uint32_t* out, uint64_t V,
+                                 unsigned long long* count) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t local = 0;
+    for (uint64_t v = tid; v < V; v += nth) {
+        if (!touched[v]) {
+            out[v] = 0xFFFFFFFFu;     // invalid_cid, wcc.cpp:54
+            continue;
+        }
+        uint32_t r = parent[v];
+        while (parent[r] != r) r = parent[r];
+        out[v] = r;
+        local += r == v;
+    }
+    warp_add_u64(count, local);
+}
+
+__global__ void wk_count_nonzero_kernel(const int32_t* deg, uint64_t V, unsigned long long* out) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t local = 0;
+    for (uint64_t v = tid; v < V; v += nth) local += deg[v] != 0;
+    warp_add_u64(out, local);
+}
+
+inline uint32_t blocks_for(uint64_t n, const gs_ctx* ctx) {
+    const uint64_t b = (n + kThreads - 1) / kThreads;
+    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(b, gs_grid_size(ctx, 16)));
+}
+
+}  // namespace
+
+// ================================================================ host ====
+struct gs_batch_query {
+    gs_graph* g = nullptr;
+    gs_algo algo = GS_ALGO_BFS;
+    int64_t arg = 0;
+    gs_status status = GS_OK;
+    bool ran = false;
+    int group = -1;          // BFS: group index, bit = lane
+    int lane = 0;
+    int64_t sweeps = 0;
+    // WCC / k-core state
+    uint32_t* parent = nullptr;
+    uint8_t* touched = nullptr;
+    int32_t* deg = nullptr;
+    uint32_t* removed = nullptr;
+    uint8_t* act = nullptr;
+    unsigned long long* cnt = nullptr;
+    // PageRank: a plain state
+    gs_state* pr = nullptr;
+};
+
+struct gs_bfs_group {
+    gs_graph* g = nullptr;
+    int bits = 64;
+    bool blocked = true;
+    std::vector<int> queries;
+    uint8_t* depth = nullptr;          // [N][bits]
+    int levels = 0;
+    unsigned long long overflow = 0;
+    std::vector<uint64_t> hist;        // [queries][256], filled on demand
+};
+
+struct gs_batch {
+    gs_ctx* ctx = nullptr;
+    std::vector<gs_batch_query> q;
+    std::vector<gs_bfs_group> groups;
+    size_t first_new = 0;              // queries before this index have run
+    uint64_t launches = 0;
+    double kernel_ms = 0.0;
+    // scratch
+    void* d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+
+// Autotuner record of one graph: per candidate, time per query of its runs.
+struct gs_tune {
+    double ms_per_query[4] = {0, 0, 0, 0};   // (bits 32/64) x (file / blocked)
+    int samples[4] = {0, 0, 0, 0};
+};
+
+namespace {
+
+std::vector<std::pair<const gs_graph*, gs_tune>> g_tune;   // per graph (single-threaded contexts)
+
+gs_tune& tune_of(const gs_graph* g) {
+    for (auto& t : g_tune)
+        if (t.first == g) return t.second;
+    g_tune.emplace_back(g, gs_tune());
+    return g_tune.back().second;
+}
+
+// Candidates: 0 = 32-bit words, file order; 1 = 32-bit, blocked; 2 = 64-bit,
+// file order; 3 = 64-bit, blocked.  Each is tried once, then the fastest per
+// query is kept.
+int pick_candidate(const gs_tune& t) {
+    for (int c = 3; c >= 0; --c)
+        if (t.samples[c] == 0) return c;
+    int best = 3;
+    for (int c = 0; c < 4; ++c)
+        if (t.ms_per_query[c] < t.ms_per_query[best]) best = c;
+    return best;
+}
+
+gs_status scratch(gs_batch* b, size_t bytes, void** out) {
+    if (bytes > b->scratch_bytes) {
+        gs_dev_free(b->d_scratch);
+        b->d_scratch = nullptr;
+        b->scratch_bytes = 0;
+        GS_TRY(gs_dev_alloc(b->ctx, &b->d_scratch, bytes));
+        b->scratch_bytes = bytes;
+    }
+    *out = b->d_scratch;
+    return GS_OK;
+}
+
+int coop_grid(gs_ctx* ctx, const void* kernel) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    return ctx->num_sms * std::min(per_sm, 4);
+}
+
+// One multi-source BFS launch over the queries of group `gi`.
+template <class W>
+gs_status run_bfs_group(gs_batch* b, gs_bfs_group& grp) {
+    gs_ctx* ctx = b->ctx;
+    gs_graph* g = grp.g;
+    constexpr int kBits = sizeof(W) * 8;
+    const int n = (int)grp.queries.size();
+    const uint64_t N = g->N;
+    // device scratch: fv (N pairs), next (N words), act (2 nw), totals, bar, err, levels, overflow, roots
+    const size_t fv_b = N * sizeof(FvPair<W>), nx_b = N * sizeof(W);
+    const size_t act_b = (2 * (size_t)g->nw + 255) & ~(size_t)255;
+    const size_t small_b = 256 * 8 + 64 + 8 * kMaxBatch + 64;
+    void* base = nullptr;
+    GS_TRY(scratch(b, fv_b + nx_b + act_b + small_b, &base));
+    char* p = (char*)base;
+    FvPair<W>* fv = (FvPair<W>*)p;
+    W* next = (W*)(p + fv_b);
+    uint8_t* act = (uint8_t*)(p + fv_b + nx_b);
+    char* small = p + fv_b + nx_b + act_b;
+    unsigned long long* total = (unsigned long long*)small;
+    unsigned int* bar = (unsigned int*)(small + 256 * 8);
+    int* err = (int*)(small + 256 * 8 + 16);
+    int* levels = (int*)(small + 256 * 8 + 32);
+    W* overflow = (W*)(small + 256 * 8 + 48);
+    uint64_t* roots = (uint64_t*)(small + 256 * 8 + 64);
+    GS_TRY(gs_dev_alloc(ctx, (void**)&grp.depth, N * kBits));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(base, 0, fv_b + nx_b + act_b + small_b, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(grp.depth, 0, N * kBits, ctx->stream));
+    std::vector<uint64_t> h_roots(n);
+    for (int i = 0; i < n; ++i) h_roots[i] = (uint64_t)b->q[grp.queries[i]].arg;
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(roots, h_roots.data(), n * 8, cudaMemcpyHostToDevice, ctx->stream));
+    msbfs_seed_kernel<W><<<1, 1, 0, ctx->stream>>>(roots, n, fv, grp.depth, act + g->nw);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    ctx->launches += 1;
+    MsArgs<W> a{grp.blocked ? g->d_runs_blk : g->d_runs,
+                grp.blocked ? g->d_units_blk : g->d_units,
+                g->d_rec,
+                grp.blocked ? g->R_blk : g->R,
+                N,
+                g->nw,
+                fv,
+                next,
+                grp.depth,
+                act,
+                total,
+                overflow,
+                bar,
+                err,
+                levels,
+                g->directed};
+    void* args[] = {&a};
+    const int grid = coop_grid(ctx, (const void*)msbfs_kernel<W>);
+    GS_CHECK_CUDA(ctx, cudaEventRecord(b->e0, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)msbfs_kernel<W>, dim3(grid), dim3(kThreads), args, 0,
+                                                   ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaEventRecord(b->e1, ctx->stream));
+    ctx->launches += 1;
+    b->launches += 1;
+    int h_err = 0, h_levels = 0;
+    W h_over = 0;
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(&h_err, err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(&h_levels, levels, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(&h_over, overflow, sizeof(W), cudaMemcpyDeviceToHost, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b->e0, b->e1);
+    b->kernel_ms += ms;
+    gs_tune& t = tune_of(g);
+    const int c = (kBits == 64 ? 2 : 0) + (grp.blocked ? 1 : 0);
+    t.ms_per_query[c] = (t.ms_per_query[c] * t.samples[c] + ms / n) / (t.samples[c] + 1);
+    t.samples[c] += 1;
+    if (h_err) return gs_fail(ctx, GS_ERR_TIMEOUT, "batched BFS: a grid barrier wait gave up");
+    grp.levels = h_levels;
+    grp.overflow = (unsigned long long)h_over;
+    for (int i = 0; i < n; ++i) {
+        gs_batch_query& q = b->q[grp.queries[i]];
+        q.ran = true;
+        q.sweeps = h_levels;
+        if (grp.overflow >> i & 1) q.status = GS_ERR_RANGE;
+    }
+    return GS_OK;
+}
+
+gs_status run_bfs_queries(gs_batch* b, std::vector<int>& idx) {
+    // group by graph, in order of first appearance
+    std::vector<gs_graph*> graphs;
+    for (int i : idx)
+        if (std::find(graphs.begin(), graphs.end(), b->q[i].g) == graphs.end()) graphs.push_back(b->q[i].g);
+    for (gs_graph* g : graphs) {
+        std::vector<int> mine;
+        for (int i : idx)
+            if (b->q[i].g == g) mine.push_back(i);
+        const int cand = pick_candidate(tune_of(g));
+        const int bits = cand >= 2 ? 64 : 32;
+        const bool blocked = (cand & 1) != 0 && g->d_runs_blk;
+        for (size_t s = 0; s < mine.size(); s += bits) {
+            gs_bfs_group grp;
+            grp.g = g;
+            grp.bits = bits;
+            grp.blocked = blocked;
+            for (size_t k = s; k < std::min(mine.size(), s + bits); ++k) {
+                grp.queries.push_back(mine[k]);
+                b->q[mine[k]].group = (int)b->groups.size();
+                b->q[mine[k]].lane = (int)(k - s);
+            }
+            b->groups.push_back(grp);
+            gs_bfs_group& gg = b->groups.back();
+            GS_TRY(bits == 64 ? run_bfs_group<unsigned long long>(b, gg) : run_bfs_group<uint32_t>(b, gg));
+        }
+    }
+    return GS_OK;
+}
+
+gs_status run_wk_queries(gs_batch* b, std::vector<int>& idx) {
+    gs_ctx* ctx = b->ctx;
+    for (size_t s = 0; s < idx.size(); s += kMaxBatch) {
+        const size_t e = std::min(idx.size(), s + kMaxBatch);
+        std::vector<BQuery> dq;
+        for (size_t k = s; k < e; ++k) {
+            gs_batch_query& q = b->q[idx[k]];
+            gs_graph* g = q.g;
+            const uint64_t N = g->N;
+            GS_TRY(gs_dev_alloc(ctx, (void**)&q.cnt, 4 * sizeof(unsigned long long)));
+            GS_CHECK_CUDA(ctx, cudaMemsetAsync(q.cnt, 0, 4 * sizeof(unsigned long long), ctx->stream));
+            GS_TRY(gs_dev_alloc(ctx, (void**)&q.act, 2 * (size_t)g->nw));
+            GS_CHECK_CUDA(ctx, cudaMemsetAsync(q.act, 0, 2 * (size_t)g->nw, ctx->stream));
+            if (q.algo == GS_ALGO_WCC) {
+                GS_TRY(gs_dev_alloc(ctx, (void**)&q.parent, N * 4));
+                GS_TRY(gs_dev_alloc(ctx, (void**)&q.touched, N));
+                wk_init_kernel<<<blocks_for(N, ctx), kThreads, 0, ctx->stream>>>(q.parent, N);
+                ctx->launches++;
+                GS_CHECK_CUDA(ctx, cudaMemsetAsync(q.touched, 0, N, ctx->stream));
+            } else {
+                GS_TRY(gs_dev_alloc(ctx, (void**)&q.deg, N * 4));
+                GS_TRY(gs_dev_alloc(ctx, (void**)&q.removed, N / 8));
+                GS_CHECK_CUDA(ctx, cudaMemcpyAsync(q.deg, g->d_degree, N * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+            }
+            BQuery d;
+            std::memset(&d, 0, sizeof(d));
+            d.runs = g->d_runs_blk ? g->d_runs_blk : g->d_runs;
+            d.units = g->d_runs_blk ? g->d_units_blk : g->d_units;
+            d.rec = g->d_rec;
+            d.R = g->d_runs_blk ? g->R_blk : g->R;
+            d.words = N / 32;
+            d.nw = g->nw;
+            d.algo = (int)q.algo;
+            d.k = (int)q.arg;
+            d.parent = q.parent;
+            d.touched = q.touched;
+            d.deg = q.deg;
+            d.removed = q.removed;
+            d.act = q.act;
+            d.cnt = q.cnt;
+            dq.push_back(d);
+        }
+        const int nq = (int)dq.size();
+        void* base = nullptr;
+        const size_t qb = ((nq * sizeof(BQuery)) + 255) & ~(size_t)255;
+        GS_TRY(scratch(b, qb + 256 + nq * sizeof(int), &base));
+        BQuery* d_q = (BQuery*)base;
+        unsigned int* bar = (unsigned int*)((char*)base + qb);
+        int* err = (int*)((char*)base + qb + 16);
+        int* sweeps = (int*)((char*)base + qb + 256);
+        for (int k = 0; k < nq; ++k) dq[k].sweeps = sweeps + k;
+        GS_CHECK_CUDA(ctx, cudaMemsetAsync((char*)base + qb, 0, 256 + nq * sizeof(int), ctx->stream));
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(d_q, dq.data(), nq * sizeof(BQuery), cudaMemcpyHostToDevice, ctx->stream));
+        BatchArgs a{d_q, nq, bar, err};
+        void* args[] = {&a};
+        const int grid = coop_grid(ctx, (const void*)wk_batch_kernel);
+        GS_CHECK_CUDA(ctx, cudaEventRecord(b->e0, ctx->stream));
+        GS_CHECK_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)wk_batch_kernel, dim3(grid), dim3(kThreads), args,
+                                                       0, ctx->stream));
+        GS_CHECK_CUDA(ctx, cudaEventRecord(b->e1, ctx->stream));
+        ctx->launches += 1;
+        b->launches += 1;
+        std::vector<int> h_sweeps(nq);
+        int h_err = 0;
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(h_sweeps.data(), sweeps, nq * sizeof(int), cudaMemcpyDeviceToHost,
+                                           ctx->stream));
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(&h_err, err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, b->e0, b->e1);
+        b->kernel_ms += ms;
+        if (h_err) return gs_fail(ctx, GS_ERR_TIMEOUT, "batched WCC/k-core: a grid barrier wait gave up");
+        for (int k = 0; k < nq; ++k) {
+            gs_batch_query& q = b->q[idx[s + k]];
+            q.ran = true;
+            q.sweeps = h_sweeps[k];
+        }
+    }
+    return GS_OK;
+}
+
+void free_query(gs_batch_query& q) {
+    gs_dev_free(q.parent);
+    gs_dev_free(q.touched);
+    gs_dev_free(q.deg);
+    gs_dev_free(q.removed);
+    gs_dev_free(q.act);
+    gs_dev_free(q.cnt);
+    q.parent = nullptr;
+    q.touched = nullptr;
+    q.deg = nullptr;
+    q.removed = nullptr;
+    q.act = nullptr;
+    q.cnt = nullptr;
+    if (q.pr) gs_state_free(q.pr);
+    q.pr = nullptr;
+}
+
+gs_status query_of(gs_batch* b, int id, gs_batch_query** out) {
+    if (!b || id < 0 || (size_t)id >= b->q.size()) return GS_ERR_ARG;
+    gs_batch_query& q = b->q[id];
+    if (!q.ran) return gs_fail(b->ctx, GS_ERR_STATE, "query has not run (call gs_batch_run)");
+    if (q.status != GS_OK) return gs_fail(b->ctx, q.status, "query failed");
+    *out = &q;
+    return GS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gs_status gs_batch_create(gs_ctx* ctx, gs_batch** out) {
+    if (!ctx || !out) return GS_ERR_ARG;
+    gs_batch* b = new (std::nothrow) gs_batch();
+    if (!b) return GS_ERR_OOM;
+    b->ctx = ctx;
+    if (cudaEventCreate(&b->e0) != cudaSuccess || cudaEventCreate(&b->e1) != cudaSuccess) {
+        delete b;
+        return gs_fail(ctx, GS_ERR_CUDA, "cudaEventCreate");
+    }
+    *out = b;
+    return GS_OK;
+}
+
+gs_status gs_batch_add(gs_batch* b, gs_graph* g, gs_algo algo, int64_t arg, int* query_id) {
+    if (!b || !g || !query_id) return GS_ERR_ARG;
+    gs_ctx* ctx = b->ctx;
+    if (g->ctx != ctx) return gs_fail(ctx, GS_ERR_ARG, "graph belongs to another context");
+    if (g->stream) return gs_fail(ctx, GS_ERR_UNSUPPORTED, "batched queries need graphs resident in HBM");
+    if (algo == GS_ALGO_BFS && (arg < 0 || (uint64_t)arg >= g->V)) return gs_fail(ctx, GS_ERR_ARG, "BFS root out of range");
+    if (algo == GS_ALGO_KCORE && g->directed)
+        return gs_fail(ctx, GS_ERR_UNSUPPORTED, "Kcore not applicable for directed graphs");
+    if (algo == GS_ALGO_PAGERANK && arg < 1) return gs_fail(ctx, GS_ERR_ARG, "iterations < 1");
+    if (algo != GS_ALGO_BFS && algo != GS_ALGO_WCC && algo != GS_ALGO_KCORE && algo != GS_ALGO_PAGERANK)
+        return GS_ERR_ARG;
+    gs_batch_query q;
+    q.g = g;
+    q.algo = algo;
+    q.arg = arg;
+    b->q.push_back(q);
+    *query_id = (int)b->q.size() - 1;
+    return GS_OK;
+}
+
+gs_status gs_batch_run(gs_batch* b) {
+    if (!b) return GS_ERR_ARG;
+    std::vector<int> bfs, wk, pr;
+    for (size_t i = b->first_new; i < b->q.size(); ++i) {
+        switch (b->q[i].algo) {
+            case GS_ALGO_BFS: bfs.push_back((int)i); break;
+            case GS_ALGO_WCC:
+            case GS_ALGO_KCORE: wk.push_back((int)i); break;
+            default: pr.push_back((int)i); break;
+        }
+    }
+    b->first_new = b->q.size();
+    GS_TRY(run_bfs_queries(b, bfs));
+    GS_TRY(run_wk_queries(b, wk));
+    for (int i : pr) {
+        gs_batch_query& q = b->q[i];
+        GS_TRY(gs_state_create(q.g, GS_ALGO_PAGERANK, q.arg, &q.pr));
+        int64_t steps = 0;
+        GS_TRY(gs_run(q.pr, &steps));
+        q.sweeps = steps;
+        q.ran = true;
+    }
+    return GS_OK;
+}
+
+gs_status gs_batch_download(gs_batch* b, int query_id, int what, void* host_dst, uint64_t bytes) {
+    gs_batch_query* q = nullptr;
+    GS_TRY(query_of(b, query_id, &q));
+    if (!host_dst) return GS_ERR_ARG;
+    gs_ctx* ctx = b->ctx;
+    gs_graph* g = q->g;
+    if (q->algo == GS_ALGO_PAGERANK) return gs_download(q->pr, what, host_dst, bytes);
+    const uint64_t need = q->algo == GS_ALGO_BFS ? g->V : g->V * 4;
+    if (bytes < need) return gs_fail(ctx, GS_ERR_ARG, "destination too small: need " + std::to_string(need));
+    void* tmp = nullptr;
+    GS_TRY(scratch(b, g->V * 4 + 16, &tmp));
+    const void* src = nullptr;
+    if (q->algo == GS_ALGO_BFS) {
+        const gs_bfs_group& grp = b->groups[q->group];
+        gather_depth_kernel<<<blocks_for(g->V, ctx), kThreads, 0, ctx->stream>>>(grp.depth, grp.bits, q->lane,
+                                                                                 (uint8_t*)tmp, g->V);
+        ctx->launches++;
+        src = tmp;
+    } else if (q->algo == GS_ALGO_WCC) {
+        wk_labels_kernel<<<blocks_for(g->V, ctx), kThreads, 0, ctx->stream>>>(q->parent, q->touched, (uint32_t*)tmp,
+                                                                              g->V, (unsigned long long*)ctx->d_scalars);
+        ctx->launches++;
+        src = tmp;
+    } else {
+        src = q->deg;
+    }
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(host_dst, src, need, cudaMemcpyDeviceToHost, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return GS_OK;
+}
+
+gs_status gs_batch_result_count(gs_batch* b, int query_id, uint64_t* count) {
+    gs_batch_query* q = nullptr;
+    GS_TRY(query_of(b, query_id, &q));
+    if (!count) return GS_ERR_ARG;
+    gs_ctx* ctx = b->ctx;
+    gs_graph* g = q->g;
+    if (q->algo == GS_ALGO_PAGERANK) return gs_result_count(q->pr, count);
+    if (q->algo == GS_ALGO_BFS) {
+        GS_TRY(gs_batch_bfs_levels(b, query_id, nullptr, 0, nullptr));
+        const uint64_t* h = b->groups[q->group].hist.data() + (size_t)q->lane * 256;
+        uint64_t s = 0;
+        for (int d = 1; d < 256; ++d) s += h[d];   // reached vertices (depth != 0)
+        *count = s;
+        return GS_OK;
+    }
+    unsigned long long* d = (unsigned long long*)ctx->d_scalars;
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(d, 0, 8, ctx->stream));
+    if (q->algo == GS_ALGO_WCC) {
+        void* tmp = nullptr;
+        GS_TRY(scratch(b, g->V * 4 + 16, &tmp));
+        wk_labels_kernel<<<blocks_for(g->V, ctx), kThreads, 0, ctx->stream>>>(q->parent, q->touched, (uint32_t*)tmp,
+                                                                              g->V, d);
+    } else {
+        wk_count_nonzero_kernel<<<blocks_for(g->V, ctx), kThreads, 0, ctx->stream>>>(q->deg, g->V, d);
+    }
+    ctx->launches++;
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->h_scalars, d, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *count = ctx->h_scalars[0];
+    return GS_OK;
+}
+
+gs_status gs_batch_bfs_levels(gs_batch* b, int query_id, uint64_t* level_counts, int max_levels, int* n_levels) {
+    gs_batch_query* q = nullptr;
+    GS_TRY(query_of(b, query_id, &q));
+    if (q->algo != GS_ALGO_BFS) return gs_fail(b->ctx, GS_ERR_ARG, "not a BFS query");
+    gs_ctx* ctx = b->ctx;
+    gs_bfs_group& grp = b->groups[q->group];
+    if (grp.hist.empty()) {
+        const int n = (int)grp.queries.size();
+        void* tmp = nullptr;
+        GS_TRY(scratch(b, (size_t)n * 256 * 8, &tmp));
+        GS_CHECK_CUDA(ctx, cudaMemsetAsync(tmp, 0, (size_t)n * 256 * 8, ctx->stream));
+        depth_histogram_kernel<<<blocks_for(grp.g->V * grp.bits, ctx), kThreads, 0, ctx->stream>>>(
+            grp.depth, grp.bits, n, grp.g->V, (unsigned long long*)tmp);
+        ctx->launches++;
+        GS_CHECK_CUDA(ctx, cudaGetLastError());
+        grp.hist.resize((size_t)n * 256);
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(grp.hist.data(), tmp, (size_t)n * 256 * 8, cudaMemcpyDeviceToHost,
+                                           ctx->stream));
+        GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    // level L's count = vertices at depth L + 1 (iteration_finalize's frontier
+    // count); the last level found nothing
+    if (!level_counts && !n_levels) return GS_OK;
+    const uint64_t* h = grp.hist.data() + (size_t)q->lane * 256;
+    int last = 1;
+    for (int d = 2; d < 256; ++d)
+        if (h[d]) last = d;
+    const int n = last;   // levels 1..last-1 found vertices, level `last` found none
+    if (level_counts)
+        for (int l = 0; l < n && l < max_levels; ++l) level_counts[l] = l + 2 < 256 ? h[l + 2] : 0;
+    if (n_levels) *n_levels = n;
+    return GS_OK;
+}
+
+gs_status gs_batch_stats(const gs_batch* b, uint64_t* launches, double* kernel_ms) {
+    if (!b) return GS_ERR_ARG;
+    if (launches) *launches = b->launches;
+    if (kernel_ms) *kernel_ms = b->kernel_ms;
+    return GS_OK;
+}
+
+gs_status gs_batch_free(gs_batch* b) {
+    if (!b) return GS_OK;
+    cudaStreamSynchronize(b->ctx->stream);
+    for (auto& q : b->q) free_query(q);
+    for (auto& grp : b->groups) gs_dev_free(grp.depth);
+    gs_dev_free(b->d_scratch);
+    if (b->e0) cudaEventDestroy(b->e0);
+    if (b->e1) cudaEventDestroy(b->e1);
+    delete b;
+    return GS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,154 @@
+// Per-record operations of the tile sweeps (sm_100a device code), shared by
+// the per-algorithm sweep kernels and the batched persistent kernels.
+//
+// Reference semantics per record (edge_t{v0, v1} in tile (i, j)):
+//   PR      pr.cpp:119-154      s[v1] += x[v0]; s[v0] += x[v1] (half grid)
+//   WCC     wcc.cpp:177-278     hook the larger root onto the smaller one
+//   k-core  kcore.cpp:63-177    --deg[other] for every removed endpoint
+#pragma once
+
+#include "gs_internal.cuh"
+
+namespace gsops {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint32_t bit_of(const uint32_t* __restrict__ bm, uint32_t v) {
+    return (__ldg(bm + (v >> 5)) >> (v & 31)) & 1u;
+}
+
+__device__ __forceinline__ uint4 load_stream(const uint4* p) { return __ldcs(p); }
+
+// One unit (<= kUnitRecords records of one tile) swept by one warp: the
+// records stream with 128-bit evict-first loads from base (file record r at
+// base[r]).  Op provides:
+//   struct Item;                                    per-unit warp-uniform context
+//   bool begin(uint32_t row, uint32_t col, Item&)   false = skip the unit
+//   void record(uint32_t rec, Item&)                one record, any lane
+//   void end(uint32_t row, uint32_t col, Item&)     warp-collective epilogue
+template <class Op>
+__device__ __forceinline__ void sweep_unit(const gs_unit d, const uint32_t* __restrict__ base, const Op& op,
+                                           uint32_t lane) {
+    const uint32_t row = d.rc >> 16, col = d.rc & 0xFFFFu;
+    typename Op::Item ic;
+    if (!op.begin(row, col, ic)) return;
+    const uint64_t b = d.rec_beg, e = d.rec_beg + d.n;
+    uint64_t ab = (b + 3) & ~3ull;
+    if (ab > e) ab = e;
+    uint64_t ae = e & ~3ull;
+    if (ae < ab) ae = ab;
+    if (b + lane < ab) op.record(__ldcs(base + b + lane), ic);
+    if (ae + lane < e) op.record(__ldcs(base + ae + lane), ic);
+    const uint4* r4 = reinterpret_cast<const uint4*>(base + ab);
+    const uint32_t n4 = (uint32_t)((ae - ab) >> 2);
+    for (uint32_t k = lane; k < n4; k += 2 * 32) {
+        const uint4 q0 = load_stream(r4 + k);
+        const bool two = k + 32 < n4;
+        uint4 q1 = make_uint4(0, 0, 0, 0);
+        if (two) q1 = load_stream(r4 + k + 32);
+        op.record(q0.x, ic);
+        op.record(q0.y, ic);
+        op.record(q0.z, ic);
+        op.record(q0.w, ic);
+        if (two) {
+            op.record(q1.x, ic);
+            op.record(q1.y, ic);
+            op.record(q1.z, ic);
+            op.record(q1.w, ic);
+        }
+    }
+    op.end(row, col, ic);
+}
+
+__device__ __forceinline__ void warp_add_u64(unsigned long long* dst, uint64_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, (unsigned long long)v);
+}
+
+// --------------------------------------------------------------- PageRank --
+struct PrOp {
+    const float* x;
+    float* y;
+    int directed;
+    struct Item {
+        uint32_t rb, cb;
+    };
+    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
+        c.rb = row << 16;
+        c.cb = col << 16;
+        return true;
+    }
+    __device__ void record(uint32_t r, Item& c) const {
+        const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
+        atomicAdd(y + b, __ldg(x + a));                 // pr.cpp:145-146
+        if (!directed) atomicAdd(y + a, __ldg(x + b));  // pr.cpp:147-150
+    }
+    __device__ void end(uint32_t, uint32_t, Item&) const {}
+};
+
+// -------------------------------------------------------------------- WCC --
+__device__ __forceinline__ uint32_t find_root(const uint32_t* parent, uint32_t v) {
+    uint32_t p = __ldcg(parent + v);
+    while (p != v) {
+        v = p;
+        p = __ldcg(parent + v);
+    }
+    return v;
+}
+
+struct WccOp {
+    uint32_t* parent;
+    uint8_t* touched;  // non-null on the first sweep
+    unsigned long long* changes;
+    struct Item {
+        uint32_t rb, cb;
+        uint32_t n;
+    };
+    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
+        c.rb = row << 16;
+        c.cb = col << 16;
+        c.n = 0;
+        return true;
+    }
+    __device__ void record(uint32_t r, Item& c) const {
+        const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
+        if (touched) {          // wcc.cpp:203-217: every record's ends get a label
+            touched[a] = 1;
+            touched[b] = 1;
+        }
+        const uint32_t ra = find_root(parent, a), rb = find_root(parent, b);
+        if (ra != rb) {         // wcc.cpp:218-231, 263-275: hook toward the smaller
+            const uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
+            if (atomicMin(parent + hi, lo) > lo) c.n += 1;
+        }
+    }
+    __device__ void end(uint32_t, uint32_t, Item& c) const { warp_add_u64(changes, c.n); }
+};
+
+// ----------------------------------------------------------------- k-core --
+struct KcoreOp {
+    int32_t* deg;
+    const uint32_t* removed;
+    const uint8_t* act;
+    struct Item {
+        uint32_t rb, cb;
+        bool fr, fc;
+    };
+    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
+        // kcore_mmap dispatch (gstore.cpp:2773-2782)
+        c.fr = act[row] != 0;
+        c.fc = act[col] != 0;
+        c.rb = row << 16;
+        c.cb = col << 16;
+        return c.fr || c.fc;
+    }
+    __device__ void record(uint32_t r, Item& c) const {
+        const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
+        if (c.fr && bit_of(removed, a)) atomicSub(deg + b, 1);  // kcore.cpp:77-78
+        if (c.fc && bit_of(removed, b)) atomicSub(deg + a, 1);  // kcore.cpp:90-91
+    }
+    __device__ void end(uint32_t, uint32_t, Item&) const {}
+};
+
+}  // namespace gsops

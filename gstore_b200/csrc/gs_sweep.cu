@@ -1,12 +1,13 @@
-// Tile-grid sweep kernels (sm_100a) and per-vertex finalize kernels for BFS,
-// PageRank, WCC and k-core.
+// Tile-grid sweep kernels (sm_100a) and per-vertex finalize kernels for
+// PageRank, WCC and k-core (BFS has its own sweep in gs_bfs.cu).
 //
-// Work decomposition: the records of every non-empty tile are cut into work
-// items of at most kItemRecords records (one tile each); a warp owns an item
-// at a time (grid-stride over items in file order, so the warps of one CTA
-// mostly work along one tile row).  Records stream with 128-bit evict-first
-// loads; the per-vertex state (bitmaps, depth, ranks, labels, degrees) is the
-// reused working set that stays in L2.
+// Work decomposition: the non-empty tiles are cut into units (<= kUnitRecords
+// records of one tile) and the units grouped into runs (units of one tile
+// row).  A CTA takes a run at a time, a warp a unit; records stream with
+// 128-bit evict-first loads and the per-vertex state (ranks, labels,
+// degrees) is the reused working set.  PageRank, WCC and k-core walk the
+// L2-blocked run order (tiles grouped by 64 x 64-window blocks), which keeps
+// that working set in L2.
 //
 // Reference semantics per record (edge_t{v0, v1} in tile (i, j)):
 //   BFS     bfs.cpp:138-185     discover the unvisited end of a frontier end
@@ -14,28 +15,19 @@
 //   WCC     wcc.cpp:177-278     hook the larger root onto the smaller one
 //   k-core  kcore.cpp:63-177    --deg[other] for every removed endpoint
 #include "gs_internal.cuh"
+#include "gs_ops.cuh"
 
 namespace {
 
 constexpr int kThreads = 256;
-constexpr unsigned kFull = 0xFFFFFFFFu;
-
-__device__ __forceinline__ uint32_t bit_of(const uint32_t* __restrict__ bm, uint32_t v) {
-    return (__ldg(bm + (v >> 5)) >> (v & 31)) & 1u;
-}
-
-__device__ __forceinline__ uint4 load_stream(const uint4* p) { return __ldcs(p); }
+using namespace gsops;
 
 // Generic run sweep.  A CTA takes one run at a time (consecutive tiles of one
 // tile row inside a group), its warps take the run's units (tile slices of at
 // most kUnitRecords records) and stream their records with 128-bit
 // evict-first loads.  When `seg` lists runs, only those are swept and their
 // units are read from a segment buffer (file record r at rec[r + delta]).
-// Op provides:
-//   struct Item;                                    per-unit warp-uniform context
-//   bool begin(uint32_t row, uint32_t col, Item&)   false = skip the unit
-//   void record(uint32_t rec, Item&)                one record, any lane
-//   void end(uint32_t row, uint32_t col, Item&)     warp-collective epilogue
+// Op is one of the per-record operations of gs_ops.cuh.
 template <class Op>
 __global__ void __launch_bounds__(kThreads) sweep_runs(const gs_tile_run* __restrict__ runs, uint64_t n_runs,
                                                        const gs_unit* __restrict__ units,
@@ -55,38 +47,7 @@ __global__ void __launch_bounds__(kThreads) sweep_runs(const gs_tile_run* __rest
             ub = runs[i].unit_beg;
             ue = runs[i].unit_end;
         }
-        for (uint32_t ui = ub + warp; ui < ue; ui += kWarps) {
-            const gs_unit d = units[ui];
-            const uint32_t row = d.rc >> 16, col = d.rc & 0xFFFFu;
-            typename Op::Item ic;
-            if (!op.begin(row, col, ic)) continue;
-            const uint64_t b = d.rec_beg, e = d.rec_beg + d.n;
-            uint64_t ab = (b + 3) & ~3ull;
-            if (ab > e) ab = e;
-            uint64_t ae = e & ~3ull;
-            if (ae < ab) ae = ab;
-            if (b + lane < ab) op.record(__ldcs(base + b + lane), ic);
-            if (ae + lane < e) op.record(__ldcs(base + ae + lane), ic);
-            const uint4* r4 = reinterpret_cast<const uint4*>(base + ab);
-            const uint32_t n4 = (uint32_t)((ae - ab) >> 2);
-            for (uint32_t k = lane; k < n4; k += 2 * 32) {
-                const uint4 q0 = load_stream(r4 + k);
-                const bool two = k + 32 < n4;
-                uint4 q1 = make_uint4(0, 0, 0, 0);
-                if (two) q1 = load_stream(r4 + k + 32);
-                op.record(q0.x, ic);
-                op.record(q0.y, ic);
-                op.record(q0.z, ic);
-                op.record(q0.w, ic);
-                if (two) {
-                    op.record(q1.x, ic);
-                    op.record(q1.y, ic);
-                    op.record(q1.z, ic);
-                    op.record(q1.w, ic);
-                }
-            }
-            op.end(row, col, ic);
-        }
+        for (uint32_t ui = ub + warp; ui < ue; ui += kWarps) sweep_unit(units[ui], base, op, lane);
     }
 }
 
@@ -113,12 +74,6 @@ gs_status launch_sweep(gs_graph* g, const Op& op, int algo, uint64_t bytes, bool
 inline uint32_t blocks_for(uint64_t n, const gs_ctx* ctx) {
     uint64_t b = (n + kThreads - 1) / kThreads;
     return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(b, gs_grid_size(ctx, 16)));
-}
-
-__device__ __forceinline__ void warp_add_u64(unsigned long long* dst, uint64_t v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-    if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, (unsigned long long)v);
 }
 
 // ---------------------------------------------------------- validation --
@@ -188,27 +143,6 @@ struct ComponentEdgesOp {
     __device__ void end(uint32_t, uint32_t, Item& c) const { warp_add_u64(out, c.n); }
 };
 
-// --------------------------------------------------------------- PageRank --
-struct PrOp {
-    const float* x;
-    float* y;
-    int directed;
-    struct Item {
-        uint32_t rb, cb;
-    };
-    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
-        c.rb = row << 16;
-        c.cb = col << 16;
-        return true;
-    }
-    __device__ void record(uint32_t r, Item& c) const {
-        const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
-        atomicAdd(y + b, __ldg(x + a));                 // pr.cpp:145-146
-        if (!directed) atomicAdd(y + a, __ldg(x + b));  // pr.cpp:147-150
-    }
-    __device__ void end(uint32_t, uint32_t, Item&) const {}
-};
-
 __global__ void pr_init_kernel(float* x, float* y, uint64_t N, uint64_t V) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
@@ -238,45 +172,6 @@ __global__ void pr_finalize_kernel(float* __restrict__ x, float* __restrict__ y,
         y[v] = 0.f;
     }
 }
-
-// -------------------------------------------------------------------- WCC --
-__device__ __forceinline__ uint32_t find_root(const uint32_t* parent, uint32_t v) {
-    uint32_t p = __ldcg(parent + v);
-    while (p != v) {
-        v = p;
-        p = __ldcg(parent + v);
-    }
-    return v;
-}
-
-struct WccOp {
-    uint32_t* parent;
-    uint8_t* touched;  // non-null on the first sweep
-    unsigned long long* changes;
-    struct Item {
-        uint32_t rb, cb;
-        uint32_t n;
-    };
-    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
-        c.rb = row << 16;
-        c.cb = col << 16;
-        c.n = 0;
-        return true;
-    }
-    __device__ void record(uint32_t r, Item& c) const {
-        const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
-        if (touched) {          // wcc.cpp:203-217: every record's ends get a label
-            touched[a] = 1;
-            touched[b] = 1;
-        }
-        const uint32_t ra = find_root(parent, a), rb = find_root(parent, b);
-        if (ra != rb) {         // wcc.cpp:218-231, 263-275: hook toward the smaller
-            const uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
-            if (atomicMin(parent + hi, lo) > lo) c.n += 1;
-        }
-    }
-    __device__ void end(uint32_t, uint32_t, Item& c) const { warp_add_u64(changes, c.n); }
-};
 
 __global__ void iota_kernel(uint32_t* parent, uint64_t N) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -310,31 +205,6 @@ __global__ void wcc_label_kernel(const uint32_t* parent, const uint8_t* touched,
     }
     warp_add_u64(count, local);
 }
-
-// ----------------------------------------------------------------- k-core --
-struct KcoreOp {
-    int32_t* deg;
-    const uint32_t* removed;
-    const uint8_t* act;
-    struct Item {
-        uint32_t rb, cb;
-        bool fr, fc;
-    };
-    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
-        // kcore_mmap dispatch (gstore.cpp:2773-2782)
-        c.fr = act[row] != 0;
-        c.fc = act[col] != 0;
-        c.rb = row << 16;
-        c.cb = col << 16;
-        return c.fr || c.fc;
-    }
-    __device__ void record(uint32_t r, Item& c) const {
-        const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
-        if (c.fr && bit_of(removed, a)) atomicSub(deg + b, 1);  // kcore.cpp:77-78
-        if (c.fc && bit_of(removed, b)) atomicSub(deg + a, 1);  // kcore.cpp:90-91
-    }
-    __device__ void end(uint32_t, uint32_t, Item&) const {}
-};
 
 // One warp per 32-vertex word (kcore.cpp:186-209): remove 0 < (int16)deg < k.
 __global__ void kcore_round_kernel(int32_t* __restrict__ deg, uint32_t* __restrict__ removed,

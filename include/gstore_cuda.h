@@ -59,6 +59,7 @@ typedef enum gs_algo {
 typedef struct gs_ctx gs_ctx;
 typedef struct gs_graph gs_graph;
 typedef struct gs_state gs_state;
+typedef struct gs_batch gs_batch;
 
 /* A run of consecutive stored tiles, mirroring part_meta_t (gstore.h:563-568):
  * part ids use the reference's encoding (group_full_index << 16 | i << 8 | j,
@@ -186,6 +187,34 @@ gs_status gs_bfs_stats(gs_state* s, uint64_t* edges_in_component, uint64_t* swep
  * and race: issue them one after another.  levels_out (may be NULL): sweeps
  * done. */
 gs_status gs_bfs_noalloc(gs_graph* g, uint64_t root, uint8_t* d_depth, int64_t* levels_out);
+
+/* ------------------------------------------------------------ batching --- */
+/* Replaces: one gstoreu process per query (the job dispatch of
+ * gstore.cpp:250-333 runs a single BFS / WCC / k-core / PageRank).  A batch
+ * collects queries on resident graphs of one context and runs them with few
+ * launches: BFS roots on the same graph run as a multi-source BFS (one bit
+ * per query in 32- or 64-bit frontier words, one persistent launch per
+ * group, word width and tile order picked per graph by a measuring
+ * autotuner); all WCC and k-core queries, over any graphs, share one
+ * persistent launch; PageRank queries run as plain gs_run.  Results per
+ * query equal gs_run's on the same graph and argument (BFS depth, WCC
+ * labels, k-core degrees bit for bit).  arg: BFS root, k-core k, PageRank
+ * iterations (ignored for WCC).  gs_batch_run runs every query added since
+ * the last run; query ids stay valid until gs_batch_free. */
+gs_status gs_batch_create(gs_ctx* ctx, gs_batch** out);
+gs_status gs_batch_add(gs_batch* b, gs_graph* g, gs_algo algo, int64_t arg, int* query_id);
+gs_status gs_batch_run(gs_batch* b);
+/* Same formats as gs_download / gs_result_count; a query that failed
+ * returns its status (e.g. GS_ERR_RANGE for a BFS over 254 levels). */
+gs_status gs_batch_download(gs_batch* b, int query_id, int what, void* host_dst, uint64_t bytes);
+gs_status gs_batch_result_count(gs_batch* b, int query_id, uint64_t* count);
+/* BFS query: vertices found per level (iteration_finalize's frontier
+ * counts; the last level found none). */
+gs_status gs_batch_bfs_levels(gs_batch* b, int query_id, uint64_t* level_counts, int max_levels,
+                              int* n_levels);
+/* Persistent launches made and their device time so far. */
+gs_status gs_batch_stats(const gs_batch* b, uint64_t* launches, double* kernel_ms);
+gs_status gs_batch_free(gs_batch* b);
 
 /* PageRank with the reference's int32 inverse-degree truncation
  * (pr.cpp:112-114) instead of the real inverse; must precede gs_run. */
