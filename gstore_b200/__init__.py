@@ -44,6 +44,8 @@ ABI_SYMBOLS = [
     "gs_bfs_noalloc", "gs_upload_graph_streamed", "gs_stream_stats",
     "gs_batch_create", "gs_batch_add", "gs_batch_run", "gs_batch_download", "gs_batch_result_count",
     "gs_batch_bfs_levels", "gs_batch_stats", "gs_batch_free",
+    "gs_serve_create", "gs_serve_add_graph", "gs_serve_submit", "gs_serve_step", "gs_serve_poll",
+    "gs_serve_result", "gs_serve_clock", "gs_serve_stats", "gs_serve_free",
 ]
 
 
@@ -105,6 +107,16 @@ def lib():
             "gs_batch_bfs_levels": [vp, i32, vp, i32, C.POINTER(C.c_int)],
             "gs_batch_stats": [vp, pu64, C.POINTER(C.c_double)],
             "gs_batch_free": [vp],
+            "gs_serve_create": [vp, u64, pvp],
+            "gs_serve_add_graph": [vp, vp, C.POINTER(C.c_int)],
+            "gs_serve_submit": [vp, i32, i32, i64, pu64],
+            "gs_serve_step": [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+            "gs_serve_poll": [vp, u64, C.POINTER(C.c_int)],
+            "gs_serve_result": [vp, u64, vp, u64, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                C.POINTER(C.c_int64)],
+            "gs_serve_clock": [vp, C.POINTER(C.c_double)],
+            "gs_serve_stats": [vp, pu64, pu64, pu64, pu64],
+            "gs_serve_free": [vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -176,7 +188,7 @@ class Context:
         (gs_destroy does not free graphs, states or batches)."""
         if self._h:
             kids = list(self._children)
-            for kind in (State, Batch, Graph):
+            for kind in (State, Batch, Server, Graph):
                 for k in kids:
                     if isinstance(k, kind):
                         k.free()
@@ -315,6 +327,84 @@ class Batch:
     def free(self):
         if self._h:
             lib().gs_batch_free(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Server:
+    """Request loop over resident graphs (gs_serve_*): continuous batching of
+    BFS / WCC / k-core / PageRank requests, admitted by HBM footprint."""
+
+    QUEUED, RUNNING, DONE, FAILED = 0, 1, 2, 3
+
+    def __init__(self, ctx: Context, state_budget: int = 0):
+        self.ctx = ctx
+        self._h = C.c_void_p()
+        ctx._check(lib().gs_serve_create(ctx._h, state_budget, C.byref(self._h)))
+        self._graphs = []
+        self._req = {}
+        ctx._children.add(self)
+
+    def add_graph(self, graph: "Graph") -> int:
+        gid = C.c_int()
+        self.ctx._check(lib().gs_serve_add_graph(self._h, graph._h, C.byref(gid)))
+        self._graphs.append(graph)
+        return gid.value
+
+    def submit(self, gid: int, algo, arg: int = 0) -> int:
+        a = ALGOS[algo] if isinstance(algo, str) else int(algo)
+        rid = C.c_uint64()
+        self.ctx._check(lib().gs_serve_submit(self._h, gid, a, arg, C.byref(rid)))
+        self._req[rid.value] = (gid, a)
+        return rid.value
+
+    def step(self):
+        """One serving step; returns (running, queued)."""
+        na, nq = C.c_int(), C.c_int()
+        self.ctx._check(lib().gs_serve_step(self._h, C.byref(na), C.byref(nq)))
+        return na.value, nq.value
+
+    def poll(self, rid: int) -> int:
+        st = C.c_int()
+        self.ctx._check(lib().gs_serve_poll(self._h, rid, C.byref(st)))
+        return st.value
+
+    def result(self, rid: int, want_data: bool = True):
+        """(result array or None, t_submit, t_done, steps); forgets the request."""
+        gid, a = self._req.pop(rid)
+        V = self._graphs[gid].V
+        dt = {GS_ALGO_BFS: np.uint8, GS_ALGO_PAGERANK: np.float32, GS_ALGO_KCORE: np.int32,
+              GS_ALGO_WCC: np.uint32}[a]
+        out = np.empty(V, dt) if want_data else None
+        ts, td, n = C.c_double(), C.c_double(), C.c_int64()
+        self.ctx._check(lib().gs_serve_result(self._h, rid, _ptr(out), 0 if out is None else out.nbytes,
+                                              C.byref(ts), C.byref(td), C.byref(n)))
+        return out, ts.value, td.value, n.value
+
+    def clock(self) -> float:
+        t = C.c_double()
+        self.ctx._check(lib().gs_serve_clock(self._h, C.byref(t)))
+        return t.value
+
+    def stats(self):
+        a, b, c, d = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+        self.ctx._check(lib().gs_serve_stats(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
+        return {"steps": a.value, "graph_launches": b.value, "kernel_launches": c.value, "hbm_in_use": d.value}
+
+    def free(self):
+        if self._h:
+            lib().gs_serve_free(self._h)
             self._h = None
 
     def __enter__(self):

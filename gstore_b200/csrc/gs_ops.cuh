@@ -151,4 +151,92 @@ struct KcoreOp {
     __device__ void end(uint32_t, uint32_t, Item&) const {}
 };
 
+// ----------------------------------------------- multi-source BFS words --
+// Per vertex {frontier, visited} words of a multi-source BFS, one bit per
+// query (W = 32 or 64 queries).
+template <class W>
+struct FvPair;
+template <>
+struct alignas(8) FvPair<uint32_t> {
+    uint32_t f, vis;
+};
+template <>
+struct alignas(16) FvPair<unsigned long long> {
+    unsigned long long f, vis;
+};
+
+__device__ __forceinline__ FvPair<uint32_t> load_fv(const FvPair<uint32_t>* p) {
+    const uint2 x = __ldcg(reinterpret_cast<const uint2*>(p));
+    return FvPair<uint32_t>{x.x, x.y};
+}
+__device__ __forceinline__ FvPair<unsigned long long> load_fv(const FvPair<unsigned long long>* p) {
+    const ulonglong2 x = __ldcg(reinterpret_cast<const ulonglong2*>(p));
+    return FvPair<unsigned long long>{x.x, x.y};
+}
+__device__ __forceinline__ void store_fv(FvPair<uint32_t>* p, uint32_t f, uint32_t vis) {
+    __stcg(reinterpret_cast<uint2*>(p), make_uint2(f, vis));
+}
+__device__ __forceinline__ void store_fv(FvPair<unsigned long long>* p, unsigned long long f,
+                                         unsigned long long vis) {
+    ulonglong2 x;
+    x.x = f;
+    x.y = vis;
+    __stcg(reinterpret_cast<ulonglong2*>(p), x);
+}
+__device__ __forceinline__ int popc_w(uint32_t x) { return __popc(x); }
+__device__ __forceinline__ int popc_w(unsigned long long x) { return __popcll(x); }
+__device__ __forceinline__ int ffs_w(uint32_t x) { return __ffs(x); }
+__device__ __forceinline__ int ffs_w(unsigned long long x) { return __ffsll((long long)x); }
+
+template <class W>
+struct MsOp {
+    FvPair<W>* fv;
+    W* next;
+    int directed;
+    struct Item {
+        uint32_t rb, cb;
+    };
+    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
+        c.rb = row << 16;
+        c.cb = col << 16;
+        return true;
+    }
+    __device__ void record(uint32_t r, Item& c) const {
+        const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
+        const FvPair<W> sa = load_fv(fv + a), sb = load_fv(fv + b);
+        const W nb = sa.f & ~sb.vis;
+        if (nb) atomicOr(next + b, nb);
+        if (!directed) {            // the half grid stores each edge once
+            const W na = sb.f & ~sa.vis;
+            if (na) atomicOr(next + a, na);
+        }
+    }
+    __device__ void end(uint32_t, uint32_t, Item&) const {}
+};
+
+// KcoreOp for a persistent kernel: the removed bits and window flags change
+// between phases, so they are read through L2 (never the non-coherent path).
+struct KcoreOpL2 {
+    int32_t* deg;
+    const uint32_t* removed;
+    const uint8_t* act;
+    struct Item {
+        uint32_t rb, cb;
+        bool fr, fc;
+    };
+    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
+        c.fr = __ldcg(act + row) != 0;     // gstore.cpp:2773-2782
+        c.fc = __ldcg(act + col) != 0;
+        c.rb = row << 16;
+        c.cb = col << 16;
+        return c.fr || c.fc;
+    }
+    __device__ void record(uint32_t r, Item& c) const {
+        const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
+        if (c.fr && (__ldcg(removed + (a >> 5)) >> (a & 31) & 1u)) atomicSub(deg + b, 1);  // kcore.cpp:77-78
+        if (c.fc && (__ldcg(removed + (b >> 5)) >> (b & 31) & 1u)) atomicSub(deg + a, 1);  // kcore.cpp:90-91
+    }
+    __device__ void end(uint32_t, uint32_t, Item&) const {}
+};
+
 }  // namespace gsops

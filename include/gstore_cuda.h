@@ -60,6 +60,7 @@ typedef struct gs_ctx gs_ctx;
 typedef struct gs_graph gs_graph;
 typedef struct gs_state gs_state;
 typedef struct gs_batch gs_batch;
+typedef struct gs_server gs_server;
 
 /* A run of consecutive stored tiles, mirroring part_meta_t (gstore.h:563-568):
  * part ids use the reference's encoding (group_full_index << 16 | i << 8 | j,
@@ -215,6 +216,35 @@ gs_status gs_batch_bfs_levels(gs_batch* b, int query_id, uint64_t* level_counts,
 /* Persistent launches made and their device time so far. */
 gs_status gs_batch_stats(const gs_batch* b, uint64_t* launches, double* kernel_ms);
 gs_status gs_batch_free(gs_batch* b);
+
+/* ------------------------------------------------------------- serving --- */
+/* Replaces: one gstoreu process per query (gstore.cpp:250-333), as a
+ * request loop.  Graphs are registered resident graphs; requests (BFS root,
+ * k-core k, PageRank iterations, WCC) are queued by gs_serve_submit and
+ * advanced by gs_serve_step: each step admits queued requests in arrival
+ * order while their device state fits state_budget_bytes (0 = 32 GiB) and a
+ * slot is free (64 BFS requests per graph share bit-parallel frontier
+ * words), runs one iteration of every admitted request in one CUDA-graph
+ * launch (a sweep kernel and a post kernel over all of them), and retires
+ * finished ones into pinned host buffers.  A request identical to one
+ * queued or running (same graph, algorithm and argument) shares its run.
+ * Results equal gs_run's for the same query (BFS/WCC/k-core bit for bit,
+ * PageRank within float rounding).  Times are seconds of the server's
+ * steady clock (gs_serve_clock).  States: 0 queued, 1 running, 2 done,
+ * 3 failed. */
+gs_status gs_serve_create(gs_ctx* ctx, uint64_t state_budget_bytes, gs_server** out);
+gs_status gs_serve_add_graph(gs_server* s, gs_graph* g, int* graph_id);
+gs_status gs_serve_submit(gs_server* s, int graph_id, gs_algo algo, int64_t arg, uint64_t* request_id);
+gs_status gs_serve_step(gs_server* s, int* n_active, int* n_queued);
+gs_status gs_serve_poll(gs_server* s, uint64_t request_id, int* state);
+/* Copies a finished request's result (gs_download's format; host_dst may be
+ * NULL) and forgets the request.  A failed request returns its status. */
+gs_status gs_serve_result(gs_server* s, uint64_t request_id, void* host_dst, uint64_t bytes,
+                          double* t_submit, double* t_done, int64_t* steps);
+gs_status gs_serve_clock(const gs_server* s, double* seconds);
+gs_status gs_serve_stats(const gs_server* s, uint64_t* steps, uint64_t* graph_launches,
+                         uint64_t* kernel_launches, uint64_t* hbm_in_use);
+gs_status gs_serve_free(gs_server* s);
 
 /* PageRank with the reference's int32 inverse-degree truncation
  * (pr.cpp:112-114) instead of the real inverse; must precede gs_run. */
