@@ -60,6 +60,12 @@ def parse_args():
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-query measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop measurement")
+    ap.add_argument("--no-stream", action="store_true", help="skip the semi-external (streamed) measurement")
+    ap.add_argument("--serve-seconds", type=float, default=1.0, help="length of the Poisson arrival trace")
+    ap.add_argument("--stream-scale", type=int, default=28)
+    ap.add_argument("--stream-budget-gb", type=float, default=4.0)
     return ap.parse_args()
 
 
@@ -273,6 +279,267 @@ def run_reference_arm(args, dist: Dist):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------- workload builders --
+def make_graph(ctx, torch, scale: int, ef: int, seed1: int = 1, seed2: int = 2):
+    """Graph500 Kronecker graph generated and converted on the device."""
+    M = ef << scale
+    d_pairs = torch.empty(2 * M, dtype=torch.int32, device="cuda")
+    ctx.kron_generate_device(scale, ef, seed1, seed2, d_pairs.data_ptr())
+    g = ctx.convert(d_pairs.data_ptr(), 1 << scale, n_pairs=M)
+    del d_pairs
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return g
+
+
+def bench_batched(ctx, torch, gs):
+    """Batched queries: 64 seeded BFS roots on Kron 24 ef16 in one persistent
+    multi-source launch vs 64 sequential plain BFS runs; and 16 WCC + 16
+    k-core (k uniform 4..32) over 8 graphs of scale 18-22 (seeds 1..8)."""
+    out = {}
+    g = make_graph(ctx, torch, 24, 16)
+    roots = splitmix64_roots(g.degree(), 64, seed=1)
+    with g.state("bfs", roots[0]) as s:
+        s.run()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        plain = []
+        for r in roots:
+            s.reset(r)
+            s.run()
+            plain.append(s.count())
+        torch.cuda.synchronize()
+        t_plain = time.perf_counter() - t0
+    for _ in range(4):                   # the autotuner tries each configuration once
+        with gs.Batch(ctx) as b:
+            for r in roots:
+                b.add(g, "bfs", r)
+            b.run()
+    with gs.Batch(ctx) as b:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ids = [b.add(g, "bfs", r) for r in roots]
+        b.run()
+        torch.cuda.synchronize()
+        t_batch = time.perf_counter() - t0
+        st = b.stats()
+        same = all(b.count(q) == plain[i] for i, q in enumerate(ids))
+    out["msbfs"] = {"workload": "64 BFS roots (splitmix64 seed 1) on Kron 24 ef16",
+                    "plain_queries_per_s": 64 / t_plain, "batched_queries_per_s": 64 / t_batch,
+                    "speedup": t_plain / t_batch, "batched_kernel_ms": st["kernel_ms"],
+                    "launches": st["launches"], "reached_counts_equal": same,
+                    "plain": "gs_state_reset + gs_run per root (per-level sweep + finalize launches)"}
+    g.free()
+    graphs = [make_graph(ctx, torch, 18 + (i % 5), 16, seed1=i + 1) for i in range(8)]
+    rng = np.random.default_rng(1)
+    ks = [int(k) for k in rng.integers(4, 33, 16)]
+    qs = [(graphs[i % 8], "wcc", 0) for i in range(16)] + [(graphs[i % 8], "kcore", ks[i]) for i in range(16)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain = []
+    for gg, a, k in qs:
+        with gg.state(a, k) as s:
+            s.run()
+            plain.append(s.count())
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    with gs.Batch(ctx) as b:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ids = [b.add(gg, a, k) for gg, a, k in qs]
+        b.run()
+        torch.cuda.synchronize()
+        t_batch = time.perf_counter() - t0
+        st = b.stats()
+        same = all(b.count(q) == plain[i] for i, q in enumerate(ids))
+    out["wcc_kcore"] = {"workload": "16 WCC + 16 k-core (k in 4..32, seed 1) over 8 Kron graphs of scale 18-22",
+                        "plain_queries_per_s": 32 / t_plain, "batched_queries_per_s": 32 / t_batch,
+                        "speedup": t_plain / t_batch, "batched_kernel_ms": st["kernel_ms"],
+                        "launches": st["launches"], "result_counts_equal": same}
+    for gg in graphs:
+        gg.free()
+    return out
+
+
+def poisson_trace(graphs, seconds: float, rate: float, seed: int = 1):
+    """Seeded Poisson arrivals: 70% BFS (random non-isolated root), 15%
+    k-core (k uniform 4..32), 10% WCC, 5% PageRank (10 iterations)."""
+    rng = np.random.default_rng(seed)
+    nz = [np.nonzero(g.degree())[0] for g in graphs]
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > seconds:
+            return out
+        gi = int(rng.integers(0, len(graphs)))
+        u = rng.random()
+        if u < 0.70:
+            out.append((t, gi, "bfs", int(rng.choice(nz[gi]))))
+        elif u < 0.85:
+            out.append((t, gi, "kcore", int(rng.integers(4, 33))))
+        elif u < 0.95:
+            out.append((t, gi, "wcc", 0))
+        else:
+            out.append((t, gi, "pagerank", 10))
+
+
+def bench_served(ctx, torch, gs, seconds: float):
+    """Serving: Poisson arrivals (2000 req/s, seeded) against 16 resident
+    Kronecker graphs of scale 16-24 and edgefactor 8-32 (seeds 1..16); the
+    server (continuous batching) vs a one-request-at-a-time plain loop on the
+    same trace.  Latency = result on the host - scheduled arrival."""
+    graphs = [make_graph(ctx, torch, 16 + (i % 9), (8, 16, 32)[i % 3], seed1=i + 1) for i in range(16)]
+    trace = poisson_trace(graphs, seconds, 2000.0)
+    res = {"workload": f"{len(trace)} requests, Poisson 2000/s for {seconds:g} s (seed 1), "
+                       "70% BFS / 15% k-core / 10% WCC / 5% PageRank(10) over 16 Kron graphs "
+                       "(scale 16-24, ef 8/16/32, seeds 1..16)",
+           "graphs_records": int(sum(g.n_edges for g in graphs))}
+
+    def summarize(lat, makespan, n):
+        lat = np.asarray(lat)
+        return {"requests": n, "throughput_req_per_s": n / makespan, "makespan_s": makespan,
+                "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                "mean_ms": float(lat.mean() * 1e3)}
+
+    # server
+    with gs.Server(ctx) as srv:
+        gids = [srv.add_graph(g) for g in graphs]
+        # warm-up: one request of each kind
+        for k in ("bfs", "wcc", "kcore", "pagerank"):
+            srv.submit(gids[0], k, 1 if k in ("bfs", "pagerank") else 8 if k == "kcore" else 0)
+        while srv.step() != (0, 0):
+            pass
+        torch.cuda.synchronize()
+        base = srv.clock()
+        ids, i = [], 0
+        while True:
+            now = srv.clock() - base
+            while i < len(trace) and trace[i][0] <= now:
+                t, gi, a, arg = trace[i]
+                ids.append(srv.submit(gids[gi], a, arg))
+                i += 1
+            na, nq = srv.step()
+            if i == len(trace) and na == 0 and nq == 0:
+                break
+            if na == 0 and nq == 0 and i < len(trace):
+                time.sleep(max(0.0, min(0.0005, trace[i][0] - (srv.clock() - base))))
+        lat, results, t_end = [], {}, 0.0
+        for k, rid in enumerate(ids):
+            keep = k % 97 == 0
+            data, t_sub, t_done, _ = srv.result(rid, want_data=keep)
+            lat.append(t_done - base - trace[k][0])
+            t_end = max(t_end, t_done - base)
+            if keep:
+                results[k] = data
+        st = srv.stats()
+        res["served"] = summarize(lat, t_end, len(ids))
+        res["served"].update({"steps": st["steps"], "graph_launches": st["graph_launches"],
+                              "kernel_launches": st["kernel_launches"]})
+    # plain one-at-a-time loop on the same trace (bounded: at most 120 s)
+    lat, t0, n_done, same, checked = [], time.perf_counter(), 0, 0, 0
+    for k, (t, gi, a, arg) in enumerate(trace):
+        now = time.perf_counter() - t0
+        if now < t:
+            time.sleep(t - now)
+        g = graphs[gi]
+        with g.state(a, arg) as s:
+            s.run()
+            data = s.download(0)
+        torch.cuda.synchronize()
+        done = time.perf_counter() - t0
+        lat.append(done - t)
+        n_done += 1
+        if k in results:
+            checked += 1
+            if a == "pagerank":
+                ok = np.abs(data.astype(np.float64) - results[k]).sum() <= 1e-6 * np.abs(data.astype(np.float64)).sum()
+            else:
+                ok = np.array_equal(data, results[k])
+            same += int(ok)
+        if done > 120.0:
+            break
+    res["plain"] = summarize(lat, time.perf_counter() - t0, n_done)
+    res["plain"]["note"] = "gs_state_create + gs_run + gs_download per request, in arrival order"
+    res["throughput_ratio"] = res["served"]["throughput_req_per_s"] / res["plain"]["throughput_req_per_s"]
+    res["results_checked_equal"] = f"{same}/{checked}"
+    for g in graphs:
+        g.free()
+    return res
+
+
+def bench_streamed(args, torch, gs, dev):
+    """Semi-external: Kron `stream_scale` ef16 with the HBM tile budget capped
+    (default 4 GB: two 2 GB segments); records stream from pinned host memory
+    over PCIe, overlapped with the sweeps.  PageRank 10 iterations and one
+    BFS; PCIe roofline = copied bytes / time over the measured pinned H2D
+    rate."""
+    scale = args.stream_scale
+    V = 1 << scale
+    budget = int(args.stream_budget_gb * (1 << 30))
+    ctx = gs.Context(dev)
+    g = make_graph(ctx, torch, scale, 16)
+    E = g.n_edges
+    h_grid = torch.empty(E, dtype=torch.int32, pin_memory=True)
+    h_start = np.empty(gs.geometry(V)[2], np.uint64)
+    h_deg = np.empty(V, np.int32)
+    gs.lib().gs_graph_download(g._h, h_start.ctypes.data, h_grid.data_ptr(), h_deg.ctypes.data)
+    g.free()
+    ctx.close()
+    torch.cuda.empty_cache()
+    # measured pinned H2D rate (1 GiB)
+    d = torch.empty(min(1 << 28, E), dtype=torch.int32, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    rates = []
+    for _ in range(3):
+        e0.record()
+        d.copy_(h_grid[: d.numel()], non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        rates.append(d.numel() * 4 / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del d
+    torch.cuda.empty_cache()
+    h2d = max(rates)
+    ctx = gs.Context(dev, hbm_budget=budget)
+    sg = ctx.upload(h_start, h_grid.numpy().view(np.uint32), h_deg, V)
+    out = {"workload": f"Kron {scale} ef16 ({E} records, {E * 4 / 1e9:.1f} GB) with a {args.stream_budget_gb:g} GB "
+                       "HBM tile budget (two segments of half the budget), records in pinned host memory",
+           "pinned_h2d_GBps": h2d}
+    st0 = sg.stream_stats()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with sg.state("pagerank", 10) as s:
+        s.run()
+    torch.cuda.synchronize()
+    t_pr = time.perf_counter() - t0
+    st1 = sg.stream_stats()
+    pr_bytes = st1["bytes"] - st0["bytes"]
+    out["pagerank"] = {"iterations": 10, "ms_per_iter": t_pr / 10 * 1e3,
+                       "edges_per_s_per_iter": E / (t_pr / 10), "pcie_bytes": pr_bytes,
+                       "pcie_GBps": pr_bytes / t_pr / 1e9, "pcie_roofline_frac": pr_bytes / t_pr / 1e9 / h2d,
+                       "segments": st1["segments"] - st0["segments"], "segments_reused": st1["reused"] - st0["reused"]}
+    root = splitmix64_roots(h_deg, 1, seed=1)[0]
+    with sg.state("bfs", root) as s:
+        s.run()                                     # warm-up of the plan
+        s.reset(root)
+        st0 = sg.stream_stats()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.run()
+        torch.cuda.synchronize()
+        t_bfs = time.perf_counter() - t0
+        st1 = sg.stream_stats()
+        stats = s.bfs_stats()
+    b = st1["bytes"] - st0["bytes"]
+    out["bfs"] = {"root": root, "levels": int(stats["level_counts"].size), "ms": t_bfs * 1e3,
+                  "gteps": stats["edges_in_component"] / t_bfs / 1e9,
+                  "edges_in_component": stats["edges_in_component"], "pcie_bytes": b,
+                  "pcie_GBps": b / t_bfs / 1e9, "pcie_roofline_frac": b / t_bfs / 1e9 / h2d}
+    sg.free()
+    ctx.close()
+    del h_grid
+    return out
+
+
 # ------------------------------------------------------------------ our arm --
 def main():
     args = parse_args()
@@ -437,6 +704,18 @@ def main():
                        "what": "per step: gs_upload_graph from pinned host tile arrays, BFS, depth download"}
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
+    # ------------------------------------- batched / served / streamed forms
+    if dist.world == 1 and not args.no_secondary:
+        graph.free()
+        torch.cuda.empty_cache()
+        sec = line.setdefault("secondary", {})
+        if not args.no_batch:
+            sec["batched"] = bench_batched(ctx, torch, gs)
+        if not args.no_serve:
+            sec["served"] = bench_served(ctx, torch, gs, args.serve_seconds)
+        if not args.no_stream:
+            ctx.set_stream(None)
+            sec["streamed"] = bench_streamed(args, torch, gs, dev)
     if dist.rank == 0:
         print(json.dumps(line), flush=True)
     graph.free()

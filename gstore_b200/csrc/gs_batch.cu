@@ -22,6 +22,9 @@
 // decrement sweeps (kcore.cpp:63-177), WCC hooking sweeps (wcc.cpp:177-278)
 // and pointer jumping (wcc.cpp:372-390).
 //
+// Identical queries of one run (same graph, algorithm and argument) run
+// once and share the result.
+//
 // Persistent launches are cooperative (every CTA resident); phases are
 // separated by a grid barrier whose wait is bounded by kBarrierNs: a CTA that
 // waits longer sets the error flag and every CTA returns.
@@ -362,6 +365,7 @@ struct gs_batch_query {
     bool ran = false;
     int group = -1;          // BFS: group index, bit = lane
     int lane = 0;
+    int leader = -1;         // an identical query of the same run answers this one
     int64_t sweeps = 0;
     // WCC / k-core state
     uint32_t* parent = nullptr;
@@ -659,6 +663,7 @@ void free_query(gs_batch_query& q) {
 
 gs_status query_of(gs_batch* b, int id, gs_batch_query** out) {
     if (!b || id < 0 || (size_t)id >= b->q.size()) return GS_ERR_ARG;
+    if (b->q[id].leader >= 0) id = b->q[id].leader;
     gs_batch_query& q = b->q[id];
     if (!q.ran) return gs_fail(b->ctx, GS_ERR_STATE, "query has not run (call gs_batch_run)");
     if (q.status != GS_OK) return gs_fail(b->ctx, q.status, "query failed");
@@ -707,6 +712,16 @@ gs_status gs_batch_run(gs_batch* b) {
     if (!b) return GS_ERR_ARG;
     std::vector<int> bfs, wk, pr;
     for (size_t i = b->first_new; i < b->q.size(); ++i) {
+        // identical queries (graph, algorithm, argument) run once
+        gs_batch_query& qi = b->q[i];
+        for (size_t j = b->first_new; j < i; ++j) {
+            const gs_batch_query& qj = b->q[j];
+            if (qj.leader < 0 && qj.g == qi.g && qj.algo == qi.algo && (qi.algo == GS_ALGO_WCC || qj.arg == qi.arg)) {
+                qi.leader = (int)j;
+                break;
+            }
+        }
+        if (qi.leader >= 0) continue;
         switch (b->q[i].algo) {
             case GS_ALGO_BFS: bfs.push_back((int)i); break;
             case GS_ALGO_WCC:

@@ -197,7 +197,8 @@ gs_status gs_bfs_noalloc(gs_graph* g, uint64_t root, uint8_t* d_depth, int64_t* 
  * per query in 32- or 64-bit frontier words, one persistent launch per
  * group, word width and tile order picked per graph by a measuring
  * autotuner); all WCC and k-core queries, over any graphs, share one
- * persistent launch; PageRank queries run as plain gs_run.  Results per
+ * persistent launch; PageRank queries run as plain gs_run; identical queries
+ * (same graph, algorithm and argument) run once.  Results per
  * query equal gs_run's on the same graph and argument (BFS depth, WCC
  * labels, k-core degrees bit for bit).  arg: BFS root, k-core k, PageRank
  * iterations (ignored for WCC).  gs_batch_run runs every query added since
