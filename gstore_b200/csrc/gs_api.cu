@@ -159,6 +159,7 @@ gs_status gs_kernel_time(gs_ctx* ctx, int algo, uint64_t* launches, double* tota
 // ------------------------------------------------------------------ graph --
 static void free_graph_arrays(gs_graph* g) {
     gs_stream_close(g);
+    pr_layout_free(g);
     gs_dev_free(g->d_rec);
     gs_dev_free(g->d_items);
     gs_dev_free(g->d_tile_off);

@@ -77,6 +77,25 @@ struct SegView {
     const uint32_t* buf = nullptr;
 };
 
+// PageRank row-slice layout (gs_pagerank.cu): a second copy of the records,
+// each tile's records grouped by row slice (v0 >> 13, 8 slices of 8192
+// vertices) and sorted by v1 inside a slice; work items are (row window,
+// slice, block of kPrColBlock column windows), their units <= kUnitRecords
+// records of one tile and slice.
+constexpr int kPrSliceBits = 13;
+constexpr uint32_t kPrColBlock = 32;
+struct gs_pr_item {
+    uint32_t unit_beg, unit_end;
+    uint32_t row, slice;
+};
+struct gs_pr_layout {
+    uint32_t* d_rec = nullptr;
+    gs_unit* d_units = nullptr;
+    gs_pr_item* d_items = nullptr;
+    uint64_t n_units = 0, n_items = 0;
+    bool built = false;
+};
+
 struct gs_streamer;   // pinned-host record stream of a graph (gs_stream.cu)
 struct gs_seglists;   // double-buffered entry lists of segment sweeps (gs_stream.cu)
 
@@ -125,6 +144,7 @@ struct gs_graph {
     uint32_t* d_tile_rc = nullptr;    // T packed (row << 16 | col)
     int32_t* d_degree = nullptr;      // N
     SegView seg;                      // set during segment sweeps
+    gs_pr_layout pr;                  // built at the first PageRank on a resident graph
     gs_streamer* stream = nullptr;    // non-null: records stay in host memory
     gs_seglists* lists = nullptr;     // segment entry lists of segment sweeps
     std::vector<gs_tile_run> h_runs;  // host copies of the run and unit tables
@@ -216,6 +236,12 @@ gs_status bfs_sweep_launch(gs_state* s);
 gs_status bfs_finalize(gs_state* s, int64_t* frontier, int* done);
 
 gs_status pr_init(gs_state* s);
+gs_status pr_layout_build(gs_graph* g);
+void pr_layout_free(gs_graph* g);
+gs_status pr_slice_launch(gs_state* s);
+gs_status pr_slice_sweep(gs_graph* g, cudaStream_t stream, const float* x, float* y, int* error);
+gs_status pr_finalize_launch(gs_ctx* ctx, cudaStream_t stream, float* x, float* y, float* r, const int32_t* deg,
+                             uint64_t N, uint64_t V, int compat);
 gs_status pr_sweep_launch(gs_state* s);
 gs_status pr_finalize(gs_state* s, int64_t* frontier, int* done);
 

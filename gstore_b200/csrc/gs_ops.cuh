@@ -71,20 +71,37 @@ struct PrOp {
     const float* x;
     float* y;
     int directed;
+    // Tiles sorted by v1 (the device converter's order) give runs of equal
+    // column ends per lane: one add to y per run (fewer atomics, shorter
+    // FP32 accumulation chains); any order stays correct.
     struct Item {
         uint32_t rb, cb;
+        uint32_t pb;     // column end of the open run, ~0 = none
+        float xb;        // x[pb]
+        float sum;       // sum of x[a] over the open run
     };
     __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
         c.rb = row << 16;
         c.cb = col << 16;
+        c.pb = ~0u;
+        c.xb = 0.f;
+        c.sum = 0.f;
         return true;
     }
     __device__ void record(uint32_t r, Item& c) const {
         const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
-        atomicAdd(y + b, __ldg(x + a));                 // pr.cpp:145-146
-        if (!directed) atomicAdd(y + a, __ldg(x + b));  // pr.cpp:147-150
+        if (b != c.pb) {
+            if (c.pb != ~0u) atomicAdd(y + c.pb, c.sum);   // pr.cpp:145-146
+            c.pb = b;
+            c.sum = 0.f;
+            if (!directed) c.xb = __ldg(x + b);
+        }
+        c.sum += __ldg(x + a);
+        if (!directed) atomicAdd(y + a, c.xb);             // pr.cpp:147-150
     }
-    __device__ void end(uint32_t, uint32_t, Item&) const {}
+    __device__ void end(uint32_t, uint32_t, Item& c) const {
+        if (c.pb != ~0u) atomicAdd(y + c.pb, c.sum);
+    }
 };
 
 // -------------------------------------------------------------------- WCC --

@@ -23,9 +23,10 @@
 //   k-core  post = round (kcore.cpp:179-217; the first step is a round
 //           only, as kcore_mmap starts with iteration_finalize), sweep =
 //           decrements (kcore.cpp:63-177); done when a round removes nothing
-//   PR      sweep = pagerank_onepart (pr.cpp:119-154), post = the
-//           iteration_finalize update (pr.cpp:229-303); done after `arg`
-//           iterations
+//   PR      not a table job: each step runs its row-slice sweep
+//           (pagerank_onepart, pr.cpp:119-154) and update (pr.cpp:229-303)
+//           on a lower-priority side stream beside the step graph; done
+//           after `arg` iterations
 // Between steps the host retires finished requests (their results are
 // copied to pinned host buffers), admits queued ones while their state fits
 // the HBM budget and a slot is free, and attaches a request to an identical
@@ -53,7 +54,7 @@ constexpr int kSlots = 64;
 constexpr int kMaxJobs = 256;
 constexpr int kCounters = 4;
 
-enum JobKind : int { kJobBfs = 0, kJobWcc = 1, kJobKcore = 2, kJobPr = 3 };
+enum JobKind : int { kJobBfs = 0, kJobWcc = 1, kJobKcore = 2 };
 constexpr int kFlagFirst = 1;      // WCC: first sweep (labels every end); k-core: round only
 
 typedef FvPair<unsigned long long> Fv64;
@@ -78,11 +79,6 @@ struct Job {
     // k-core
     int32_t* deg;
     uint32_t* removed;
-    // PR
-    float* x;
-    float* y;
-    float* r;
-    const int32_t* degree;
     unsigned long long* cnt;      // kCounters per job
     uint8_t level[kSlots];        // BFS: frontier depth per slot (0 = slot idle)
 };
@@ -142,12 +138,8 @@ __global__ void __launch_bounds__(kThreads) serve_sweep_kernel(const Table* __re
                     sweep_unit(jb.units[ui], jb.rec, op, lane);
                 break;
             }
-            default: {
-                const PrOp op{jb.x, jb.y, jb.directed};
-                for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps)
-                    sweep_unit(jb.units[ui], jb.rec, op, lane);
+            default:
                 break;
-            }
         }
     }
 }
@@ -211,15 +203,8 @@ __global__ void __launch_bounds__(kThreads) serve_post_kernel(const Table* __res
                 }
                 break;
             }
-            default: {
-                const double r = 0.15 + 0.85 * (double)jb.y[v];      // pr.cpp:281-302
-                const int32_t d = jb.degree[v];
-                const double xn = (d == 0 || v >= jb.V) ? 0.0 : r / (double)d;
-                jb.r[v] = v < jb.V ? (float)r : 0.f;
-                jb.x[v] = (float)xn;
-                jb.y[v] = 0.f;
+            default:
                 break;
-            }
         }
     }
 }
@@ -334,6 +319,7 @@ struct Request {
     float* x = nullptr;
     float* y = nullptr;
     float* r = nullptr;
+    int* err = nullptr;                  // PageRank: bounded-wait flag of its sweeps
     unsigned long long* cnt = nullptr;
     std::shared_ptr<HostBuf> result;     // pinned host copy of the result
     uint64_t result_bytes = 0;
@@ -346,6 +332,8 @@ struct gs_server {
     uint64_t budget = 0;
     uint64_t used = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t pr_stream = nullptr;    // PageRank sweeps, beside the step graph
+    cudaEvent_t ev_step = nullptr, ev_pr = nullptr;
     cudaGraphExec_t step_exec = nullptr;
     cudaGraph_t step_graph = nullptr;
     Table* h_table = nullptr;            // pinned
@@ -513,9 +501,13 @@ gs_status admit(gs_server* s, Request& r) {
             GS_CHECK_CUDA(ctx, cudaMemsetAsync(r.act[1], 0, g->nw, s->stream));
             break;
         default:
+            // PageRank sweeps the graph's row-slice layout (built once)
+            if (!g->pr.built) GS_TRY(pr_layout_build(sg.g));
             GS_TRY(pool_dev(s, N * 4, (void**)&r.x));
             GS_TRY(pool_dev(s, N * 4, (void**)&r.y));
             GS_TRY(pool_dev(s, N * 4, (void**)&r.r));
+            GS_TRY(pool_dev(s, 256, (void**)&r.err));
+            GS_CHECK_CUDA(ctx, cudaMemsetAsync(r.err, 0, 256, s->stream));
             serve_pr_init<<<blocks_for(N, ctx), kThreads, 0, s->stream>>>(r.x, r.y, N, g->V);
             s->kernel_launches++;
             break;
@@ -554,6 +546,7 @@ void release(gs_server* s, Request& r) {
             pool_dev_put(s, r.x, N * 4);
             pool_dev_put(s, r.y, N * 4);
             pool_dev_put(s, r.r, N * 4);
+            pool_dev_put(s, r.err, 256);
             break;
     }
     r.parent = nullptr;
@@ -563,6 +556,7 @@ void release(gs_server* s, Request& r) {
     r.removed = nullptr;
     r.act[0] = r.act[1] = nullptr;
     r.x = r.y = r.r = nullptr;
+    r.err = nullptr;
     s->used -= r.footprint;
     r.footprint = 0;
 }
@@ -652,6 +646,9 @@ gs_status gs_serve_create(gs_ctx* ctx, uint64_t state_budget_bytes, gs_server** 
     cudaDeviceGetStreamPriorityRange(&lo, &hi);
     gs_status st = GS_OK;
     cudaError_t e = cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, hi);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->pr_stream, cudaStreamNonBlocking, lo);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_step, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_pr, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaHostAlloc((void**)&s->h_table, sizeof(Table), cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc((void**)&s->h_cnt, sizeof(unsigned long long) * kMaxJobs * kCounters,
                                             cudaHostAllocDefault);
@@ -738,9 +735,28 @@ gs_status gs_serve_step(gs_server* s, int* n_active, int* n_queued) {
         int nj = 0;
         uint64_t runs = 0, words = 0;
         std::vector<int> group_job(s->graphs.size(), -1);
+        // PageRank requests: one row-slice sweep and one update each, on the
+        // side stream, overlapping the step graph
+        bool any_pr = false;
+        for (uint64_t id : s->active) {
+            Request& r = s->reqs[id];
+            if (r.algo != GS_ALGO_PAGERANK) continue;
+            if (!any_pr) {   // after this step's admissions (their init kernels)
+                GS_CHECK_CUDA(ctx, cudaEventRecord(s->ev_step, s->stream));
+                GS_CHECK_CUDA(ctx, cudaStreamWaitEvent(s->pr_stream, s->ev_step, 0));
+            }
+            any_pr = true;
+            gs_graph* g = s->graphs[r.graph].g;
+            GS_TRY(pr_slice_sweep(g, s->pr_stream, r.x, r.y, r.err));
+            GS_TRY(pr_finalize_launch(ctx, s->pr_stream, r.x, r.y, r.r, g->d_degree, g->N, g->V, 0));
+            s->kernel_launches += 2;
+            r.job = -1;
+        }
+        if (any_pr) GS_CHECK_CUDA(ctx, cudaEventRecord(s->ev_pr, s->pr_stream));
         for (uint64_t id : s->active) {
             Request& r = s->reqs[id];
             SrvGraph& sg = s->graphs[r.graph];
+            if (r.algo == GS_ALGO_PAGERANK) continue;
             if (r.algo == GS_ALGO_BFS && group_job[r.graph] >= 0) {
                 r.job = group_job[r.graph];
                 continue;
@@ -779,11 +795,6 @@ gs_status gs_serve_step(gs_server* s, int* n_active, int* n_queued) {
                     j.act_next = r.act[r.cur ^ 1];
                     break;
                 default:
-                    j.kind = kJobPr;
-                    j.x = r.x;
-                    j.y = r.y;
-                    j.r = r.r;
-                    j.degree = sg.g->d_degree;
                     break;
             }
             r.job = nj;
@@ -795,6 +806,7 @@ gs_status gs_serve_step(gs_server* s, int* n_active, int* n_queued) {
         t->total_runs = runs;
         t->total_words = words;
         GS_CHECK_CUDA(ctx, cudaGraphLaunch(s->step_exec, s->stream));
+        if (any_pr) GS_CHECK_CUDA(ctx, cudaStreamWaitEvent(s->stream, s->ev_pr, 0));
         GS_CHECK_CUDA(ctx, cudaStreamSynchronize(s->stream));
         s->graph_launches++;
         s->kernel_launches += 2;
@@ -805,7 +817,7 @@ gs_status gs_serve_step(gs_server* s, int* n_active, int* n_queued) {
         for (uint64_t id : s->active) {
             Request& r = s->reqs[id];
             SrvGraph& sg = s->graphs[r.graph];
-            const unsigned long long* c = s->h_cnt + (size_t)r.job * kCounters;
+            const unsigned long long* c = s->h_cnt + (size_t)std::max(r.job, 0) * kCounters;
             r.steps += 1;
             bool done = false;
             switch (r.algo) {
@@ -834,6 +846,11 @@ gs_status gs_serve_step(gs_server* s, int* n_active, int* n_queued) {
         if (!finished.empty()) {
             for (uint64_t id : finished) {
                 Request& r = s->reqs[id];
+                if (r.algo == GS_ALGO_PAGERANK) {
+                    int h_err = 0;
+                    GS_CHECK_CUDA(ctx, cudaMemcpy(&h_err, r.err, sizeof(int), cudaMemcpyDeviceToHost));
+                    if (h_err) r.status = GS_ERR_TIMEOUT;
+                }
                 if (r.status == GS_OK) GS_TRY(take_result(s, r));
                 else if (r.algo == GS_ALGO_BFS) {
                     // clear the slot for its next request (result discarded)
@@ -920,6 +937,7 @@ gs_status gs_serve_stats(const gs_server* s, uint64_t* steps, uint64_t* graph_la
 gs_status gs_serve_free(gs_server* s) {
     if (!s) return GS_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->pr_stream) cudaStreamSynchronize(s->pr_stream);
     s->reqs.clear();   // drops result buffers into the host pool
     if (s->step_exec) cudaGraphExecDestroy(s->step_exec);
     if (s->step_graph) cudaGraphDestroy(s->step_graph);
@@ -930,6 +948,9 @@ gs_status gs_serve_free(gs_server* s) {
     if (s->h_table) cudaFreeHost(s->h_table);
     if (s->h_cnt) cudaFreeHost(s->h_cnt);
     if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->pr_stream) cudaStreamDestroy(s->pr_stream);
+    if (s->ev_step) cudaEventDestroy(s->ev_step);
+    if (s->ev_pr) cudaEventDestroy(s->ev_pr);
     delete s;
     return GS_OK;
 }

@@ -303,14 +303,26 @@ gs_status pr_init(gs_state* s) {
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_r, 0, g->N * 4, ctx->stream));
+    if (s->d_error) GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_error, 0, sizeof(uint64_t), ctx->stream));
+    // resident graphs sweep the row-slice layout (built once per graph)
+    if (!g->stream && g->E && !g->pr.built) GS_TRY(pr_layout_build(g));
     return GS_OK;
 }
 
 gs_status pr_sweep_launch(gs_state* s) {
     gs_graph* g = s->g;
+    if (!g->seg.list && g->pr.built) return pr_slice_launch(s);
     PrOp op{s->d_x, s->d_y, g->directed};
     // algorithmic bytes per iteration: 4E + 12V (records, x, s, inv)
     return launch_sweep(g, op, GS_ALGO_PAGERANK, 4 * g->E + 12 * g->V, true);
+}
+
+gs_status pr_finalize_launch(gs_ctx* ctx, cudaStream_t stream, float* x, float* y, float* r, const int32_t* deg,
+                             uint64_t N, uint64_t V, int compat) {
+    pr_finalize_kernel<<<blocks_for(N, ctx), kThreads, 0, stream>>>(x, y, r, deg, N, V, compat);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    ctx->launches++;
+    return GS_OK;
 }
 
 gs_status pr_finalize(gs_state* s, int64_t* frontier, int* done) {
@@ -322,7 +334,14 @@ gs_status pr_finalize(gs_state* s, int64_t* frontier, int* done) {
     ctx->launches++;
     *frontier = s->step;
     *done = s->step >= s->arg;
-    if (*done) GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (*done && s->d_error) {
+        // the row-slice sweep's bounded waits report here, once per run
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->h_scalars, s->d_error, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        if (ctx->h_scalars[0]) return gs_fail(ctx, GS_ERR_TIMEOUT, "PageRank sweep: a bounded wait gave up");
+    } else if (*done) {
+        GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
     return GS_OK;
 }
 
