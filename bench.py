@@ -153,25 +153,36 @@ class ClockSampler:
 
 
 class Dist:
-    def __init__(self, gpus: int):
+    """One process per GPU (torchrun): rank/world from the environment, a
+    process group for the barrier and the max/sum of two scalars per run
+    (NCCL on the GPUs; gloo for host-only runs of the same logic)."""
+
+    def __init__(self, gpus: int, backend: str = "nccl"):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
         self.pg = False
         if self.world > 1:
             import datetime
 
             import torch.distributed as td
 
-            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            td.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
             self.pg = True
+
+    def _device(self):
+        return "cuda" if self.backend == "nccl" else "cpu"
 
     def barrier(self):
         if self.pg:
             import torch
             import torch.distributed as td
 
-            td.barrier(device_ids=[torch.cuda.current_device()])
+            if self.backend == "nccl":
+                td.barrier(device_ids=[torch.cuda.current_device()])
+            else:
+                td.barrier()
 
     def reduce(self, x: float, op: str) -> float:
         if not self.pg:
@@ -179,7 +190,7 @@ class Dist:
         import torch
         import torch.distributed as td
 
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device=self._device())
         td.all_reduce(t, op=td.ReduceOp.MAX if op == "max" else td.ReduceOp.SUM)
         return float(t.item())
 
@@ -188,6 +199,7 @@ class Dist:
             import torch.distributed as td
 
             td.destroy_process_group()
+            self.pg = False
 
 
 # ------------------------------------------------------------ CPU reference --
