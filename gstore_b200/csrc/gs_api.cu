@@ -36,6 +36,37 @@ void gs_dev_free(void* ptr) {
     if (ptr) cudaFree(ptr);
 }
 
+constexpr uint64_t kPoolMaxBytes = 16ull << 30;
+
+gs_status gs_pool_get(gs_ctx* ctx, size_t bytes, void** out) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    auto it = ctx->pool_free.find(bytes);
+    if (it != ctx->pool_free.end()) {
+        *out = it->second;
+        ctx->pool_free.erase(it);
+        ctx->pool_bytes -= bytes;
+        return GS_OK;
+    }
+    return gs_dev_alloc(ctx, out, bytes);
+}
+
+void gs_pool_put(gs_ctx* ctx, void* ptr, size_t bytes) {
+    if (!ptr) return;
+    bytes = (bytes + 255) & ~(size_t)255;
+    if (ctx->pool_bytes + bytes > kPoolMaxBytes) {
+        gs_dev_free(ptr);
+        return;
+    }
+    ctx->pool_free.emplace(bytes, ptr);
+    ctx->pool_bytes += bytes;
+}
+
+void gs_pool_clear(gs_ctx* ctx) {
+    for (auto& kv : ctx->pool_free) gs_dev_free(kv.second);
+    ctx->pool_free.clear();
+    ctx->pool_bytes = 0;
+}
+
 gs_status gs_alloc_records(gs_ctx* ctx, uint32_t** ptr, uint64_t n_records) {
     GS_TRY(gs_dev_alloc(ctx, (void**)ptr, (n_records + kRecPad) * 4));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(*ptr + n_records, 0, kRecPad * 4, ctx->stream));
@@ -109,6 +140,7 @@ gs_status gs_destroy(gs_ctx* ctx) {
     if (!ctx) return GS_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    gs_pool_clear(ctx);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);

@@ -433,10 +433,10 @@ int pick_candidate(const gs_tune& t) {
 
 gs_status scratch(gs_batch* b, size_t bytes, void** out) {
     if (bytes > b->scratch_bytes) {
-        gs_dev_free(b->d_scratch);
+        gs_pool_put(b->ctx, b->d_scratch, b->scratch_bytes);
         b->d_scratch = nullptr;
         b->scratch_bytes = 0;
-        GS_TRY(gs_dev_alloc(b->ctx, &b->d_scratch, bytes));
+        GS_TRY(gs_pool_get(b->ctx, bytes, &b->d_scratch));
         b->scratch_bytes = bytes;
     }
     *out = b->d_scratch;
@@ -475,7 +475,7 @@ gs_status run_bfs_group(gs_batch* b, gs_bfs_group& grp) {
     int* levels = (int*)(small + 256 * 8 + 32);
     W* overflow = (W*)(small + 256 * 8 + 48);
     uint64_t* roots = (uint64_t*)(small + 256 * 8 + 64);
-    GS_TRY(gs_dev_alloc(ctx, (void**)&grp.depth, N * kBits));
+    GS_TRY(gs_pool_get(ctx, N * kBits, (void**)&grp.depth));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(base, 0, fv_b + nx_b + act_b + small_b, ctx->stream));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(grp.depth, 0, N * kBits, ctx->stream));
     std::vector<uint64_t> h_roots(n);
@@ -572,19 +572,19 @@ gs_status run_wk_queries(gs_batch* b, std::vector<int>& idx) {
             gs_batch_query& q = b->q[idx[k]];
             gs_graph* g = q.g;
             const uint64_t N = g->N;
-            GS_TRY(gs_dev_alloc(ctx, (void**)&q.cnt, 4 * sizeof(unsigned long long)));
+            GS_TRY(gs_pool_get(ctx, 4 * sizeof(unsigned long long), (void**)&q.cnt));
             GS_CHECK_CUDA(ctx, cudaMemsetAsync(q.cnt, 0, 4 * sizeof(unsigned long long), ctx->stream));
-            GS_TRY(gs_dev_alloc(ctx, (void**)&q.act, 2 * (size_t)g->nw));
+            GS_TRY(gs_pool_get(ctx, 2 * (size_t)g->nw, (void**)&q.act));
             GS_CHECK_CUDA(ctx, cudaMemsetAsync(q.act, 0, 2 * (size_t)g->nw, ctx->stream));
             if (q.algo == GS_ALGO_WCC) {
-                GS_TRY(gs_dev_alloc(ctx, (void**)&q.parent, N * 4));
-                GS_TRY(gs_dev_alloc(ctx, (void**)&q.touched, N));
+                GS_TRY(gs_pool_get(ctx, N * 4, (void**)&q.parent));
+                GS_TRY(gs_pool_get(ctx, N, (void**)&q.touched));
                 wk_init_kernel<<<blocks_for(N, ctx), kThreads, 0, ctx->stream>>>(q.parent, N);
                 ctx->launches++;
                 GS_CHECK_CUDA(ctx, cudaMemsetAsync(q.touched, 0, N, ctx->stream));
             } else {
-                GS_TRY(gs_dev_alloc(ctx, (void**)&q.deg, N * 4));
-                GS_TRY(gs_dev_alloc(ctx, (void**)&q.removed, N / 8));
+                GS_TRY(gs_pool_get(ctx, N * 4, (void**)&q.deg));
+                GS_TRY(gs_pool_get(ctx, N / 8, (void**)&q.removed));
                 GS_CHECK_CUDA(ctx, cudaMemcpyAsync(q.deg, g->d_degree, N * 4, cudaMemcpyDeviceToDevice, ctx->stream));
             }
             BQuery d;
@@ -644,13 +644,16 @@ gs_status run_wk_queries(gs_batch* b, std::vector<int>& idx) {
     return GS_OK;
 }
 
-void free_query(gs_batch_query& q) {
-    gs_dev_free(q.parent);
-    gs_dev_free(q.touched);
-    gs_dev_free(q.deg);
-    gs_dev_free(q.removed);
-    gs_dev_free(q.act);
-    gs_dev_free(q.cnt);
+void free_query(gs_ctx* ctx, gs_batch_query& q) {
+    if (q.g) {
+        const uint64_t N = q.g->N;
+        gs_pool_put(ctx, q.parent, N * 4);
+        gs_pool_put(ctx, q.touched, N);
+        gs_pool_put(ctx, q.deg, N * 4);
+        gs_pool_put(ctx, q.removed, N / 8);
+        gs_pool_put(ctx, q.act, 2 * (size_t)q.g->nw);
+        gs_pool_put(ctx, q.cnt, 4 * sizeof(unsigned long long));
+    }
     q.parent = nullptr;
     q.touched = nullptr;
     q.deg = nullptr;
@@ -852,9 +855,9 @@ gs_status gs_batch_stats(const gs_batch* b, uint64_t* launches, double* kernel_m
 gs_status gs_batch_free(gs_batch* b) {
     if (!b) return GS_OK;
     cudaStreamSynchronize(b->ctx->stream);
-    for (auto& q : b->q) free_query(q);
-    for (auto& grp : b->groups) gs_dev_free(grp.depth);
-    gs_dev_free(b->d_scratch);
+    for (auto& q : b->q) free_query(b->ctx, q);
+    for (auto& grp : b->groups) gs_pool_put(b->ctx, grp.depth, grp.g->N * grp.bits);
+    gs_pool_put(b->ctx, b->d_scratch, b->scratch_bytes);
     if (b->e0) cudaEventDestroy(b->e0);
     if (b->e1) cudaEventDestroy(b->e1);
     delete b;

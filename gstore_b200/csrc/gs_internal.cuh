@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -119,6 +120,10 @@ struct gs_ctx {
     uint64_t* h_scalars = nullptr;   // pinned mirror
     int num_sms = 148;
     uint64_t launches = 0;           // kernels launched on this context
+    // device blocks returned by finished batches, by exact size (reused by
+    // the next batch instead of cudaMalloc / cudaFree)
+    std::multimap<size_t, void*> pool_free;
+    uint64_t pool_bytes = 0;
 };
 
 struct gs_graph {
@@ -223,6 +228,11 @@ void gs_geometry_of(uint64_t V, int directed, uint32_t* p, uint32_t* p_s, uint64
 gs_status gs_dev_alloc(gs_ctx* ctx, void** ptr, size_t bytes);
 gs_status gs_alloc_records(gs_ctx* ctx, uint32_t** ptr, uint64_t n_records);
 void gs_dev_free(void* ptr);
+// Context pool: a cached block of exactly `bytes` (rounded to 256), or a new
+// one; gs_pool_put returns it (blocks beyond kPoolMaxBytes are freed).
+gs_status gs_pool_get(gs_ctx* ctx, size_t bytes, void** out);
+void gs_pool_put(gs_ctx* ctx, void* ptr, size_t bytes);
+void gs_pool_clear(gs_ctx* ctx);
 
 gs_status launch_validate_records(gs_graph* g, int* d_flag);
 gs_status launch_degree_from_records(gs_graph* g);
