@@ -322,7 +322,7 @@ def bench_batched(ctx, torch, gs):
             plain.append(s.count())
         torch.cuda.synchronize()
         t_plain = time.perf_counter() - t0
-    for _ in range(4):                   # the autotuner tries each configuration once
+    for _ in range(8):                   # the autotuner tries each configuration once
         with gs.Batch(ctx) as b:
             for r in roots:
                 b.add(g, "bfs", r)

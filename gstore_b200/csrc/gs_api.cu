@@ -201,6 +201,10 @@ static void free_graph_arrays(gs_graph* g) {
     gs_dev_free(g->d_units);
     gs_dev_free(g->d_runs_blk);
     gs_dev_free(g->d_units_blk);
+    gs_dev_free(g->d_runs_blk2);
+    gs_dev_free(g->d_units_blk2);
+    g->d_runs_blk2 = nullptr;
+    g->d_units_blk2 = nullptr;
     g->d_runs = nullptr;
     g->d_units = nullptr;
     g->d_runs_blk = nullptr;
@@ -212,13 +216,16 @@ static void free_graph_arrays(gs_graph* g) {
     g->d_degree = nullptr;
 }
 
-// The L2-blocked sweep order: tiles grouped into blocks of kBlockWindows x
-// kBlockWindows windows (row-major inside a block), so the vertex state the
-// tiles in flight touch (2 kBlockWindows windows) stays in L2.  Runs are
-// short (one tile row, <= kBlockRunUnits units, one per warp of a CTA) so
-// the CTAs in flight work inside one or two blocks.  Used by the sweeps whose per-record state is large (PageRank,
-// WCC, k-core); their results do not depend on the order.
-static gs_status build_blocked_order(gs_graph* g) {
+// An L2-blocked sweep order: tiles grouped into blocks of `block` x `block`
+// windows (row-major inside a block), so the vertex state the tiles in
+// flight touch (2 `block` windows) stays in L2.  Runs are short (one tile
+// row, <= kBlockRunUnits units, one per warp of a CTA) so the CTAs in flight
+// work inside one or two blocks.  Used by the sweeps whose per-record state
+// is large (WCC, k-core, batches, serving: kBlockWindows; multi-source BFS
+// with 16-byte vertex state may pick kBlockWindowsSmall); their results do
+// not depend on the order.
+static gs_status build_blocked_order(gs_graph* g, uint32_t block, uint64_t* R_out, gs_tile_run** d_runs_out,
+                                     gs_unit** d_units_out) {
     gs_ctx* ctx = g->ctx;
     const uint64_t T = g->T;
     std::vector<uint32_t> tile_unit(T + 1, 0);
@@ -233,7 +240,7 @@ static gs_status build_blocked_order(gs_graph* g) {
     for (uint32_t k = 0; k < T; ++k) order[k] = k;
     auto block_of = [&](uint32_t k) {
         const uint32_t rc = g->h_tile_rc[k];
-        return ((uint64_t)((rc >> 16) / kBlockWindows) << 32) | ((rc & 0xFFFFu) / kBlockWindows);
+        return ((uint64_t)((rc >> 16) / block) << 32) | ((rc & 0xFFFFu) / block);
     };
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return block_of(a) < block_of(b); });
     std::vector<gs_unit> units;
@@ -258,14 +265,14 @@ static gs_status build_blocked_order(gs_graph* g) {
             runs.back().unit_end = (uint32_t)units.size();
         }
     }
-    g->R_blk = runs.size();
-    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_units_blk, std::max<size_t>(1, units.size()) * sizeof(gs_unit)));
-    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_runs_blk, std::max<size_t>(1, runs.size()) * sizeof(gs_tile_run)));
+    *R_out = runs.size();
+    GS_TRY(gs_dev_alloc(ctx, (void**)d_units_out, std::max<size_t>(1, units.size()) * sizeof(gs_unit)));
+    GS_TRY(gs_dev_alloc(ctx, (void**)d_runs_out, std::max<size_t>(1, runs.size()) * sizeof(gs_tile_run)));
     if (!units.empty())
-        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_units_blk, units.data(), units.size() * sizeof(gs_unit),
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(*d_units_out, units.data(), units.size() * sizeof(gs_unit),
                                            cudaMemcpyHostToDevice, ctx->stream));
     if (!runs.empty())
-        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_runs_blk, runs.data(), runs.size() * sizeof(gs_tile_run),
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(*d_runs_out, runs.data(), runs.size() * sizeof(gs_tile_run),
                                            cudaMemcpyHostToDevice, ctx->stream));
     GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return GS_OK;
@@ -345,7 +352,10 @@ static gs_status build_tables(gs_graph* g) {
     g->I = n_items;
     g->R = runs.size();
     g->U = units.size();
-    if (!g->stream) GS_TRY(build_blocked_order(g));
+    if (!g->stream) {
+        GS_TRY(build_blocked_order(g, kBlockWindows, &g->R_blk, &g->d_runs_blk, &g->d_units_blk));
+        GS_TRY(build_blocked_order(g, kBlockWindowsSmall, &g->R_blk2, &g->d_runs_blk2, &g->d_units_blk2));
+    }
     GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_units, std::max<size_t>(1, units.size()) * sizeof(gs_unit)));
     if (!units.empty())
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_units, units.data(), units.size() * sizeof(gs_unit),

@@ -31,9 +31,9 @@
 //
 // Autotuning.  For the BFS groups of a graph the tuner tries each candidate
 // configuration once — frontier word width (32 or 64 queries per group) and
-// run order (file order, 64-unit runs; or L2-blocked, 8-unit runs) — timing
-// each launch with CUDA events per query, then keeps the fastest for that
-// graph.
+// run order (file order with 64-unit runs, or L2-blocked with 8-unit runs in
+// blocks of 64 or 32 windows) — timing each launch with CUDA events per
+// query, then keeps the fastest for that graph.
 #include "gs_internal.cuh"
 #include "gs_ops.cuh"
 
@@ -105,6 +105,8 @@ struct MsArgs {
     int* err;
     int* levels;
     int directed;
+    const gs_pr_item* items;         // row-slice order: (row, slice, column block) items
+    uint64_t n_items;
 };
 
 template <class W>
@@ -162,6 +164,116 @@ __global__ void __launch_bounds__(kThreads) msbfs_kernel(MsArgs<W> a) {
         }
     }
     if (tid == 0) *a.levels = 254;
+}
+
+// ------------------------------------------- MS-BFS over row slices ----
+// The same level loop over the row-slice layout (a copy of the records with
+// each tile grouped by row slice v0 >> 13 and sorted by v1 inside it; items
+// are (row window, slice, 32-window column block)).  A CTA stages the
+// {frontier, visited} words of its item's row slice (8,192 vertices) in
+// shared memory with coalesced loads and collects the row ends' discoveries
+// in a shared `next` slice, flushed once per item; only the column end
+// reads global memory per record.
+constexpr int kSliceThreads = 1024;
+constexpr int kSliceWarps = kSliceThreads / 32;
+constexpr uint32_t kSliceV = 1u << kPrSliceBits;
+
+template <class W>
+struct MsSliceOp {
+    const FvPair<W>* fvs;   // shared: row slice
+    W* nxs;                 // shared: row slice discoveries
+    FvPair<W>* fv;
+    W* next;
+    int directed;
+    struct Item {
+        uint32_t cb;
+    };
+    __device__ bool begin(uint32_t, uint32_t col, Item& c) const {
+        c.cb = col << 16;
+        return true;
+    }
+    __device__ void record(uint32_t r, Item& c) const {
+        const uint32_t a = r & (kSliceV - 1), b = c.cb + (r >> 16);
+        const FvPair<W> sa = fvs[a], sb = load_fv(fv + b);
+        const W nb = sa.f & ~sb.vis;
+        if (nb) atomicOr(next + b, nb);
+        if (!directed) {
+            const W na = sb.f & ~sa.vis;
+            if (na) atomicOr(nxs + a, na);
+        }
+    }
+    __device__ void end(uint32_t, uint32_t, Item&) const {}
+};
+
+template <class W>
+__global__ void __launch_bounds__(kSliceThreads) msbfs_slice_kernel(MsArgs<W> a) {
+    constexpr int kBits = sizeof(W) * 8;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    FvPair<W>* fvs = reinterpret_cast<FvPair<W>*>(smem_raw);
+    W* nxs = reinterpret_cast<W*>(smem_raw + kSliceV * sizeof(FvPair<W>));
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    const MsSliceOp<W> op{fvs, nxs, a.fv, a.next, a.directed};
+    for (int level = 1; level < 255; ++level) {
+        const uint8_t* act = a.act + (level & 1) * a.nw;
+        uint8_t* act_next = a.act + ((level + 1) & 1) * a.nw;
+        for (uint64_t w = gtid; w < a.nw; w += nth) act_next[w] = 0;
+        for (uint64_t i = blockIdx.x; i < a.n_items; i += gridDim.x) {
+            const gs_pr_item it = a.items[i];
+            const bool ar = __ldcg(act + it.row) != 0;
+            int any = ar ? 1 : 0;
+            if (!ar && !a.directed)
+                for (uint32_t ui = it.unit_beg + tid; ui < it.unit_end; ui += kSliceThreads)
+                    any |= __ldcg(act + (a.units[ui].rc & 0xFFFFu)) != 0;
+            if (!__syncthreads_or(any)) continue;
+            const uint64_t base = ((uint64_t)it.row << kTileBits) + ((uint64_t)it.slice << kPrSliceBits);
+            const uint4* src = reinterpret_cast<const uint4*>(a.fv + base);
+            uint4* dst = reinterpret_cast<uint4*>(fvs);
+            for (uint32_t k = tid; k < kSliceV * sizeof(FvPair<W>) / 16; k += kSliceThreads) dst[k] = __ldcg(src + k);
+            if (!a.directed)
+                for (uint32_t k = tid; k < kSliceV; k += kSliceThreads) nxs[k] = 0;
+            __syncthreads();
+            for (uint32_t ui = it.unit_beg + warp; ui < it.unit_end; ui += kSliceWarps) {
+                const gs_unit d = a.units[ui];
+                if (!ar && (a.directed || !__ldcg(act + (d.rc & 0xFFFFu)))) continue;
+                sweep_unit(d, a.rec, op, lane);
+            }
+            __syncthreads();
+            if (!a.directed)
+                for (uint32_t k = tid; k < kSliceV; k += kSliceThreads)
+                    if (nxs[k]) atomicOr(a.next + base + k, nxs[k]);
+            __syncthreads();
+        }
+        if (!grid_barrier(a.bar, a.err)) return;
+        uint64_t local = 0;
+        for (uint64_t v = gtid; v < a.N; v += nth) {
+            const W nx = __ldcg(a.next + v);
+            const FvPair<W> s = load_fv(a.fv + v);
+            if (nx == 0 && s.f == 0) continue;
+            if (nx) __stcg(a.next + v, (W)0);
+            const W fresh = nx & ~s.vis;
+            store_fv(a.fv + v, fresh, s.vis | fresh);
+            if (fresh) {
+                local += popc_w(fresh);
+                act_next[v >> 16] = 1;
+                if (level == 254) atomicOr(a.overflow, fresh);
+                W x = fresh;
+                while (x) {
+                    const int q = ffs_w(x) - 1;
+                    a.depth[v * kBits + q] = (uint8_t)(level + 1);
+                    x &= x - 1;
+                }
+            }
+        }
+        warp_add_u64(a.total + level, local);
+        if (!grid_barrier(a.bar, a.err)) return;
+        if (__ldcg(a.total + level) == 0) {
+            if (gtid == 0) *a.levels = level;
+            return;
+        }
+    }
+    if (gtid == 0) *a.levels = 254;
 }
 
 // Root seeding: depth 1, frontier and visited bit of query q (bfs.cpp:70).
@@ -381,7 +493,7 @@ struct gs_batch_query {
 struct gs_bfs_group {
     gs_graph* g = nullptr;
     int bits = 64;
-    bool blocked = true;
+    int order = 1;                     // 0 file order, 1 / 2: 64- / 32-window blocks, 3 row slices
     std::vector<int> queries;
     uint8_t* depth = nullptr;          // [N][bits]
     int levels = 0;
@@ -403,9 +515,12 @@ struct gs_batch {
 };
 
 // Autotuner record of one graph: per candidate, time per query of its runs.
+// (bits 32 / 64) x (file order / 64-window blocks / 32-window blocks / row slices)
+constexpr int kOrders = 4;
+constexpr int kCandidates = 2 * kOrders;
 struct gs_tune {
-    double ms_per_query[4] = {0, 0, 0, 0};   // (bits 32/64) x (file / blocked)
-    int samples[4] = {0, 0, 0, 0};
+    double ms_per_query[kCandidates] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int samples[kCandidates] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 namespace {
@@ -419,14 +534,15 @@ gs_tune& tune_of(const gs_graph* g) {
     return g_tune.back().second;
 }
 
-// Candidates: 0 = 32-bit words, file order; 1 = 32-bit, blocked; 2 = 64-bit,
-// file order; 3 = 64-bit, blocked.  Each is tried once, then the fastest per
-// query is kept.
+// Candidate c: word width 32 (c < kOrders) or 64 bits; order c % kOrders:
+// file order (64-unit runs), 64-window or 32-window blocks (8-unit runs), or
+// the row-slice layout (msbfs_slice_kernel).  Each is tried once, then the
+// fastest per query is kept.
 int pick_candidate(const gs_tune& t) {
-    for (int c = 3; c >= 0; --c)
+    for (int c = kCandidates - 1; c >= 0; --c)
         if (t.samples[c] == 0) return c;
-    int best = 3;
-    for (int c = 0; c < 4; ++c)
+    int best = kCandidates - 1;
+    for (int c = 0; c < kCandidates; ++c)
         if (t.ms_per_query[c] < t.ms_per_query[best]) best = c;
     return best;
 }
@@ -484,10 +600,13 @@ gs_status run_bfs_group(gs_batch* b, gs_bfs_group& grp) {
     msbfs_seed_kernel<W><<<1, 1, 0, ctx->stream>>>(roots, n, fv, grp.depth, act + g->nw);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches += 1;
-    MsArgs<W> a{grp.blocked ? g->d_runs_blk : g->d_runs,
-                grp.blocked ? g->d_units_blk : g->d_units,
+    const gs_tile_run* runs = grp.order == 1 ? g->d_runs_blk : grp.order == 2 ? g->d_runs_blk2 : g->d_runs;
+    const gs_unit* units = grp.order == 1 ? g->d_units_blk : grp.order == 2 ? g->d_units_blk2 : g->d_units;
+    const uint64_t n_runs = grp.order == 1 ? g->R_blk : grp.order == 2 ? g->R_blk2 : g->R;
+    MsArgs<W> a{runs,
+                units,
                 g->d_rec,
-                grp.blocked ? g->R_blk : g->R,
+                n_runs,
                 N,
                 g->nw,
                 fv,
@@ -499,12 +618,32 @@ gs_status run_bfs_group(gs_batch* b, gs_bfs_group& grp) {
                 bar,
                 err,
                 levels,
-                g->directed};
+                g->directed,
+                nullptr,
+                0};
     void* args[] = {&a};
-    const int grid = coop_grid(ctx, (const void*)msbfs_kernel<W>);
     GS_CHECK_CUDA(ctx, cudaEventRecord(b->e0, ctx->stream));
-    GS_CHECK_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)msbfs_kernel<W>, dim3(grid), dim3(kThreads), args, 0,
-                                                   ctx->stream));
+    if (grp.order == 3) {
+        a.units = g->pr.d_units;
+        a.rec = g->pr.d_rec;
+        a.items = g->pr.d_items;
+        a.n_items = g->pr.n_items;
+        const int smem = (int)(kSliceV * (sizeof(FvPair<W>) + sizeof(W)));
+        GS_CHECK_CUDA(ctx, cudaFuncSetAttribute((const void*)msbfs_slice_kernel<W>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, msbfs_slice_kernel<W>, kSliceThreads, smem) !=
+                cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+        GS_CHECK_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)msbfs_slice_kernel<W>,
+                                                       dim3(ctx->num_sms * per_sm), dim3(kSliceThreads), args, smem,
+                                                       ctx->stream));
+    } else {
+        const int grid = coop_grid(ctx, (const void*)msbfs_kernel<W>);
+        GS_CHECK_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)msbfs_kernel<W>, dim3(grid), dim3(kThreads), args,
+                                                       0, ctx->stream));
+    }
     GS_CHECK_CUDA(ctx, cudaEventRecord(b->e1, ctx->stream));
     ctx->launches += 1;
     b->launches += 1;
@@ -518,7 +657,7 @@ gs_status run_bfs_group(gs_batch* b, gs_bfs_group& grp) {
     cudaEventElapsedTime(&ms, b->e0, b->e1);
     b->kernel_ms += ms;
     gs_tune& t = tune_of(g);
-    const int c = (kBits == 64 ? 2 : 0) + (grp.blocked ? 1 : 0);
+    const int c = (kBits == 64 ? kOrders : 0) + grp.order;
     t.ms_per_query[c] = (t.ms_per_query[c] * t.samples[c] + ms / n) / (t.samples[c] + 1);
     t.samples[c] += 1;
     if (h_err) return gs_fail(ctx, GS_ERR_TIMEOUT, "batched BFS: a grid barrier wait gave up");
@@ -543,13 +682,14 @@ gs_status run_bfs_queries(gs_batch* b, std::vector<int>& idx) {
         for (int i : idx)
             if (b->q[i].g == g) mine.push_back(i);
         const int cand = pick_candidate(tune_of(g));
-        const int bits = cand >= 2 ? 64 : 32;
-        const bool blocked = (cand & 1) != 0 && g->d_runs_blk;
+        const int bits = cand >= kOrders ? 64 : 32;
+        const int order = g->d_runs_blk ? cand % kOrders : 0;
+        if (order == 3 && !g->pr.built) GS_TRY(pr_layout_build(g));
         for (size_t s = 0; s < mine.size(); s += bits) {
             gs_bfs_group grp;
             grp.g = g;
             grp.bits = bits;
-            grp.blocked = blocked;
+            grp.order = order;
             for (size_t k = s; k < std::min(mine.size(), s + bits); ++k) {
                 grp.queries.push_back(mine[k]);
                 b->q[mine[k]].group = (int)b->groups.size();

@@ -48,6 +48,7 @@ struct alignas(8) gs_tile_run {
 constexpr uint32_t kUnitRecords = 2048;
 // Side of a block of the L2-blocked sweep order, in windows.
 constexpr uint32_t kBlockWindows = 64;
+constexpr uint32_t kBlockWindowsSmall = 32;
 // Units per run of the L2-blocked order.
 constexpr uint32_t kBlockRunUnits = 8;
 
@@ -145,6 +146,9 @@ struct gs_graph {
     uint64_t R_blk = 0;               // runs of the L2-blocked order (resident graphs)
     gs_tile_run* d_runs_blk = nullptr;
     gs_unit* d_units_blk = nullptr;
+    uint64_t R_blk2 = 0;              // the same with kBlockWindowsSmall blocks
+    gs_tile_run* d_runs_blk2 = nullptr;
+    gs_unit* d_units_blk2 = nullptr;
     uint64_t* d_tile_off = nullptr;   // T + 1 record offsets of non-empty tiles
     uint32_t* d_tile_rc = nullptr;    // T packed (row << 16 | col)
     int32_t* d_degree = nullptr;      // N

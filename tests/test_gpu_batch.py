@@ -5,7 +5,7 @@ plain entry point (gs_state_create / gs_run / gs_download): BFS depths and
 per-level counts, WCC labels and k-core degrees bit for bit, PageRank within
 PR_TOL.  BFS roots on one graph run as a multi-source BFS in 32- or 64-bit
 frontier words; the autotuner tries every word width / tile order once, so
-the BFS checks repeat the batch until all four configurations have run.
+the BFS checks repeat the batch until all eight configurations have run.
 """
 import numpy as np
 import pytest
@@ -52,7 +52,7 @@ def test_msbfs_matches_plain(n_roots, gs, graphs, gpu_ctx_factory):
     roots = _roots(g, n_roots, n_roots)
     roots[1] = roots[0]                      # two queries on one root
     want = {r: _plain_bfs(g, r) for r in set(roots)}
-    for rep in range(4):                     # every autotuner candidate runs once
+    for rep in range(8):                     # every autotuner candidate runs once
         with gs.Batch(ctx) as b:
             ids = [b.add(g, "bfs", r) for r in roots]
             b.run()
