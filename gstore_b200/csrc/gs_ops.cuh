@@ -114,6 +114,24 @@ __device__ __forceinline__ uint32_t find_root(const uint32_t* parent, uint32_t v
     return v;
 }
 
+// find_root with path halving: every vertex passed on the way points to its
+// grandparent afterwards.  Hooking only lowers pointers toward smaller ids,
+// so a vertex's grandparent is always one of its ancestors and the forest
+// stays a forest; a plain store that overwrites a concurrent hook loses that
+// hook, which the next sweep redoes (a sweep ends the loop only when it
+// changed nothing).  Without it the hooking sweeps build long parent chains
+// and spend their time chasing them.
+__device__ __forceinline__ uint32_t find_root_halving(uint32_t* parent, uint32_t v) {
+    while (true) {
+        const uint32_t p = __ldcg(parent + v);
+        if (p == v) return v;
+        const uint32_t gp = __ldcg(parent + p);
+        if (gp == p) return p;
+        __stcg(parent + v, gp);
+        v = gp;
+    }
+}
+
 struct WccOp {
     uint32_t* parent;
     uint8_t* touched;  // non-null on the first sweep
@@ -134,7 +152,7 @@ struct WccOp {
             touched[a] = 1;
             touched[b] = 1;
         }
-        const uint32_t ra = find_root(parent, a), rb = find_root(parent, b);
+        const uint32_t ra = find_root_halving(parent, a), rb = find_root_halving(parent, b);
         if (ra != rb) {         // wcc.cpp:218-231, 263-275: hook toward the smaller
             const uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
             if (atomicMin(parent + hi, lo) > lo) c.n += 1;
