@@ -152,6 +152,9 @@ struct WccOp {
             touched[a] = 1;
             touched[b] = 1;
         }
+        // ends with one parent are in one tree (after pointer jumping most
+        // vertices point at their root): two loads instead of four
+        if (__ldcg(parent + a) == __ldcg(parent + b)) return;
         const uint32_t ra = find_root_halving(parent, a), rb = find_root_halving(parent, b);
         if (ra != rb) {         // wcc.cpp:218-231, 263-275: hook toward the smaller
             const uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
