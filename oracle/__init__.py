@@ -66,6 +66,10 @@ def lib():
                                 C.c_void_p, u64p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
         L.orc_convert.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_int, C.c_uint64,
                                   C.c_void_p, C.c_void_p, C.c_void_p, u64p]
+        L.orc_bfs2.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_uint64, C.c_uint64,
+                               C.c_void_p, C.POINTER(C.c_int)]
+        L.orc_traverse.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_uint64, C.c_uint64,
+                                   C.c_void_p, u64p, C.POINTER(C.c_int)]
         _lib = L
     return _lib
 
@@ -105,6 +109,31 @@ def bfs(start, grid, p, directed, n, root, max_levels=256):
     if st != 0:
         raise ValueError(f"orc_bfs status {st}")
     return depth, counts[: nl.value].copy(), swept[: nl.value].copy()
+
+
+def bfs2(start, grid, p, directed, n, root):
+    """Label-correcting BFS (-j 30): (u8 depth, sweeps)."""
+    start = np.ascontiguousarray(start, np.uint64)
+    grid = np.ascontiguousarray(grid, np.uint32)
+    depth = np.empty(n, np.uint8)
+    ns = C.c_int()
+    st = lib().orc_bfs2(_ptr(start), _ptr(grid), p, int(directed), n, root, _ptr(depth), C.byref(ns))
+    if st != 0:
+        raise ValueError(f"orc_bfs2 status {st}")
+    return depth, ns.value
+
+
+def traverse(start, grid, p, directed, n, pivot):
+    """Single-colour propagation (-j 4): (u32 cid, coloured count, sweeps)."""
+    start = np.ascontiguousarray(start, np.uint64)
+    grid = np.ascontiguousarray(grid, np.uint32)
+    cid = np.empty(n, np.uint32)
+    cnt, ns = C.c_uint64(), C.c_int()
+    st = lib().orc_traverse(_ptr(start), _ptr(grid), p, int(directed), n, pivot, _ptr(cid), C.byref(cnt),
+                            C.byref(ns))
+    if st != 0:
+        raise ValueError(f"orc_traverse status {st}")
+    return cid, cnt.value, ns.value
 
 
 def pagerank(start, grid, degree, p, directed, n, iterations, compat=False):
@@ -206,7 +235,8 @@ def ref_run(prefix: Path, V: int, algo: str, arg: int, directed: bool = False):
     out = Path(str(prefix) + f".{algo}.out")
     r = subprocess.run([str(exe), str(prefix), str(V), algo, str(arg), str(out)],
                        check=True, capture_output=True, text=True)
-    dt = {"bfs": np.uint8, "kcore": np.int32, "wcc": np.uint32, "pr": np.float32}[algo]
+    dt = {"bfs": np.uint8, "kcore": np.int32, "wcc": np.uint32, "pr": np.float32, "bfs2": np.uint8,
+          "traverse": np.uint32}[algo]
     arr = np.fromfile(out, dt)
     out.unlink()
     return arr, r.stdout

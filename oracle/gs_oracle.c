@@ -162,6 +162,74 @@ int orc_bfs(const uint64_t* start, const uint32_t* grid, uint32_t p,
     return status;
 }
 
+/* --------------------------------------------------------------- bfs2 --- */
+int orc_bfs2(const uint64_t* start, const uint32_t* grid, uint32_t p, int directed,
+             uint64_t n, uint64_t root, uint8_t* depth, int* n_sweeps)
+{
+    tiles_t tl;
+    if (root >= n || tiles_make(p, directed, &tl)) return -1;
+    if (check_range(start, grid, &tl, n)) { tiles_free(&tl); return -1; }
+    memset(depth, 0, n);                       /* INFTY = 0 (bfs.cpp:54) */
+    depth[root] = 1;                           /* bfs2.cpp:73 */
+    int status = 0, sweeps = 0;
+    for (;;) {
+        uint64_t changed = 0;
+        for (uint64_t t = 0; t < tl.T && status == 0; ++t) {
+            uint8_t* d0 = depth + ((uint64_t)tl.row[t] << TILE_BITS);
+            uint8_t* d1 = depth + ((uint64_t)tl.col[t] << TILE_BITS);
+            for (uint64_t e = start[t]; e < start[t + 1]; ++e) {
+                uint32_t v0 = grid[e] & 0xFFFF, v1 = grid[e] >> 16;
+                int l0 = d0[v0], l1 = d1[v1];
+                /* relax either end (bfs2_t::bfs_onepart, bfs2.cpp:102-117) */
+                if (l0 != 0 && (l1 == 0 || l1 - l0 > 1)) {
+                    if (l0 == 255) { status = -2; break; }
+                    d1[v1] = (uint8_t)(l0 + 1); ++changed;
+                } else if (!directed && l1 != 0 && (l0 == 0 || l0 - l1 > 1)) {
+                    if (l1 == 255) { status = -2; break; }
+                    d0[v0] = (uint8_t)(l1 + 1); ++changed;
+                }
+            }
+        }
+        ++sweeps;
+        if (status || changed == 0) break;     /* bfs2_t::iteration_finalize */
+    }
+    if (n_sweeps) *n_sweeps = sweeps;
+    tiles_free(&tl);
+    return status;
+}
+
+/* ----------------------------------------------------------- traverse --- */
+int orc_traverse(const uint64_t* start, const uint32_t* grid, uint32_t p, int directed,
+                 uint64_t n, uint64_t pivot, uint32_t* cid, uint64_t* colored, int* n_sweeps)
+{
+    tiles_t tl;
+    if (pivot >= n || tiles_make(p, directed, &tl)) return -1;
+    if (check_range(start, grid, &tl, n)) { tiles_free(&tl); return -1; }
+    for (uint64_t v = 0; v < n; ++v) cid[v] = 0xFFFFFFFFu;   /* invalid_cid, traverse.cpp:66-70 */
+    cid[pivot] = 0;                                          /* colour 0 */
+    uint64_t total = 1;
+    int sweeps = 0;
+    for (;;) {
+        uint64_t changed = 0;
+        for (uint64_t t = 0; t < tl.T; ++t) {
+            uint32_t* c0 = cid + ((uint64_t)tl.row[t] << TILE_BITS);
+            uint32_t* c1 = cid + ((uint64_t)tl.col[t] << TILE_BITS);
+            for (uint64_t e = start[t]; e < start[t + 1]; ++e) {
+                uint32_t v0 = grid[e] & 0xFFFF, v1 = grid[e] >> 16;
+                /* traverse_onepart (traverse.cpp:173-188): v0 -> v1 only */
+                if (c0[v0] == 0 && c1[v1] == 0xFFFFFFFFu) { c1[v1] = 0; ++changed; }
+            }
+        }
+        ++sweeps;
+        total += changed;
+        if (changed == 0) break;               /* traverse_t::iteration_finalize */
+    }
+    if (colored) *colored = total;
+    if (n_sweeps) *n_sweeps = sweeps;
+    tiles_free(&tl);
+    return 0;
+}
+
 /* ----------------------------------------------------------- PageRank --- */
 int orc_pagerank(const uint64_t* start, const uint32_t* grid,
                  const int32_t* degree, uint32_t p, int directed, uint64_t n,

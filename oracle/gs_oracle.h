@@ -45,6 +45,20 @@ int orc_bfs(const uint64_t* start, const uint32_t* grid, uint32_t p,
             uint64_t* level_counts, uint64_t* swept, int max_levels,
             int* n_levels);
 
+/* Label-correcting BFS, "-j 30" (bfs2.cpp:56-181): every tile each sweep;
+ * a record lowers the depth of an end to the other end's depth + 1 (u8,
+ * root 1, 0 = unreached), until a sweep changes nothing.  The result is the
+ * BFS depth; *n_sweeps counts the sweeps in file order. */
+int orc_bfs2(const uint64_t* start, const uint32_t* grid, uint32_t p, int directed,
+             uint64_t n, uint64_t root, uint8_t* depth, int* n_sweeps);
+
+/* Single-colour propagation, "-j 4" (traverse.cpp:56-212): cid[pivot] = 0,
+ * others 0xFFFFFFFF; a record colours v1 from v0 (one direction, in the
+ * half grid too) until a sweep colours nothing.  *colored = vertices with
+ * colour 0. */
+int orc_traverse(const uint64_t* start, const uint32_t* grid, uint32_t p, int directed,
+                 uint64_t n, uint64_t pivot, uint32_t* cid, uint64_t* colored, int* n_sweeps);
+
 /* PageRank in FP64 (pr.cpp:82-303, grid::pagerank_mmap gstore.cpp:2572-2629).
  * x0 = 1/n; per iteration s[v] = sum over records of the other end's x;
  * r = 0.15 + 0.85 s; x = r * inv.  inv = 1/deg (deg > 0) else 0; with

@@ -13,6 +13,8 @@
  *   pr    : vert_rank_prior (f32) after the  (pr_t,    pr.cpp:82-303;
  *           last iteration_finalize             its int32 inverse-degree
  *                                               truncation included)
+ *   bfs2  : depth_t (u8) per vertex          (bfs2_t,  bfs2.cpp:56-181)
+ *   traverse : vert_cid (u32) per vertex     (traverse_t, traverse.cpp:56-212)
  *
  * The tile loop follows grid::bfs_mmap / kcore_mmap / wcc_mmap /
  * pagerank_mmap (gstore.cpp:2502-2804): every stored tile of the half
@@ -34,6 +36,8 @@
 #include "pr.h"
 #include "wcc.h"
 #include "kcore.h"
+#include "bfs2.h"
+#include "traverse.h"
 
 extern grid* g;
 extern cache_driver* cache;
@@ -84,7 +88,7 @@ static void write_out(const char* path, const void* data, size_t bytes)
 int main(int argc, char* argv[])
 {
     if (argc != 6) {
-        fprintf(stderr, "usage: %s prefix vert_count bfs|kcore|wcc|pr arg out\n", argv[0]);
+        fprintf(stderr, "usage: %s prefix vert_count bfs|kcore|wcc|pr|bfs2|traverse arg out\n", argv[0]);
         return 2;
     }
     std::string prefix = argv[1];
@@ -108,7 +112,7 @@ int main(int argc, char* argv[])
     /* BFS and k-core index depth/bitmaps up to p_s << 16 (bfs.cpp:431-440),
      * so their arrays are sized to the whole tile range. */
     vertex_t alloc = V;
-    if (algo == "bfs" || algo == "kcore") {
+    if (algo == "bfs" || algo == "kcore" || algo == "bfs2") {
         vertex_t full = (vertex_t)p_s << bit_shift2;
         if (full > alloc) alloc = full;
     }
@@ -188,6 +192,30 @@ int main(int argc, char* argv[])
             pr.iteration_finalize(it);
         }
         write_out(out, pr.vert_rank_prior, V * sizeof(float));
+    } else if (algo == "bfs2") {
+        /* label-correcting BFS (bfs2.cpp:56-181): every tile each sweep,
+         * until a sweep changes nothing */
+        bfs2_t bf;
+        bf.init(alloc, (vertex_t)arg, g->read_part);
+        while (true) {
+            index_t fc = 0;
+            for_each_tile([&](edge_t* e, index_t c, part_t i, part_t j) { fc += bf.bfs_onepart(e, c, i, j); });
+            bf.front_count[0] += fc;
+            if (0 == bf.iteration_finalize()) break;
+        }
+        write_out(out, bf.depth, V);
+    } else if (algo == "traverse") {
+        /* single-colour propagation from pivot `arg`, colour 0
+         * (traverse.cpp:56-212) */
+        traverse_t tr;
+        tr.init(alloc, (vertex_t)arg, 0);
+        while (true) {
+            index_t fc = 0;
+            for_each_tile([&](edge_t* e, index_t c, part_t i, part_t j) { fc += tr.traverse_onepart(e, c, i, j); });
+            tr.front_count[0] += fc;
+            if (0 == tr.iteration_finalize()) break;
+        }
+        write_out(out, tr.vert_cid, V * sizeof(uint32_t));
     } else {
         fprintf(stderr, "unknown algo %s\n", algo.c_str());
         return 2;

@@ -12,6 +12,8 @@ wrote and the per-vertex arrays the reference's own code computed on them:
                  of each component                              (wcc.cpp)
   pr_compat_x    pr_t vert_rank_prior after 5 iterations        (pr.cpp),
                  i.e. with the reference's int32 inverse degree
+  bfs2_depth[r]  bfs2_t depth_t array for root bfs_roots[r]    (bfs2.cpp)
+  traverse_cid[r] traverse_t vert_cid from pivot bfs_roots[r]  (traverse.cpp)
 
 Graphs: Graph500 Kronecker (seeds 1, 2) and small hand-made edge lists that
 exercise several tile windows, a ragged last window, self-loops, duplicates,
@@ -88,6 +90,8 @@ def reference_arrays(prefix: Path, V: int, directed: bool, roots, ks):
         d["kcore_count"] = np.array(counts, np.int64)
     x, _ = O.ref_run(prefix, V, "pr", 5, directed)
     d["pr_compat_x"] = x
+    d["bfs2_depth"] = np.stack([O.ref_run(prefix, V, "bfs2", int(r), directed)[0] for r in roots])
+    d["traverse_cid"] = np.stack([O.ref_run(prefix, V, "traverse", int(r), directed)[0] for r in roots])
     return d
 
 

@@ -2,7 +2,7 @@
 
 The fixtures hold the reference's own outputs (tests/golden/make_golden.py):
 tile files written by the reference converter and the per-vertex arrays of
-its bfs_t / kcore_t / wcc2_t / pr_t classes.  Passing here pins the oracle
+its bfs_t / kcore_t / wcc2_t / pr_t / bfs2_t / traverse_t classes.  Passing here pins the oracle
 that the GPU parity tests then use at sizes the fixtures do not cover.
 """
 import numpy as np
@@ -71,6 +71,20 @@ def test_pagerank_compat_matches_reference(name, oracle_lib):
     ref = g["pr_compat_x"].astype(np.float64)
     denom = max(np.abs(x).sum(), 1e-300)
     assert np.abs(ref - x).sum() / denom <= 1e-6
+
+
+@pytest.mark.parametrize("name", GOLDEN_NAMES)
+def test_bfs2_and_traverse_match_reference(name, oracle_lib):
+    """-j 30 (bfs2_t) and -j 4 (traverse_t) from every fixture root."""
+    g = load_golden(name)
+    p, _, _ = oracle_lib.geometry(g["V"], g["directed"])
+    for r, root in enumerate(g["bfs_roots"]):
+        depth, _ = oracle_lib.bfs2(g["start"], g["grid"], p, g["directed"], g["V"], int(root))
+        assert np.array_equal(depth, g["bfs2_depth"][r]), f"root {root}"
+        assert np.array_equal(depth, g["bfs_depth"][r])          # the label-correcting BFS ends at BFS depth
+        cid, colored, _ = oracle_lib.traverse(g["start"], g["grid"], p, g["directed"], g["V"], int(root))
+        assert np.array_equal(cid, g["traverse_cid"][r]), f"pivot {root}"
+        assert colored == int(np.count_nonzero(cid == 0))
 
 
 def test_bfs_level_overflow_is_an_error(oracle_lib):
