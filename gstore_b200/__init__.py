@@ -27,9 +27,11 @@ import numpy as np
 PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "lib" / "libgstore_cuda.so"
 
-GS_ALGO_BFS, GS_ALGO_PAGERANK, GS_ALGO_KCORE, GS_ALGO_WCC = 0, 1, 2, 3
+GS_ALGO_BFS, GS_ALGO_PAGERANK, GS_ALGO_KCORE, GS_ALGO_WCC, GS_ALGO_BFS2, GS_ALGO_TRAVERSE = 0, 1, 2, 3, 4, 5
 ALGOS = {"bfs": GS_ALGO_BFS, "pagerank": GS_ALGO_PAGERANK, "pr": GS_ALGO_PAGERANK,
-         "kcore": GS_ALGO_KCORE, "wcc": GS_ALGO_WCC}
+         "kcore": GS_ALGO_KCORE, "wcc": GS_ALGO_WCC, "bfs2": GS_ALGO_BFS2, "traverse": GS_ALGO_TRAVERSE}
+_RESULT_DTYPE = {GS_ALGO_BFS: np.uint8, GS_ALGO_PAGERANK: np.float32, GS_ALGO_KCORE: np.int32,
+                 GS_ALGO_WCC: np.uint32, GS_ALGO_BFS2: np.uint8, GS_ALGO_TRAVERSE: np.uint32}
 STATUS = {0: "GS_OK", 1: "GS_ERR_CUDA", 2: "GS_ERR_OOM", 3: "GS_ERR_FORMAT", 4: "GS_ERR_TIMEOUT",
           5: "GS_ERR_ARG", 6: "GS_ERR_RANGE", 7: "GS_ERR_STATE", 8: "GS_ERR_UNSUPPORTED"}
 
@@ -302,8 +304,7 @@ class Batch:
 
     def download(self, qid: int, what: int = 0) -> np.ndarray:
         graph, a = self._graphs[qid]
-        dt = {GS_ALGO_BFS: np.uint8, GS_ALGO_PAGERANK: np.float32, GS_ALGO_KCORE: np.int32,
-              GS_ALGO_WCC: np.uint32}[a]
+        dt = _RESULT_DTYPE[a]
         out = np.empty(graph.V, dt)
         self.ctx._check(lib().gs_batch_download(self._h, qid, what, _ptr(out), out.nbytes))
         return out
@@ -384,8 +385,7 @@ class Server:
         """(result array or None, t_submit, t_done, steps); forgets the request."""
         gid, a = self._req.pop(rid)
         V = self._graphs[gid].V
-        dt = {GS_ALGO_BFS: np.uint8, GS_ALGO_PAGERANK: np.float32, GS_ALGO_KCORE: np.int32,
-              GS_ALGO_WCC: np.uint32}[a]
+        dt = _RESULT_DTYPE[a]
         out = np.empty(V, dt) if want_data else None
         ts, td, n = C.c_double(), C.c_double(), C.c_int64()
         self.ctx._check(lib().gs_serve_result(self._h, rid, _ptr(out), 0 if out is None else out.nbytes,
@@ -560,8 +560,7 @@ class State:
 
     def download(self, what: int = 0) -> np.ndarray:
         V = self.graph.V
-        dt = {GS_ALGO_BFS: np.uint8, GS_ALGO_PAGERANK: np.float32, GS_ALGO_KCORE: np.int32,
-              GS_ALGO_WCC: np.uint32}[self.algo]
+        dt = _RESULT_DTYPE[self.algo]
         out = np.empty(V, dt)
         self._check(lib().gs_download(self._h, what, _ptr(out), out.nbytes))
         return out

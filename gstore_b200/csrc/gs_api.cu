@@ -93,7 +93,7 @@ void gs_timer_end(gs_ctx* ctx, int algo, uint64_t bytes) {
     cudaEventSynchronize(ctx->ev1);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-    KernelTimes& k = ctx->ktime[algo & 3];
+    KernelTimes& k = ctx->ktime[algo & 7];
     k.launches += 1;
     k.ms += ms;
     k.bytes += bytes;
@@ -614,6 +614,8 @@ gs_status gs_state_create(gs_graph* g, gs_algo algo, int64_t arg, gs_state** out
     if (algo == GS_ALGO_BFS && (arg < 0 || (uint64_t)arg >= g->V))
         return gs_fail(ctx, GS_ERR_ARG, "BFS root out of range");
     if (algo == GS_ALGO_PAGERANK && arg < 1) return gs_fail(ctx, GS_ERR_ARG, "iterations < 1");
+    if ((algo == GS_ALGO_BFS2 || algo == GS_ALGO_TRAVERSE) && (arg < 0 || (uint64_t)arg >= g->V))
+        return gs_fail(ctx, GS_ERR_ARG, "root out of range");
     gs_state* s = new (std::nothrow) gs_state();
     if (!s) return GS_ERR_OOM;
     s->g = g;
@@ -625,6 +627,8 @@ gs_status gs_state_create(gs_graph* g, gs_algo algo, int64_t arg, gs_state** out
         case GS_ALGO_PAGERANK: st = pr_init(s); break;
         case GS_ALGO_WCC: st = wcc_init(s); break;
         case GS_ALGO_KCORE: st = kcore_init(s); break;
+        case GS_ALGO_BFS2:
+        case GS_ALGO_TRAVERSE: st = lab_init(s); break;
     }
     if (st != GS_OK) {
         gs_state_free(s);
@@ -637,7 +641,8 @@ gs_status gs_state_create(gs_graph* g, gs_algo algo, int64_t arg, gs_state** out
 gs_status gs_state_reset(gs_state* s, int64_t arg) {
     if (!s) return GS_ERR_ARG;
     gs_graph* g = s->g;
-    if (s->algo == GS_ALGO_BFS && (arg < 0 || (uint64_t)arg >= g->V))
+    if ((s->algo == GS_ALGO_BFS || s->algo == GS_ALGO_BFS2 || s->algo == GS_ALGO_TRAVERSE) &&
+        (arg < 0 || (uint64_t)arg >= g->V))
         return gs_fail(g->ctx, GS_ERR_ARG, "BFS root out of range");
     if (s->algo == GS_ALGO_PAGERANK && arg < 1) return gs_fail(g->ctx, GS_ERR_ARG, "iterations < 1");
     s->arg = arg;
@@ -650,6 +655,8 @@ gs_status gs_state_reset(gs_state* s, int64_t arg) {
         case GS_ALGO_PAGERANK: return pr_init(s);
         case GS_ALGO_WCC: return wcc_init(s);
         case GS_ALGO_KCORE: return kcore_init(s);
+        case GS_ALGO_BFS2:
+        case GS_ALGO_TRAVERSE: return lab_init(s);
     }
     return GS_ERR_ARG;
 }
@@ -669,6 +676,7 @@ gs_status gs_state_free(gs_state* s) {
     gs_dev_free(s->d_touched);
     gs_dev_free(s->d_deg);
     gs_dev_free(s->d_kactive);
+    gs_dev_free(s->d_lab);
     gs_dev_free(s->d_error);
     gs_dev_free(s->d_fv);
     gs_dev_free(s->d_uflags);
@@ -693,6 +701,8 @@ static gs_status sweep_launch(gs_state* s) {
         case GS_ALGO_PAGERANK: return pr_sweep_launch(s);
         case GS_ALGO_WCC: return wcc_sweep_launch(s);
         case GS_ALGO_KCORE: return kcore_sweep_launch(s);
+        case GS_ALGO_BFS2:
+        case GS_ALGO_TRAVERSE: return lab_sweep_launch(s);
     }
     return GS_ERR_ARG;
 }
@@ -709,13 +719,14 @@ gs_status gs_sweep(gs_state* s, const gs_segment* segs, int n_segs) {
         // once per sweep, however many segment calls make it up
         if (s->algo == GS_ALGO_BFS) GS_TRY(bfs_sweep_begin(s));
         if (s->algo == GS_ALGO_WCC) GS_TRY(wcc_sweep_begin(s));
+        if (s->algo == GS_ALGO_BFS2 || s->algo == GS_ALGO_TRAVERSE) GS_TRY(lab_sweep_begin(s));
         s->swept = true;
     }
     auto launch = [s]() { return sweep_launch(s); };
     if (n_segs > 0) return gs_each_part(g, segs, n_segs, launch);
     gs_need need;
     std::vector<uint8_t> act;
-    if (g->stream && (s->algo == GS_ALGO_BFS || s->algo == GS_ALGO_KCORE)) {
+    if (g->stream && s->algo != GS_ALGO_PAGERANK && s->algo != GS_ALGO_WCC) {
         // the window flags the skip rule reads: BFS frontier windows
         // (bfs.cpp:290-312), k-core windows of removed vertices
         // (gstore.cpp:2773-2782)
@@ -723,7 +734,8 @@ gs_status gs_sweep(gs_state* s, const gs_segment* segs, int n_segs) {
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(act.data(), s->d_act, g->nw, cudaMemcpyDeviceToHost, ctx->stream));
         GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         need.act = act.data();
-        need.by_col = !g->directed;
+        // traverse colours v1 from v0 only: its tiles follow their row window
+        need.by_col = !g->directed && s->algo != GS_ALGO_TRAVERSE;
     }
     return gs_each_segment(g, need, s->step & 1, launch);
 }
@@ -742,6 +754,8 @@ gs_status gs_finalize(gs_state* s, int64_t* frontier_out, int* done_out) {
         case GS_ALGO_PAGERANK: st = pr_finalize(s, &f, &d); break;
         case GS_ALGO_WCC: st = wcc_finalize(s, &f, &d); break;
         case GS_ALGO_KCORE: st = kcore_finalize(s, &f, &d); break;
+        case GS_ALGO_BFS2:
+        case GS_ALGO_TRAVERSE: st = lab_finalize(s, &f, &d); break;
     }
     if (st != GS_OK) return st;
     s->last_count = f;
@@ -783,6 +797,19 @@ gs_status gs_download(gs_state* s, int what, void* host_dst, uint64_t bytes) {
         case GS_ALGO_BFS: src = s->d_depth; need = g->V; break;
         case GS_ALGO_PAGERANK: src = what == 1 ? s->d_x : s->d_r; need = g->V * 4; break;
         case GS_ALGO_KCORE: src = s->d_deg; need = g->V * 4; break;
+        case GS_ALGO_TRAVERSE: src = s->d_lab; need = g->V * 4; break;
+        case GS_ALGO_BFS2: {
+            GS_TRY(gs_dev_alloc(ctx, (void**)&tmp, g->N));
+            uint64_t cnt;
+            gs_status st = lab_result(s, (uint8_t*)tmp, &cnt);
+            if (st != GS_OK) {
+                gs_dev_free(tmp);
+                return st;
+            }
+            src = tmp;
+            need = g->V;
+            break;
+        }
         case GS_ALGO_WCC: {
             GS_TRY(gs_dev_alloc(ctx, (void**)&tmp, g->N * 4));
             uint64_t cnt;
@@ -823,6 +850,8 @@ gs_status gs_result_count(gs_state* s, uint64_t* count) {
             return st;
         }
         case GS_ALGO_PAGERANK: *count = (uint64_t)s->step; return GS_OK;
+        case GS_ALGO_BFS2:
+        case GS_ALGO_TRAVERSE: return lab_result(s, nullptr, count);
     }
     return GS_ERR_ARG;
 }

@@ -115,7 +115,7 @@ struct gs_ctx {
     bool own_stream = false;
     std::string err;
     bool profile = false;
-    KernelTimes ktime[4];
+    KernelTimes ktime[8];
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint64_t* d_scalars = nullptr;   // small device scratch for counters/flags
     uint64_t* h_scalars = nullptr;   // pinned mirror
@@ -197,6 +197,8 @@ struct gs_state {
     // k-core
     int32_t* d_deg = nullptr;        // N
     uint32_t* d_kactive = nullptr;   // N/32
+    // bfs2 / traverse
+    uint32_t* d_lab = nullptr;       // N: depth (bfs2) or colour (traverse)
     int64_t last_count = 0;
 };
 
@@ -297,6 +299,13 @@ gs_status gs_each_part(gs_graph* g, const gs_segment* segs, int n_segs, F launch
 gs_status gs_stream_open(gs_graph* g, const uint32_t* host_grid, uint64_t segment_bytes);
 void gs_stream_close(gs_graph* g);
 const uint32_t* gs_stream_records(const gs_graph* g);   // host records of a streamed graph
+
+// bfs2 (-j 30) and traverse (-j 4): one u32 label per vertex in d_lab
+gs_status lab_init(gs_state* s);
+gs_status lab_sweep_begin(gs_state* s);
+gs_status lab_sweep_launch(gs_state* s);
+gs_status lab_finalize(gs_state* s, int64_t* frontier, int* done);
+gs_status lab_result(gs_state* s, uint8_t* d_out, uint64_t* count);
 
 gs_status gs_count_reached(gs_state* s, uint64_t* reached, uint64_t* edges_in_component);
 gs_status gs_count_kcore(gs_state* s, uint64_t* members);

@@ -237,6 +237,106 @@ __global__ void count_nonzero_kernel(const int32_t* __restrict__ deg, uint64_t n
     warp_add_u64(out, local);
 }
 
+// ------------------------------------------------------ bfs2, traverse --
+constexpr uint32_t kInf = 0xFFFFFFFFu;
+
+// bfs2_t::bfs_onepart (bfs2.cpp:102-117): a record lowers the depth of an end
+// to the other end's depth + 1 (depth 1 = root, kInf = unreached).  A tile is
+// swept when its row or column window changed in the previous sweep (all
+// windows before the first); a change marks its window for the next one.
+struct Bfs2Op {
+    uint32_t* dist;
+    const uint8_t* act;
+    uint8_t* act_next;
+    unsigned long long* changes;
+    int* overflow;
+    int directed;
+    struct Item {
+        uint32_t rb, cb, n;
+        bool cr, cc;
+    };
+    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
+        c.rb = row << 16;
+        c.cb = col << 16;
+        c.n = 0;
+        c.cr = c.cc = false;
+        return act[row] || act[col];
+    }
+    __device__ void record(uint32_t r, Item& c) const {
+        const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
+        const uint32_t da = __ldcg(dist + a), db = __ldcg(dist + b);
+        if (da != kInf && (db == kInf || db > da + 1)) {
+            if (da >= 255) { *overflow = 1; return; }        // u8 depth_t
+            if (atomicMin(dist + b, da + 1) > da + 1) { ++c.n; c.cc = true; }
+        } else if (!directed && db != kInf && (da == kInf || da > db + 1)) {
+            if (db >= 255) { *overflow = 1; return; }
+            if (atomicMin(dist + a, db + 1) > db + 1) { ++c.n; c.cr = true; }
+        }
+    }
+    __device__ void end(uint32_t row, uint32_t col, Item& c) const {
+        warp_add_u64(changes, c.n);
+        const bool cr = __any_sync(kFull, c.cr), cc = __any_sync(kFull, c.cc);
+        if ((threadIdx.x & 31) == 0) {
+            if (cr) act_next[row] = 1;   // read_part_next->set_bit_atomic(i), bfs2.cpp:126-128
+            if (cc) act_next[col] = 1;   // bfs2.cpp:120-123
+        }
+    }
+};
+
+// traverse_t::traverse_onepart (traverse.cpp:173-188): a record colours v1
+// from v0 (one direction, also in the half grid).  A tile is swept when its
+// row window gained colour in the previous sweep (the pivot's window first).
+struct TraverseOp {
+    uint32_t* cid;
+    const uint8_t* act;
+    uint8_t* act_next;
+    unsigned long long* changes;
+    struct Item {
+        uint32_t rb, cb, n;
+        bool cc;
+    };
+    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
+        c.rb = row << 16;
+        c.cb = col << 16;
+        c.n = 0;
+        c.cc = false;
+        return act[row] != 0;
+    }
+    __device__ void record(uint32_t r, Item& c) const {
+        const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
+        if (__ldcg(cid + a) == 0 && __ldcg(cid + b) == kInf && atomicCAS(cid + b, kInf, 0u) == kInf) {
+            ++c.n;
+            c.cc = true;
+        }
+    }
+    __device__ void end(uint32_t, uint32_t col, Item& c) const {
+        warp_add_u64(changes, c.n);
+        if (__any_sync(kFull, c.cc) && (threadIdx.x & 31) == 0) act_next[col] = 1;
+    }
+};
+
+__global__ void lab_to_depth_kernel(const uint32_t* __restrict__ dist, uint8_t* __restrict__ depth, uint64_t V,
+                                    unsigned long long* reached) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t local = 0;
+    for (uint64_t v = tid; v < V; v += nth) {
+        const uint32_t d = dist[v];
+        if (depth) depth[v] = d == kInf ? 0 : (uint8_t)d;
+        local += d != kInf;
+    }
+    warp_add_u64(reached, local);
+}
+
+__global__ void count_value_kernel(const uint32_t* __restrict__ lab, uint64_t V, uint32_t value,
+                                   unsigned long long* out) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t local = 0;
+    for (uint64_t v = tid; v < V; v += nth) local += lab[v] == value;
+    warp_add_u64(out, local);
+}
+
 gs_status read_scalar(gs_ctx* ctx, uint64_t* value) {
     GS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->h_scalars, ctx->d_scalars, sizeof(uint64_t),
                                        cudaMemcpyDeviceToHost, ctx->stream));
@@ -436,4 +536,77 @@ gs_status gs_count_kcore(gs_state* s, uint64_t* members) {
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
     return read_scalar(ctx, members);
+}
+
+// ------------------------------------------------------- bfs2 / traverse ----
+gs_status lab_init(gs_state* s) {
+    gs_graph* g = s->g;
+    gs_ctx* ctx = g->ctx;
+    if (!s->d_lab) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_lab, g->N * 4));
+    if (!s->d_act) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_act, g->nw));
+    if (!s->d_act_next) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_act_next, g->nw));
+    if (!s->d_error) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_error, sizeof(uint64_t)));
+    const uint64_t v = (uint64_t)s->arg;
+    const bool bfs2 = s->algo == GS_ALGO_BFS2;
+    // bfs2: every vertex unreached, root depth 1, every window active
+    // (bfs2.cpp:56-78); traverse: invalid colour, pivot colour 0, the
+    // pivot's window active (traverse.cpp:56-72)
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_lab, 0xFF, g->N * 4, ctx->stream));
+    const uint32_t first = bfs2 ? 1u : 0u;
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(s->d_lab + v, &first, 4, cudaMemcpyHostToDevice, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_act, bfs2 ? 1 : 0, g->nw, ctx->stream));
+    if (!bfs2) GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_act + (v >> 16), 1, 1, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_act_next, 0, g->nw, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_error, 0, sizeof(uint64_t), ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // `first` lives on this stack frame
+    return GS_OK;
+}
+
+gs_status lab_sweep_begin(gs_state* s) { return zero_scalar(s->g->ctx); }
+
+gs_status lab_sweep_launch(gs_state* s) {
+    gs_graph* g = s->g;
+    unsigned long long* changes = (unsigned long long*)g->ctx->d_scalars;
+    if (s->algo == GS_ALGO_BFS2) {
+        Bfs2Op op{s->d_lab, s->d_act, s->d_act_next, changes, (int*)s->d_error, g->directed};
+        return launch_sweep(g, op, GS_ALGO_BFS2, 0, true);
+    }
+    TraverseOp op{s->d_lab, s->d_act, s->d_act_next, changes};
+    return launch_sweep(g, op, GS_ALGO_TRAVERSE, 0, true);
+}
+
+// iteration_finalize of bfs2_t / traverse_t (bfs2.cpp:130-181,
+// traverse.cpp:191-212): the sweep's changes; done when there were none.
+gs_status lab_finalize(gs_state* s, int64_t* frontier, int* done) {
+    gs_graph* g = s->g;
+    gs_ctx* ctx = g->ctx;
+    uint64_t changes = 0;
+    GS_TRY(read_scalar(ctx, &changes));
+    std::swap(s->d_act, s->d_act_next);
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_act_next, 0, g->nw, ctx->stream));
+    *frontier = (int64_t)changes;
+    *done = changes == 0;
+    if (s->algo == GS_ALGO_BFS2) {
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->h_scalars, s->d_error, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        if (ctx->h_scalars[0]) return gs_fail(ctx, GS_ERR_RANGE, "bfs2 exceeds 254 levels (u8 depth_t)");
+    }
+    return GS_OK;
+}
+
+// bfs2: u8 depth into d_out (may be null) and the reached count; traverse:
+// the number of vertices with colour 0.
+gs_status lab_result(gs_state* s, uint8_t* d_out, uint64_t* count) {
+    gs_graph* g = s->g;
+    gs_ctx* ctx = g->ctx;
+    GS_TRY(zero_scalar(ctx));
+    if (s->algo == GS_ALGO_BFS2)
+        lab_to_depth_kernel<<<blocks_for(g->V, ctx), kThreads, 0, ctx->stream>>>(
+            s->d_lab, d_out, g->V, (unsigned long long*)ctx->d_scalars);
+    else
+        count_value_kernel<<<blocks_for(g->V, ctx), kThreads, 0, ctx->stream>>>(
+            s->d_lab, g->V, 0u, (unsigned long long*)ctx->d_scalars);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    ctx->launches++;
+    return read_scalar(ctx, count);
 }

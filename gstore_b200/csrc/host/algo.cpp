@@ -1,5 +1,6 @@
 #include "algo.h"
 
+#include <algorithm>
 #include <iostream>
 
 algo_t::~algo_t() {
@@ -116,4 +117,46 @@ int wcc2_t::iteration_finalize() {
         return 0;
     }
     return 1;
+}
+
+// ----------------------------------------------------------------- bfs2 ---
+void bfs2_t::init(gs_ctx* ctx, gs_graph* g, vertex_t root) {
+    ctx_ = ctx;
+    check(gs_state_create(g, GS_ALGO_BFS2, (int64_t)root, &st_));
+    level = 1;
+    std::cout << "Root = " << root << std::endl;   // bfs2.cpp:75
+}
+
+void bfs2_t::algo_mem_part(segment* seg) { sweep(seg); }
+
+int bfs2_t::iteration_finalize() {
+    if (status_ != GS_OK) return 0;
+    int64_t changed = 0;
+    int done = 0;
+    if (!check(gs_finalize(st_, &changed, &done))) return 0;
+    std::cout << "level: " << (int)level << " frontier count: " << changed << std::endl;   // bfs2.cpp:140-141
+    if (done) return 0;
+    ++level;
+    return (int)std::min<int64_t>(changed, 1 << 30);
+}
+
+// ------------------------------------------------------------- traverse ---
+void traverse_t::init(gs_ctx* ctx, gs_graph* g, vertex_t pivot) {
+    ctx_ = ctx;
+    check(gs_state_create(g, GS_ALGO_TRAVERSE, (int64_t)pivot, &st_));
+    iteration = 0;
+}
+
+void traverse_t::algo_mem_part(segment* seg) { sweep(seg); }
+
+int traverse_t::iteration_finalize() {
+    if (status_ != GS_OK) return 0;
+    int64_t colored = 0;
+    int done = 0;
+    if (!check(gs_finalize(st_, &colored, &done))) return 0;
+    // traverse.cpp:199-201
+    std::cout << "level: " << iteration << " frontier count: " << colored << std::endl << std::endl;
+    if (done) return 0;
+    ++iteration;
+    return (int)std::min<int64_t>(colored, 1 << 30);
 }

@@ -105,3 +105,21 @@ public:
     int iteration_finalize() override;   // 0 once no label changed
     uint64_t wcc_count = 0;
 };
+
+// bfs2_t (bfs2.h:38-52): label-correcting BFS ("-j 30").
+class bfs2_t : public algo_t {
+public:
+    void init(gs_ctx* ctx, gs_graph* g, vertex_t root);
+    void algo_mem_part(segment* seg) override;
+    int iteration_finalize() override;   // changes in the sweep; 0 ends the run
+    uint8_t level = 1;
+};
+
+// traverse_t (traverse.h:38-50): single-colour propagation ("-j 4").
+class traverse_t : public algo_t {
+public:
+    void init(gs_ctx* ctx, gs_graph* g, vertex_t pivot);
+    void algo_mem_part(segment* seg) override;
+    int iteration_finalize() override;   // vertices coloured in the sweep; 0 ends the run
+    int iteration = 0;
+};

@@ -13,8 +13,8 @@
 //
 // Differences, by design: "-s" below 24 maps to one tile group instead of
 // wrapping to 2^32 groups (gstore.cpp:145-146 computes 1 << (scale - 24) in
-// unsigned arithmetic); jobs 4, 30, 100 and converter modes other than 1/6
-// are not part of this engine.
+// unsigned arithmetic); job 100 and converter modes other than 1/6 are not
+// part of this engine.
 #include <getopt.h>
 #include <sys/time.h>
 
@@ -125,6 +125,38 @@ static int run_kcore(gs_ctx* ctx, gs_graph* g, int kc) {
     return 0;
 }
 
+static int run_bfs2(gs_ctx* ctx, gs_graph* g, uint64_t root) {
+    bfs2_t bf;
+    bf.init(ctx, g, root);
+    if (bf.status() != GS_OK) return fail(ctx, "bfs2 init");
+    while (true) {
+        bf.algo_mem_part(nullptr);
+        const int more = bf.iteration_finalize();
+        if (bf.status() != GS_OK) return fail(ctx, "bfs2");
+        if (0 == more) break;
+    }
+    uint64_t reached = 0;
+    gs_result_count(bf.state(), &reached);
+    std::cout << "reached vertices = " << reached << std::endl;
+    return 0;
+}
+
+static int run_traverse(gs_ctx* ctx, gs_graph* g, uint64_t pivot) {
+    traverse_t tr;
+    tr.init(ctx, g, pivot);
+    if (tr.status() != GS_OK) return fail(ctx, "traverse init");
+    while (true) {
+        tr.algo_mem_part(nullptr);
+        const int more = tr.iteration_finalize();
+        if (tr.status() != GS_OK) return fail(ctx, "traverse");
+        if (0 == more) break;
+    }
+    uint64_t colored = 0;
+    gs_result_count(tr.state(), &colored);
+    std::cout << "coloured vertices = " << colored << std::endl;
+    return 0;
+}
+
 static int run_wcc(gs_ctx* ctx, gs_graph* g) {
     wcc2_t w;
     w.init(ctx, g);
@@ -223,13 +255,15 @@ int main(int argc, char* argv[]) {
     const bool pr = job == 1 || job == 11 || job == 21;
     const bool kc = job == 2 || job == 12 || job == 22;
     const bool wcc = job == 3 || job == 13 || job == 23;
-    if (!(bfs || pr || kc || wcc)) {
-        if (job == 4 || job == 30 || job == 100) std::cout << "job " << job << " is not provided by this engine" << std::endl;
+    const bool bfs2 = job == 30;   // gstore.cpp:257-263
+    const bool trav = job == 4;    // gstore.cpp:334-341
+    if (!(bfs || pr || kc || wcc || bfs2 || trav)) {
+        if (job == 100) std::cout << "job " << job << " is not provided by this engine" << std::endl;
         else std::cout << "Wrong value for -j argument" << std::endl;
         return 1;
     }
     // Jobs 2x exclude file loading from the printed time (gstore.cpp:250-333).
-    const bool exclude_load = job >= 20;
+    const bool exclude_load = job >= 20 && job < 30;
     const bool want_degree = pr || kc;
     double start = mywtime();
     tile_files tf;
@@ -239,7 +273,7 @@ int main(int argc, char* argv[]) {
     // segments, gstore.cpp:3044-3119): a grid above the budget streams from
     // host memory through two HBM segments.  The mmap and in-memory jobs
     // (1x, 2x) keep the grid resident.
-    const uint64_t budget = job < 10 ? o.total_size : 0;
+    const uint64_t budget = (job < 10 || job == 30) ? o.total_size : 0;
     gs_ctx* ctx = nullptr;
     if (gs_create(&ctx, 0, budget, kDirected) != GS_OK) return fail(nullptr, "no usable CUDA device");
     gs_graph* g = nullptr;
@@ -259,6 +293,12 @@ int main(int argc, char* argv[]) {
         } else if (kc) {
             rc = run_kcore(ctx, g, o.arg);
             label = "Kcore time = ";
+        } else if (bfs2) {
+            rc = run_bfs2(ctx, g, o.arg == -1 ? 1 : (uint64_t)o.arg);   // gstore.cpp:1913-1914
+            label = "Half BFS time = ";
+        } else if (trav) {
+            rc = run_traverse(ctx, g, o.arg == -1 ? 1 : (uint64_t)o.arg);   // gstore.cpp:2172-2173
+            label = "Single color propagation time = ";
         } else {
             rc = run_wcc(ctx, g);
             label = "WCC time = ";

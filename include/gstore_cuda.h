@@ -53,7 +53,9 @@ typedef enum gs_algo {
     GS_ALGO_BFS = 0,      /* bfs_t   (bfs.cpp)   arg = root                 */
     GS_ALGO_PAGERANK = 1, /* pr_t    (pr.cpp)    arg = iterations           */
     GS_ALGO_KCORE = 2,    /* kcore_t (kcore.cpp) arg = k                    */
-    GS_ALGO_WCC = 3       /* wcc2_t  (wcc.cpp)   arg unused                 */
+    GS_ALGO_WCC = 3,      /* wcc2_t  (wcc.cpp)   arg unused                 */
+    GS_ALGO_BFS2 = 4,     /* bfs2_t  (bfs2.cpp)  arg = root ("-j 30")       */
+    GS_ALGO_TRAVERSE = 5  /* traverse_t (traverse.cpp) arg = pivot ("-j 4") */
 } gs_algo;
 
 typedef struct gs_ctx gs_ctx;
@@ -135,9 +137,10 @@ gs_status gs_graph_info(const gs_graph* g, uint64_t* n_edges, uint64_t* n_tiles,
 gs_status gs_graph_degree(const gs_graph* g, int32_t* host_degree);
 
 /* ------------------------------------------------- algo_t plug-in layer --- */
-/* Replaces: bfs_t/pr_t/kcore_t/wcc2_t ::init (bfs.cpp:56-75, pr.cpp:82-117,
- * kcore.cpp:55-61, wcc.cpp:57-83).  arg: BFS root, PageRank iterations,
- * k-core k; unused for WCC.  The state lives in HBM. */
+/* Replaces: bfs_t/pr_t/kcore_t/wcc2_t/bfs2_t/traverse_t ::init (bfs.cpp:56-75,
+ * pr.cpp:82-117, kcore.cpp:55-61, wcc.cpp:57-83, bfs2.cpp:56-78,
+ * traverse.cpp:56-72).  arg: BFS / BFS2 root, PageRank iterations, k-core k,
+ * TRAVERSE pivot; unused for WCC.  The state lives in HBM. */
 gs_status gs_state_create(gs_graph* g, gs_algo algo, int64_t arg, gs_state** out);
 gs_status gs_state_free(gs_state* s);
 /* Re-initialise a state for a new run (new root / iterations / k) without
@@ -159,7 +162,10 @@ gs_status gs_finalize(gs_state* s, int64_t* frontier_out, int* done_out);
  * steps_out: number of sweeps. */
 gs_status gs_run(gs_state* s, int64_t* steps_out);
 
-/* Results.  BFS: uint8 depth[V] (root 1, unreached 0, bfs.cpp:54).
+/* Results.  BFS and BFS2: uint8 depth[V] (root 1, unreached 0, bfs.cpp:54;
+ * the label-correcting bfs2 ends at the same depths).  TRAVERSE: uint32
+ * cid[V], 0 for vertices reached from the pivot along records v0 -> v1,
+ * 0xFFFFFFFF for the others (traverse.cpp:56-188).
  * PageRank: float rank[V] = 0.15 + 0.85 s after the last iteration
  * (what = 0) or float x[V] = rank * inv_degree (what = 1, the reference's
  * vert_rank_prior after its final swap).  k-core: int32 degree[V] (final,
@@ -167,8 +173,9 @@ gs_status gs_run(gs_state* s, int64_t* steps_out);
  * the smallest vertex id of the component, 0xFFFFFFFF for vertices without
  * records (wcc.cpp:54). */
 gs_status gs_download(gs_state* s, int what, void* host_dst, uint64_t bytes);
-/* Scalar summary: BFS reached vertices, k-core members (deg != 0,
- * gstore.cpp:2796-2803), WCC component count (wcc.cpp:324-336). */
+/* Scalar summary: BFS / BFS2 reached vertices, k-core members (deg != 0,
+ * gstore.cpp:2796-2803), WCC component count (wcc.cpp:324-336), TRAVERSE
+ * vertices with colour 0. */
 gs_status gs_result_count(gs_state* s, uint64_t* count);
 /* BFS: records with both endpoints reached (the GTEPS numerator) and the
  * records swept per level under the reference's tile-skip rule. */

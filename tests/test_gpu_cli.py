@@ -1,8 +1,8 @@
 """The gstoreu command line on the GPU, beside the reference's own gstoreu
 (compiled from its sources into oracle/_ref): the -c 1 converter writes the
 same .start/.degree bytes and the same records per tile, and the jobs print
-the reference's result lines (k-core members, WCC count) and the known BFS
-level counts of Graph500 Kron 16 from root 1."""
+the reference's result lines (k-core members, WCC count, the coloured set
+of -j 4) and the known BFS level counts of Graph500 Kron 16 from root 1."""
 import re
 import subprocess
 from pathlib import Path
@@ -66,3 +66,12 @@ def test_jobs_print_reference_results(kron16):
     assert "Half BFS time = " in bfs
     pr = run(OURS, "-s", 24, "-j", 21, "-a", 5, "-i", prefix)
     assert "Page-rank_mmap time = " in pr
+    # -j 30: label-correcting BFS from 1 reaches what -j 20 reaches
+    bfs2 = run(OURS, "-s", 24, "-j", 30, "-i", prefix)
+    assert "reached vertices = %d" % (1 + sum(counts)) in bfs2 and "Half BFS time = " in bfs2
+    # -j 4: the reference's coloured set from pivot 1 has 1 + sum(frontier counts) vertices
+    ours = run(OURS, "-s", 24, "-j", 4, "-i", prefix)
+    ref = run(REF / "gstoreu", "-s", 24, "-j", 4, "-i", d / "ref")
+    ref_colored = 1 + sum(int(c) for c in re.findall(r"frontier count: (\d+)", ref))
+    assert "coloured vertices = %d" % ref_colored in ours
+    assert "Single color propagation time = " in ours

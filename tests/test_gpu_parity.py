@@ -248,3 +248,40 @@ def test_pagerank_edgefactor32_matches_oracle(iterations, gpu_ctx_factory, oracl
     r, x = g.pagerank(iterations)
     assert rel_l1(r, r64) <= PR_TOL and rel_l1(x, x64) <= PR_TOL
     g.free()
+
+
+@pytest.mark.parametrize("name", GOLDEN_NAMES)
+def test_bfs2_and_traverse_golden(name, gpu_ctx_factory):
+    """-j 30 (label-correcting BFS) and -j 4 (single-colour propagation)
+    against the reference's bfs2_t / traverse_t arrays, resident and
+    streamed."""
+    g = load_golden(name)
+    ctx = gpu_ctx_factory(g["directed"])
+    graphs = [ctx.upload(g["start"], g["grid"], g["degree"], g["V"]),
+              ctx.upload_streamed(g["start"], g["grid"], g["degree"], g["V"], 2 * (131072 + 8) * 4)]
+    for graph in graphs:
+        for r, root in enumerate(g["bfs_roots"]):
+            with graph.state("bfs2", int(root)) as s:
+                s.run()
+                assert np.array_equal(s.download(), g["bfs2_depth"][r]), f"root {root}"
+                assert s.count() == int(np.count_nonzero(g["bfs2_depth"][r]))
+            with graph.state("traverse", int(root)) as s:
+                s.run()
+                assert np.array_equal(s.download(), g["traverse_cid"][r]), f"pivot {root}"
+                assert s.count() == int(np.count_nonzero(g["traverse_cid"][r] == 0))
+        graph.free()
+
+
+def test_bfs2_and_traverse_kron20(kron, oracle_lib):
+    k = kron[20]
+    p, _, _ = oracle_lib.geometry(k["V"])
+    nz = np.nonzero(k["degree"])[0]
+    for root in [1, int(nz[len(nz) // 3])]:
+        with k["graph"].state("bfs2", root) as s:
+            s.run()
+            assert np.array_equal(s.download(), k["graph"].bfs(root))
+        cid_o, colored_o, _ = oracle_lib.traverse(k["start"], k["grid"], p, False, k["V"], root)
+        with k["graph"].state("traverse", root) as s:
+            s.run()
+            assert np.array_equal(s.download(), cid_o)
+            assert s.count() == colored_o

@@ -72,4 +72,4 @@ def test_bad_edge_list_is_rejected(tmp_path):
 
 def test_unsupported_modes():
     assert "not provided" in run("gstoreu", "-v", 100, "-c", 2, "-i", "x").stderr
-    assert "not provided" in run("gstoreu", "-v", 100, "-j", 30, "-i", "x").stdout
+    assert "not provided" in run("gstoreu", "-v", 100, "-j", 100, "-i", "x").stdout
