@@ -2,35 +2,32 @@
 // resident graphs, admitted by HBM footprint and batched continuously.
 //
 // The reference answers one query per process run (gstore.cpp:250-333).
-// Here a server keeps many requests in flight and advances all of them one
-// iteration per step:
+// Here a server keeps many requests in flight:
 //
-//   step = [ table upload | counter reset | sweep kernel | post kernel |
-//            counter readback ]
+//   * BFS requests on one graph share a multi-source BFS: up to 64 of them as
+//     bits of 64-bit frontier words, each bit with its own level, so requests
+//     join a running group at any step (bfs_onepart for all bits,
+//     bfs.cpp:138-185; iteration_finalize, bfs.cpp:187-224).  A step
 //
-// captured once as a CUDA graph and replayed every step; the host rewrites
-// the job table (pinned) between steps.  The sweep kernel walks the
-// concatenated run lists of every job, the post kernel the concatenated
-// 32-vertex words, so requests on graphs of different sizes share each
-// launch.  Jobs:
-//   BFS     one job per graph: up to 64 requests as bits of 64-bit frontier
-//           words (a multi-source BFS whose requests start at different
-//           steps; each bit keeps its own level), sweep = bfs_onepart for
-//           all bits (bfs.cpp:138-185), post = iteration_finalize
-//           (bfs.cpp:187-224)
-//   WCC     sweep = hooking (wcc.cpp:177-278), post = pointer jumping
-//           (wcc.cpp:372-390); done when a sweep changes nothing
-//   k-core  post = round (kcore.cpp:179-217; the first step is a round
-//           only, as kcore_mmap starts with iteration_finalize), sweep =
-//           decrements (kcore.cpp:63-177); done when a round removes nothing
-//   PR      not a table job: each step runs its row-slice sweep
-//           (pagerank_onepart, pr.cpp:119-154) and update (pr.cpp:229-303)
-//           on a lower-priority side stream beside the step graph; done
-//           after `arg` iterations
-// Between steps the host retires finished requests (their results are
-// copied to pinned host buffers), admits queued ones while their state fits
-// the HBM budget and a slot is free, and attaches a request to an identical
-// one already queued or running (same graph, algorithm and argument).
+//       [ table upload | counter reset | sweep kernel | post kernel |
+//         counter readback ]
+//
+//     is captured once as a CUDA graph and replayed; the host rewrites the
+//     pinned job table between steps, the sweep kernel walks the
+//     concatenated runs of every group, the post kernel their vertex words.
+//   * WCC, k-core and PageRank requests run to completion on side streams
+//     (lower priority), beside the steps: chunks of iterations are queued
+//     without waiting, each kernel first reading the request's device-side
+//     done flag, and the host polls one event per chunk.  WCC: hooking sweep
+//     (wcc.cpp:177-278) + pointer jumping (wcc.cpp:372-390), done when a
+//     sweep changed nothing; k-core: round (kcore.cpp:179-217, first) +
+//     decrement sweep (kcore.cpp:63-177), done when a round removed
+//     nothing; PageRank: row-slice sweep + update, `arg` iterations.
+//
+// Between steps the host retires finished requests (results copied to
+// pinned host buffers), admits queued ones while their state fits the HBM
+// budget and a slot is free, and attaches a request to an identical one
+// already queued or running (same graph, algorithm and argument).
 #include "gs_internal.cuh"
 #include "gs_ops.cuh"
 
@@ -53,34 +50,29 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kSlots = 64;
 constexpr int kMaxJobs = 256;
 constexpr int kCounters = 4;
-
-enum JobKind : int { kJobBfs = 0, kJobWcc = 1, kJobKcore = 2 };
-constexpr int kFlagFirst = 1;      // WCC: first sweep (labels every end); k-core: round only
+constexpr int kSideSlots = 64;
+constexpr int kSideStreams = 8;
+constexpr int kWccChunk = 4;        // iterations queued per chunk
+constexpr int kKcoreChunk = 8;
 
 typedef FvPair<unsigned long long> Fv64;
 
+// One BFS group of the step table.
 struct Job {
     const gs_tile_run* runs;
     const gs_unit* units;
     const uint32_t* rec;
-    uint64_t R, words, N, V;
+    uint64_t R, words;
     uint64_t run_beg, word_beg;   // offsets in the concatenated lists
     uint32_t nw;
-    int kind, flags, k, directed;
-    // BFS group
+    int directed;
     Fv64* fv;
     unsigned long long* next;
     uint8_t* depth;               // [N][64]
     uint8_t* act_cur;
     uint8_t* act_next;
-    // WCC
-    uint32_t* parent;
-    uint8_t* touched;
-    // k-core
-    int32_t* deg;
-    uint32_t* removed;
     unsigned long long* cnt;      // kCounters per job
-    uint8_t level[kSlots];        // BFS: frontier depth per slot (0 = slot idle)
+    uint8_t level[kSlots];        // frontier depth per slot (0 = slot idle)
 };
 
 struct Table {
@@ -107,39 +99,18 @@ __global__ void __launch_bounds__(kThreads) serve_sweep_kernel(const Table* __re
     // the flags the post kernel sets start empty
     for (int j = blockIdx.x; j < n_jobs; j += gridDim.x) {
         const Job& jb = t->jobs[j];
-        if (jb.act_next)
-            for (uint32_t w = threadIdx.x; w < jb.nw; w += blockDim.x) jb.act_next[w] = 0;
+        for (uint32_t w = threadIdx.x; w < jb.nw; w += blockDim.x) jb.act_next[w] = 0;
     }
     for (uint64_t x = blockIdx.x; x < t->total_runs; x += gridDim.x) {
         const Job& jb = t->jobs[job_of(t, x, false)];
         const gs_tile_run run = jb.runs[x - jb.run_beg];
-        switch (jb.kind) {
-            case kJobBfs: {
-                const uint32_t row = jb.units[run.unit_beg].rc >> 16;
-                const bool ar = jb.act_cur[row] != 0;
-                const MsOp<unsigned long long> op{jb.fv, jb.next, jb.directed};
-                for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps) {
-                    const gs_unit d = jb.units[ui];
-                    if (!ar && (jb.directed || !jb.act_cur[d.rc & 0xFFFFu])) continue;
-                    sweep_unit(d, jb.rec, op, lane);
-                }
-                break;
-            }
-            case kJobWcc: {
-                const WccOp op{jb.parent, (jb.flags & kFlagFirst) ? jb.touched : nullptr, jb.cnt};
-                for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps)
-                    sweep_unit(jb.units[ui], jb.rec, op, lane);
-                break;
-            }
-            case kJobKcore: {
-                if (jb.flags & kFlagFirst) break;
-                const KcoreOpL2 op{jb.deg, jb.removed, jb.act_cur};
-                for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps)
-                    sweep_unit(jb.units[ui], jb.rec, op, lane);
-                break;
-            }
-            default:
-                break;
+        const uint32_t row = jb.units[run.unit_beg].rc >> 16;
+        const bool ar = jb.act_cur[row] != 0;
+        const MsOp<unsigned long long> op{jb.fv, jb.next, jb.directed};
+        for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps) {
+            const gs_unit d = jb.units[ui];
+            if (!ar && (jb.directed || !jb.act_cur[d.rc & 0xFFFFu])) continue;
+            sweep_unit(d, jb.rec, op, lane);
         }
     }
 }
@@ -150,63 +121,105 @@ __global__ void __launch_bounds__(kThreads) serve_post_kernel(const Table* __res
     const uint64_t nwarps = (uint64_t)gridDim.x * kWarps;
     for (uint64_t x = gwarp; x < t->total_words; x += nwarps) {
         const Job& jb = t->jobs[job_of(t, x, true)];
-        const uint64_t w = x - jb.word_beg;
-        const uint64_t v = w * 32 + lane;
-        switch (jb.kind) {
-            case kJobBfs: {
-                const unsigned long long nx = jb.next[v];
-                const Fv64 s = load_fv(jb.fv + v);
-                unsigned long long fresh = 0, over = 0;
-                if (nx || s.f) {
-                    if (nx) jb.next[v] = 0;
-                    fresh = nx & ~s.vis;
-                    store_fv(jb.fv + v, fresh, s.vis | fresh);
-                    if (fresh) {
-                        jb.act_next[v >> 16] = 1;
-                        unsigned long long m = fresh;
-                        while (m) {
-                            const int q = __ffsll((long long)m) - 1;
-                            const int d = jb.level[q] + 1;
-                            if (d >= 255) over |= 1ull << q;   // bfs.cpp level limit (u8 depth_t)
-                            else jb.depth[v * kSlots + q] = (uint8_t)d;
-                            m &= m - 1;
-                        }
-                    }
+        const uint64_t v = (x - jb.word_beg) * 32 + lane;
+        const unsigned long long nx = jb.next[v];
+        const Fv64 s = load_fv(jb.fv + v);
+        unsigned long long fresh = 0, over = 0;
+        if (nx || s.f) {
+            if (nx) jb.next[v] = 0;
+            fresh = nx & ~s.vis;
+            store_fv(jb.fv + v, fresh, s.vis | fresh);
+            if (fresh) {
+                jb.act_next[v >> 16] = 1;
+                unsigned long long m = fresh;
+                while (m) {
+                    const int q = __ffsll((long long)m) - 1;
+                    const int d = jb.level[q] + 1;
+                    if (d >= 255) over |= 1ull << q;   // bfs.cpp level limit (u8 depth_t)
+                    else jb.depth[v * kSlots + q] = (uint8_t)d;
+                    m &= m - 1;
                 }
+            }
+        }
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    fresh |= __shfl_xor_sync(kFull, fresh, o);
-                    over |= __shfl_xor_sync(kFull, over, o);
-                }
-                if (lane == 0) {
-                    if (fresh) atomicOr(jb.cnt + 0, fresh);
-                    if (over) atomicOr(jb.cnt + 1, over);
-                }
-                break;
-            }
-            case kJobWcc: {
-                const uint32_t r = find_root(jb.parent, (uint32_t)v);
-                if (r != v) jb.parent[v] = r;
-                break;
-            }
-            case kJobKcore: {
-                const int16_t m = (int16_t)jb.deg[v];      // kcore.cpp:189
-                const bool gone = m < jb.k && m > 0;
-                if (gone) jb.deg[v] = 0;
-                const uint32_t bits = __ballot_sync(kFull, gone);
-                if (lane == 0) {
-                    jb.removed[w] = bits;
-                    if (bits) {
-                        jb.act_next[w >> 11] = 1;
-                        atomicAdd(jb.cnt, (unsigned long long)__popc(bits));
-                    }
-                }
-                break;
-            }
-            default:
-                break;
+        for (int o = 16; o > 0; o >>= 1) {
+            fresh |= __shfl_xor_sync(kFull, fresh, o);
+            over |= __shfl_xor_sync(kFull, over, o);
+        }
+        if (lane == 0) {
+            if (fresh) atomicOr(jb.cnt + 0, fresh);
+            if (over) atomicOr(jb.cnt + 1, over);
         }
     }
+}
+
+// ------------------------------------------------------- side requests --
+// Kernels of WCC / k-core requests queued in chunks: each returns at once
+// when the request's done flag is set.  Iteration `it` uses counter
+// cnt[it & 1] and clears cnt[(it + 1) & 1] for the next one.
+
+// One sweep of a request's graph; `gate` (k-core: the round's removals)
+// zero means the request is done.
+template <class Op>
+__global__ void __launch_bounds__(kThreads) side_sweep_kernel(const gs_tile_run* __restrict__ runs, uint64_t R,
+                                                              const gs_unit* __restrict__ units,
+                                                              const uint32_t* __restrict__ rec, Op op, int* done,
+                                                              const unsigned long long* gate) {
+    if (__ldcg(done)) return;
+    if (gate && __ldcg(gate) == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *done = 1;
+        return;
+    }
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint64_t i = blockIdx.x; i < R; i += gridDim.x) {
+        const gs_tile_run run = runs[i];
+        for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps) sweep_unit(units[ui], rec, op, lane);
+    }
+}
+
+// WCC after sweep `it`: pointer jumping (wcc.cpp:372-390); done when the
+// sweep hooked nothing.
+__global__ void side_wcc_post(uint32_t* parent, uint64_t N, unsigned long long* cnt, int it, int* done) {
+    if (__ldcg(done)) return;
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = tid; v < N; v += nth) {
+        const uint32_t r = find_root(parent, (uint32_t)v);
+        if (r != v) parent[v] = r;
+    }
+    if (tid == 0) {
+        cnt[(it + 1) & 1] = 0;
+        if (__ldcg(cnt + (it & 1)) == 0) *done = 1;
+    }
+}
+
+// k-core round `it` (kcore.cpp:179-217): remove 0 < (int16)deg < k; their
+// windows go to act_w (cleared by the previous round); act_z is cleared for
+// the next round.
+__global__ void side_kcore_round(int32_t* __restrict__ deg, uint32_t* __restrict__ removed, uint8_t* act_w,
+                                 uint8_t* act_z, uint32_t nw, uint64_t n_words, int k, unsigned long long* cnt,
+                                 int it, int* done) {
+    if (__ldcg(done)) return;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t w = tid; w < nw; w += nth) act_z[w] = 0;
+    if (tid == 0) cnt[(it + 1) & 1] = 0;
+    const uint64_t warp = tid >> 5, nwarps = nth >> 5;
+    uint64_t local = 0;
+    for (uint64_t w = warp; w < n_words; w += nwarps) {
+        const uint64_t v = w * 32 + lane;
+        const int16_t m = (int16_t)deg[v];      // kcore.cpp:189
+        const bool gone = m < k && m > 0;
+        if (gone) deg[v] = 0;
+        const uint32_t bits = __ballot_sync(kFull, gone);
+        if (lane == 0) {
+            removed[w] = bits;
+            if (bits) act_w[w >> 11] = 1;
+            local += __popc(bits);
+        }
+    }
+    if (lane == 0 && local) atomicAdd(cnt + (it & 1), (unsigned long long)local);
 }
 
 // Admission: request q of a BFS group starts at `root` (bfs.cpp:70).
@@ -319,8 +332,12 @@ struct Request {
     float* x = nullptr;
     float* y = nullptr;
     float* r = nullptr;
-    int* err = nullptr;                  // PageRank: bounded-wait flag of its sweeps
-    unsigned long long* cnt = nullptr;
+    int* flags = nullptr;                // side requests: [0] done, [1] bounded-wait error
+    unsigned long long* cnt = nullptr;   // side requests: two iteration counters
+    int side = -1;                       // side slot (WCC, k-core, PageRank)
+    int iter = 0;                        // iterations queued so far
+    bool chunk_pending = false;
+    bool result_pending = false;         // result copy queued, event not yet seen
     std::shared_ptr<HostBuf> result;     // pinned host copy of the result
     uint64_t result_bytes = 0;
 };
@@ -332,8 +349,13 @@ struct gs_server {
     uint64_t budget = 0;
     uint64_t used = 0;
     cudaStream_t stream = nullptr;
-    cudaStream_t pr_stream = nullptr;    // PageRank sweeps, beside the step graph
-    cudaEvent_t ev_step = nullptr, ev_pr = nullptr;
+    // side requests (WCC, k-core, PageRank): kSideSlots slots over
+    // kSideStreams lower-priority streams, an event and a pinned flag pair
+    // per slot
+    cudaStream_t side_stream[kSideStreams] = {};
+    cudaEvent_t side_ev[kSideSlots] = {};
+    int* h_flags = nullptr;              // pinned, kSideSlots x 2
+    std::vector<int> side_free;
     cudaGraphExec_t step_exec = nullptr;
     cudaGraph_t step_graph = nullptr;
     Table* h_table = nullptr;            // pinned
@@ -466,51 +488,58 @@ gs_status admit(gs_server* s, Request& r) {
     const gs_graph* g = sg.g;
     const uint64_t N = g->N;
     r.footprint = footprint(s, r);
-    switch (r.algo) {
-        case GS_ALGO_BFS: {
-            if (!sg.fv) {
-                GS_TRY(open_group(s, sg));
-                s->used += sg.group_bytes;
-                r.footprint = 0;
-            }
-            int q = 0;
-            while (sg.used >> q & 1) ++q;
-            sg.used |= 1ull << q;
-            sg.slot_req[q] = (int64_t)r.id;
-            sg.slot_start[q] = s->step;
-            r.slot = q;
-            serve_seed_bfs<<<1, 1, 0, s->stream>>>(sg.fv, sg.depth, sg.act[sg.cur], (uint64_t)r.arg, q);
-            s->kernel_launches++;
-            break;
+    if (r.algo == GS_ALGO_BFS) {
+        if (!sg.fv) {
+            GS_TRY(open_group(s, sg));
+            s->used += sg.group_bytes;
+            r.footprint = 0;
         }
-        case GS_ALGO_WCC:
-            GS_TRY(pool_dev(s, N * 4, (void**)&r.parent));
-            GS_TRY(pool_dev(s, N, (void**)&r.touched));
-            GS_TRY(pool_dev(s, g->V * 4 + 16, (void**)&r.labels));
-            serve_iota<<<blocks_for(N, ctx), kThreads, 0, s->stream>>>(r.parent, N);
-            s->kernel_launches++;
-            GS_CHECK_CUDA(ctx, cudaMemsetAsync(r.touched, 0, N, s->stream));
-            break;
-        case GS_ALGO_KCORE:
-            GS_TRY(pool_dev(s, N * 4, (void**)&r.deg));
-            GS_TRY(pool_dev(s, N / 8, (void**)&r.removed));
-            GS_TRY(pool_dev(s, g->nw, (void**)&r.act[0]));
-            GS_TRY(pool_dev(s, g->nw, (void**)&r.act[1]));
-            GS_CHECK_CUDA(ctx, cudaMemcpyAsync(r.deg, g->d_degree, N * 4, cudaMemcpyDeviceToDevice, s->stream));
-            GS_CHECK_CUDA(ctx, cudaMemsetAsync(r.act[0], 0, g->nw, s->stream));
-            GS_CHECK_CUDA(ctx, cudaMemsetAsync(r.act[1], 0, g->nw, s->stream));
-            break;
-        default:
-            // PageRank sweeps the graph's row-slice layout (built once)
-            if (!g->pr.built) GS_TRY(pr_layout_build(sg.g));
-            GS_TRY(pool_dev(s, N * 4, (void**)&r.x));
-            GS_TRY(pool_dev(s, N * 4, (void**)&r.y));
-            GS_TRY(pool_dev(s, N * 4, (void**)&r.r));
-            GS_TRY(pool_dev(s, 256, (void**)&r.err));
-            GS_CHECK_CUDA(ctx, cudaMemsetAsync(r.err, 0, 256, s->stream));
-            serve_pr_init<<<blocks_for(N, ctx), kThreads, 0, s->stream>>>(r.x, r.y, N, g->V);
-            s->kernel_launches++;
-            break;
+        int q = 0;
+        while (sg.used >> q & 1) ++q;
+        sg.used |= 1ull << q;
+        sg.slot_req[q] = (int64_t)r.id;
+        sg.slot_start[q] = s->step;
+        r.slot = q;
+        serve_seed_bfs<<<1, 1, 0, s->stream>>>(sg.fv, sg.depth, sg.act[sg.cur], (uint64_t)r.arg, q);
+        s->kernel_launches++;
+    } else {
+        r.side = s->side_free.back();
+        s->side_free.pop_back();
+        cudaStream_t st = s->side_stream[r.side % kSideStreams];
+        GS_TRY(pool_dev(s, 256, (void**)&r.flags));
+        GS_TRY(pool_dev(s, 2 * sizeof(unsigned long long), (void**)&r.cnt));
+        GS_CHECK_CUDA(ctx, cudaMemsetAsync(r.flags, 0, 256, st));
+        GS_CHECK_CUDA(ctx, cudaMemsetAsync(r.cnt, 0, 2 * sizeof(unsigned long long), st));
+        switch (r.algo) {
+            case GS_ALGO_WCC:
+                GS_TRY(pool_dev(s, N * 4, (void**)&r.parent));
+                GS_TRY(pool_dev(s, N, (void**)&r.touched));
+                GS_TRY(pool_dev(s, g->V * 4 + 16, (void**)&r.labels));
+                serve_iota<<<blocks_for(N, ctx), kThreads, 0, st>>>(r.parent, N);
+                s->kernel_launches++;
+                GS_CHECK_CUDA(ctx, cudaMemsetAsync(r.touched, 0, N, st));
+                break;
+            case GS_ALGO_KCORE:
+                GS_TRY(pool_dev(s, N * 4, (void**)&r.deg));
+                GS_TRY(pool_dev(s, N / 8, (void**)&r.removed));
+                GS_TRY(pool_dev(s, g->nw, (void**)&r.act[0]));
+                GS_TRY(pool_dev(s, g->nw, (void**)&r.act[1]));
+                GS_CHECK_CUDA(ctx, cudaMemcpyAsync(r.deg, g->d_degree, N * 4, cudaMemcpyDeviceToDevice, st));
+                GS_CHECK_CUDA(ctx, cudaMemsetAsync(r.act[0], 0, g->nw, st));
+                GS_CHECK_CUDA(ctx, cudaMemsetAsync(r.act[1], 0, g->nw, st));
+                break;
+            default:
+                // PageRank sweeps the graph's row-slice layout (built once)
+                if (!g->pr.built) GS_TRY(pr_layout_build(sg.g));
+                GS_TRY(pool_dev(s, N * 4, (void**)&r.x));
+                GS_TRY(pool_dev(s, N * 4, (void**)&r.y));
+                GS_TRY(pool_dev(s, N * 4, (void**)&r.r));
+                serve_pr_init<<<blocks_for(N, ctx), kThreads, 0, st>>>(r.x, r.y, N, g->V);
+                s->kernel_launches++;
+                break;
+        }
+        r.iter = 0;
+        r.chunk_pending = false;
     }
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     s->used += r.footprint;
@@ -546,9 +575,16 @@ void release(gs_server* s, Request& r) {
             pool_dev_put(s, r.x, N * 4);
             pool_dev_put(s, r.y, N * 4);
             pool_dev_put(s, r.r, N * 4);
-            pool_dev_put(s, r.err, 256);
             break;
     }
+    if (r.side >= 0) {
+        pool_dev_put(s, r.flags, 256);
+        pool_dev_put(s, r.cnt, 2 * sizeof(unsigned long long));
+        s->side_free.push_back(r.side);
+        r.side = -1;
+    }
+    r.flags = nullptr;
+    r.cnt = nullptr;
     r.parent = nullptr;
     r.touched = nullptr;
     r.labels = nullptr;
@@ -556,7 +592,6 @@ void release(gs_server* s, Request& r) {
     r.removed = nullptr;
     r.act[0] = r.act[1] = nullptr;
     r.x = r.y = r.r = nullptr;
-    r.err = nullptr;
     s->used -= r.footprint;
     r.footprint = 0;
 }
@@ -567,28 +602,28 @@ void fill_graph_tables(Job& j, const gs_graph* g) {
     j.rec = g->d_rec;
     j.R = g->d_runs_blk ? g->R_blk : g->R;
     j.words = g->N / 32;
-    j.N = g->N;
-    j.V = g->V;
     j.nw = g->nw;
     j.directed = g->directed;
 }
 
-// Enqueues the copy of a finished request's result to pinned host memory.
+// Enqueues the copy of a finished request's result to pinned host memory
+// on the request's stream.
 gs_status take_result(gs_server* s, Request& r) {
     gs_ctx* ctx = s->ctx;
     SrvGraph& sg = s->graphs[r.graph];
     const gs_graph* g = sg.g;
     const void* src = nullptr;
+    cudaStream_t stream = r.side >= 0 ? s->side_stream[r.side % kSideStreams] : s->stream;
     switch (r.algo) {
         case GS_ALGO_BFS:
-            serve_take_bfs<<<blocks_for(g->N, ctx), kThreads, 0, s->stream>>>(sg.fv, sg.depth, r.slot, sg.out, g->V,
+            serve_take_bfs<<<blocks_for(g->N, ctx), kThreads, 0, stream>>>(sg.fv, sg.depth, r.slot, sg.out, g->V,
                                                                                 g->N);
             s->kernel_launches++;
             src = sg.out;
             r.result_bytes = g->V;
             break;
         case GS_ALGO_WCC:
-            serve_wcc_labels<<<blocks_for(g->V, ctx), kThreads, 0, s->stream>>>(r.parent, r.touched, r.labels,
+            serve_wcc_labels<<<blocks_for(g->V, ctx), kThreads, 0, stream>>>(r.parent, r.touched, r.labels,
                                                                                  g->V);
             s->kernel_launches++;
             src = r.labels;
@@ -607,7 +642,7 @@ gs_status take_result(gs_server* s, Request& r) {
     gs_status st = GS_OK;
     r.result = host_buf(s, r.result_bytes, &st);
     if (st != GS_OK) return st;
-    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(r.result->p, src, r.result_bytes, cudaMemcpyDeviceToHost, s->stream));
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(r.result->p, src, r.result_bytes, cudaMemcpyDeviceToHost, stream));
     return GS_OK;
 }
 
@@ -630,6 +665,50 @@ bool same_query(const Request& a, const Request& b) {
     return a.graph == b.graph && a.algo == b.algo && (a.algo == GS_ALGO_WCC || a.arg == b.arg);
 }
 
+// Queues the next chunk of a side request's iterations on its stream, then
+// the copy of its flags and the chunk's event.
+gs_status queue_chunk(gs_server* s, Request& r) {
+    gs_ctx* ctx = s->ctx;
+    gs_graph* g = s->graphs[r.graph].g;
+    cudaStream_t st = s->side_stream[r.side % kSideStreams];
+    const gs_tile_run* runs = g->d_runs_blk ? g->d_runs_blk : g->d_runs;
+    const gs_unit* units = g->d_runs_blk ? g->d_units_blk : g->d_units;
+    const uint64_t R = g->d_runs_blk ? g->R_blk : g->R;
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(R, gs_grid_size(ctx, 8)));
+    switch (r.algo) {
+        case GS_ALGO_WCC:
+            for (int k = 0; k < kWccChunk; ++k, ++r.iter) {
+                const WccOp op{r.parent, r.iter == 0 ? r.touched : nullptr, r.cnt + (r.iter & 1)};
+                side_sweep_kernel<<<grid, kThreads, 0, st>>>(runs, R, units, g->d_rec, op, r.flags, nullptr);
+                side_wcc_post<<<blocks_for(g->N, ctx), kThreads, 0, st>>>(r.parent, g->N, r.cnt, r.iter, r.flags);
+                s->kernel_launches += 2;
+            }
+            break;
+        case GS_ALGO_KCORE:
+            for (int k = 0; k < kKcoreChunk; ++k, ++r.iter) {
+                const int p = r.iter & 1;
+                side_kcore_round<<<blocks_for(g->N, ctx), kThreads, 0, st>>>(
+                    r.deg, r.removed, r.act[p], r.act[p ^ 1], g->nw, g->N / 32, (int)r.arg, r.cnt, r.iter, r.flags);
+                const KcoreOp op{r.deg, r.removed, r.act[p]};
+                side_sweep_kernel<<<grid, kThreads, 0, st>>>(runs, R, units, g->d_rec, op, r.flags, r.cnt + p);
+                s->kernel_launches += 2;
+            }
+            break;
+        default:
+            for (; r.iter < r.arg; ++r.iter) {
+                GS_TRY(pr_slice_sweep(g, st, r.x, r.y, r.flags + 1));
+                GS_TRY(pr_finalize_launch(ctx, st, r.x, r.y, r.r, g->d_degree, g->N, g->V, 0));
+                s->kernel_launches += 2;
+            }
+            break;
+    }
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(s->h_flags + 2 * r.side, r.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    GS_CHECK_CUDA(ctx, cudaEventRecord(s->side_ev[r.side], st));
+    r.chunk_pending = true;
+    return GS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -646,9 +725,12 @@ gs_status gs_serve_create(gs_ctx* ctx, uint64_t state_budget_bytes, gs_server** 
     cudaDeviceGetStreamPriorityRange(&lo, &hi);
     gs_status st = GS_OK;
     cudaError_t e = cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, hi);
-    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->pr_stream, cudaStreamNonBlocking, lo);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_step, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_pr, cudaEventDisableTiming);
+    for (int k = 0; k < kSideStreams && e == cudaSuccess; ++k)
+        e = cudaStreamCreateWithPriority(&s->side_stream[k], cudaStreamNonBlocking, lo);
+    for (int k = 0; k < kSideSlots && e == cudaSuccess; ++k)
+        e = cudaEventCreateWithFlags(&s->side_ev[k], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaHostAlloc((void**)&s->h_flags, 2 * sizeof(int) * kSideSlots, cudaHostAllocDefault);
+    for (int k = kSideSlots - 1; k >= 0; --k) s->side_free.push_back(k);
     if (e == cudaSuccess) e = cudaHostAlloc((void**)&s->h_table, sizeof(Table), cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc((void**)&s->h_cnt, sizeof(unsigned long long) * kMaxJobs * kCounters,
                                             cudaHostAllocDefault);
@@ -717,172 +799,173 @@ gs_status gs_serve_submit(gs_server* s, int graph_id, gs_algo algo, int64_t arg,
     return GS_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Marks finished requests done (their result copies were queued and have
+// completed), hands results to attached requests and frees their state.
+void retire(gs_server* s, const std::vector<uint64_t>& finished, double t) {
+    for (uint64_t id : finished) {
+        Request& r = s->reqs[id];
+        r.state = r.status == GS_OK ? kDone : kFailed;
+        r.t_done = t;
+        release(s, r);
+        for (uint64_t f : r.followers) {
+            Request& fr = s->reqs[f];
+            fr.state = r.state;
+            fr.status = r.status;
+            fr.t_admit = r.t_admit;
+            fr.t_done = t;
+            fr.steps = r.steps;
+            fr.result = r.result;
+            fr.result_bytes = r.result_bytes;
+        }
+        s->active.erase(std::find(s->active.begin(), s->active.end(), id));
+    }
+}
+
+// One step of the BFS groups (the captured step graph).
+gs_status bfs_step(gs_server* s) {
+    gs_ctx* ctx = s->ctx;
+    Table* t = s->h_table;
+    int nj = 0;
+    uint64_t runs = 0, words = 0;
+    std::vector<int> group_job(s->graphs.size(), -1);
+    for (uint64_t id : s->active) {
+        Request& r = s->reqs[id];
+        if (r.algo != GS_ALGO_BFS) continue;
+        SrvGraph& sg = s->graphs[r.graph];
+        if (group_job[r.graph] >= 0) {
+            r.job = group_job[r.graph];
+            continue;
+        }
+        Job& j = t->jobs[nj];
+        std::memset(&j, 0, sizeof(Job));
+        fill_graph_tables(j, sg.g);
+        j.run_beg = runs;
+        j.word_beg = words;
+        j.cnt = s->d_cnt + (size_t)nj * kCounters;
+        j.fv = sg.fv;
+        j.next = sg.next;
+        j.depth = sg.depth;
+        j.act_cur = sg.act[sg.cur];
+        j.act_next = sg.act[sg.cur ^ 1];
+        for (int q = 0; q < kSlots; ++q)
+            j.level[q] = (sg.used >> q & 1) ? (uint8_t)std::min(255, s->step - sg.slot_start[q] + 1) : 0;
+        group_job[r.graph] = nj;
+        r.job = nj;
+        runs += j.R;
+        words += j.words;
+        ++nj;
+    }
+    if (nj == 0) return GS_OK;
+    t->n_jobs = nj;
+    t->total_runs = runs;
+    t->total_words = words;
+    GS_CHECK_CUDA(ctx, cudaGraphLaunch(s->step_exec, s->stream));
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(s->stream));
+    s->graph_launches++;
+    s->kernel_launches += 2;
+    s->steps_run++;
+    std::vector<uint64_t> finished;
+    for (int g = 0; g < (int)s->graphs.size(); ++g)
+        if (group_job[g] >= 0) s->graphs[g].cur ^= 1;
+    for (uint64_t id : s->active) {
+        Request& r = s->reqs[id];
+        if (r.algo != GS_ALGO_BFS) continue;
+        const unsigned long long* c = s->h_cnt + (size_t)r.job * kCounters;
+        r.steps += 1;
+        bool done;
+        if (c[1] >> r.slot & 1) {
+            r.status = GS_ERR_RANGE;
+            done = true;
+        } else {
+            done = !(c[0] >> r.slot & 1);
+        }
+        if (done) finished.push_back(id);
+    }
+    s->step += 1;
+    if (finished.empty()) return GS_OK;
+    for (uint64_t id : finished) {
+        Request& r = s->reqs[id];
+        if (r.status == GS_OK) {
+            GS_TRY(take_result(s, r));
+        } else {
+            // clear the slot for its next request (result discarded)
+            SrvGraph& sg = s->graphs[r.graph];
+            serve_take_bfs<<<blocks_for(sg.g->N, ctx), kThreads, 0, s->stream>>>(sg.fv, sg.depth, r.slot, sg.out,
+                                                                                 sg.g->V, sg.g->N);
+            s->kernel_launches++;
+        }
+    }
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(s->stream));
+    retire(s, finished, now_s(s));
+    return GS_OK;
+}
+
+// Progress of the side requests: queue a chunk where none is in flight,
+// queue the result copy of a request whose last chunk found it done, retire
+// a request whose result copy has landed.  Nothing here waits on a stream.
+gs_status side_step(gs_server* s) {
+    gs_ctx* ctx = s->ctx;
+    std::vector<uint64_t> finished;
+    for (uint64_t id : s->active) {
+        Request& r = s->reqs[id];
+        if (r.side < 0) continue;
+        if (r.chunk_pending || r.result_pending) {
+            const cudaError_t e = cudaEventQuery(s->side_ev[r.side]);
+            if (e == cudaErrorNotReady) continue;
+            if (e != cudaSuccess) return gs_cuda_fail(ctx, e, "side request");
+        }
+        if (r.result_pending) {
+            r.result_pending = false;
+            finished.push_back(id);
+            continue;
+        }
+        if (r.chunk_pending) {
+            r.chunk_pending = false;
+            const int* f = s->h_flags + 2 * r.side;
+            r.steps = r.iter;
+            const bool done = r.algo == GS_ALGO_PAGERANK ? r.iter >= r.arg : f[0] != 0;
+            if (f[1]) {
+                r.status = GS_ERR_TIMEOUT;
+                finished.push_back(id);
+                continue;
+            }
+            if (done) {
+                GS_TRY(take_result(s, r));
+                GS_CHECK_CUDA(ctx, cudaEventRecord(s->side_ev[r.side], s->side_stream[r.side % kSideStreams]));
+                r.result_pending = true;
+                continue;
+            }
+        }
+        GS_TRY(queue_chunk(s, r));
+    }
+    if (!finished.empty()) retire(s, finished, now_s(s));
+    return GS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 gs_status gs_serve_step(gs_server* s, int* n_active, int* n_queued) {
     if (!s) return GS_ERR_ARG;
-    gs_ctx* ctx = s->ctx;
     // admission: FIFO while the state fits the budget and a slot is free
     while (!s->queue.empty() && (int)s->active.size() < kMaxJobs) {
         Request& r = s->reqs[s->queue.front()];
         const SrvGraph& sg = s->graphs[r.graph];
         if (r.algo == GS_ALGO_BFS && sg.fv && sg.used == ~0ull) break;
+        if (r.algo != GS_ALGO_BFS && s->side_free.empty()) break;
         const size_t need = footprint(s, r);
         if (s->used + need > s->budget && !s->active.empty()) break;
         GS_TRY(admit(s, r));
         s->active.push_back(r.id);
         s->queue.pop_front();
     }
-    if (!s->active.empty()) {
-        // one job per BFS group, one per other request
-        Table* t = s->h_table;
-        int nj = 0;
-        uint64_t runs = 0, words = 0;
-        std::vector<int> group_job(s->graphs.size(), -1);
-        // PageRank requests: one row-slice sweep and one update each, on the
-        // side stream, overlapping the step graph
-        bool any_pr = false;
-        for (uint64_t id : s->active) {
-            Request& r = s->reqs[id];
-            if (r.algo != GS_ALGO_PAGERANK) continue;
-            if (!any_pr) {   // after this step's admissions (their init kernels)
-                GS_CHECK_CUDA(ctx, cudaEventRecord(s->ev_step, s->stream));
-                GS_CHECK_CUDA(ctx, cudaStreamWaitEvent(s->pr_stream, s->ev_step, 0));
-            }
-            any_pr = true;
-            gs_graph* g = s->graphs[r.graph].g;
-            GS_TRY(pr_slice_sweep(g, s->pr_stream, r.x, r.y, r.err));
-            GS_TRY(pr_finalize_launch(ctx, s->pr_stream, r.x, r.y, r.r, g->d_degree, g->N, g->V, 0));
-            s->kernel_launches += 2;
-            r.job = -1;
-        }
-        if (any_pr) GS_CHECK_CUDA(ctx, cudaEventRecord(s->ev_pr, s->pr_stream));
-        for (uint64_t id : s->active) {
-            Request& r = s->reqs[id];
-            SrvGraph& sg = s->graphs[r.graph];
-            if (r.algo == GS_ALGO_PAGERANK) continue;
-            if (r.algo == GS_ALGO_BFS && group_job[r.graph] >= 0) {
-                r.job = group_job[r.graph];
-                continue;
-            }
-            Job& j = t->jobs[nj];
-            std::memset(&j, 0, sizeof(Job));
-            fill_graph_tables(j, sg.g);
-            j.run_beg = runs;
-            j.word_beg = words;
-            j.cnt = s->d_cnt + (size_t)nj * kCounters;
-            switch (r.algo) {
-                case GS_ALGO_BFS:
-                    j.kind = kJobBfs;
-                    j.fv = sg.fv;
-                    j.next = sg.next;
-                    j.depth = sg.depth;
-                    j.act_cur = sg.act[sg.cur];
-                    j.act_next = sg.act[sg.cur ^ 1];
-                    for (int q = 0; q < kSlots; ++q)
-                        j.level[q] = (sg.used >> q & 1) ? (uint8_t)std::min(255, s->step - sg.slot_start[q] + 1) : 0;
-                    group_job[r.graph] = nj;
-                    break;
-                case GS_ALGO_WCC:
-                    j.kind = kJobWcc;
-                    j.flags = r.steps == 0 ? kFlagFirst : 0;
-                    j.parent = r.parent;
-                    j.touched = r.touched;
-                    break;
-                case GS_ALGO_KCORE:
-                    j.kind = kJobKcore;
-                    j.flags = r.steps == 0 ? kFlagFirst : 0;
-                    j.k = (int)r.arg;
-                    j.deg = r.deg;
-                    j.removed = r.removed;
-                    j.act_cur = r.act[r.cur];
-                    j.act_next = r.act[r.cur ^ 1];
-                    break;
-                default:
-                    break;
-            }
-            r.job = nj;
-            runs += j.R;
-            words += j.words;
-            ++nj;
-        }
-        t->n_jobs = nj;
-        t->total_runs = runs;
-        t->total_words = words;
-        GS_CHECK_CUDA(ctx, cudaGraphLaunch(s->step_exec, s->stream));
-        if (any_pr) GS_CHECK_CUDA(ctx, cudaStreamWaitEvent(s->stream, s->ev_pr, 0));
-        GS_CHECK_CUDA(ctx, cudaStreamSynchronize(s->stream));
-        s->graph_launches++;
-        s->kernel_launches += 2;
-        s->steps_run++;
-        // outcomes
-        std::vector<uint64_t> finished;
-        std::vector<bool> group_swapped(s->graphs.size(), false);
-        for (uint64_t id : s->active) {
-            Request& r = s->reqs[id];
-            SrvGraph& sg = s->graphs[r.graph];
-            const unsigned long long* c = s->h_cnt + (size_t)std::max(r.job, 0) * kCounters;
-            r.steps += 1;
-            bool done = false;
-            switch (r.algo) {
-                case GS_ALGO_BFS:
-                    if (c[1] >> r.slot & 1) {
-                        r.status = GS_ERR_RANGE;
-                        done = true;
-                    } else {
-                        done = !(c[0] >> r.slot & 1);
-                    }
-                    if (!group_swapped[r.graph]) {
-                        sg.cur ^= 1;
-                        group_swapped[r.graph] = true;
-                    }
-                    break;
-                case GS_ALGO_WCC: done = c[0] == 0; break;
-                case GS_ALGO_KCORE:
-                    done = c[0] == 0;
-                    r.cur ^= 1;
-                    break;
-                default: done = r.steps >= r.arg; break;
-            }
-            if (done) finished.push_back(id);
-        }
-        s->step += 1;
-        if (!finished.empty()) {
-            for (uint64_t id : finished) {
-                Request& r = s->reqs[id];
-                if (r.algo == GS_ALGO_PAGERANK) {
-                    int h_err = 0;
-                    GS_CHECK_CUDA(ctx, cudaMemcpy(&h_err, r.err, sizeof(int), cudaMemcpyDeviceToHost));
-                    if (h_err) r.status = GS_ERR_TIMEOUT;
-                }
-                if (r.status == GS_OK) GS_TRY(take_result(s, r));
-                else if (r.algo == GS_ALGO_BFS) {
-                    // clear the slot for its next request (result discarded)
-                    SrvGraph& sg = s->graphs[r.graph];
-                    serve_take_bfs<<<blocks_for(sg.g->N, ctx), kThreads, 0, s->stream>>>(sg.fv, sg.depth, r.slot, sg.out,
-                                                                                         sg.g->V, sg.g->N);
-                    s->kernel_launches++;
-                }
-            }
-            GS_CHECK_CUDA(ctx, cudaStreamSynchronize(s->stream));
-            const double t = now_s(s);
-            for (uint64_t id : finished) {
-                Request& r = s->reqs[id];
-                r.state = r.status == GS_OK ? kDone : kFailed;
-                r.t_done = t;
-                release(s, r);
-                for (uint64_t f : r.followers) {
-                    Request& fr = s->reqs[f];
-                    fr.state = r.state;
-                    fr.status = r.status;
-                    fr.t_admit = r.t_admit;
-                    fr.t_done = t;
-                    fr.steps = r.steps;
-                    fr.result = r.result;
-                    fr.result_bytes = r.result_bytes;
-                }
-                s->active.erase(std::find(s->active.begin(), s->active.end(), id));
-            }
-        }
-    }
+    GS_TRY(side_step(s));   // queue side chunks first: they run beside the step
+    GS_TRY(bfs_step(s));
     if (n_active) *n_active = (int)s->active.size();
     if (n_queued) *n_queued = (int)s->queue.size();
     return GS_OK;
@@ -939,7 +1022,8 @@ gs_status gs_serve_stats(const gs_server* s, uint64_t* steps, uint64_t* graph_la
 gs_status gs_serve_free(gs_server* s) {
     if (!s) return GS_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
-    if (s->pr_stream) cudaStreamSynchronize(s->pr_stream);
+    for (int k = 0; k < kSideStreams; ++k)
+        if (s->side_stream[k]) cudaStreamSynchronize(s->side_stream[k]);
     s->reqs.clear();   // drops result buffers into the host pool
     if (s->step_exec) cudaGraphExecDestroy(s->step_exec);
     if (s->step_graph) cudaGraphDestroy(s->step_graph);
@@ -950,9 +1034,11 @@ gs_status gs_serve_free(gs_server* s) {
     if (s->h_table) cudaFreeHost(s->h_table);
     if (s->h_cnt) cudaFreeHost(s->h_cnt);
     if (s->stream) cudaStreamDestroy(s->stream);
-    if (s->pr_stream) cudaStreamDestroy(s->pr_stream);
-    if (s->ev_step) cudaEventDestroy(s->ev_step);
-    if (s->ev_pr) cudaEventDestroy(s->ev_pr);
+    for (int k = 0; k < kSideStreams; ++k)
+        if (s->side_stream[k]) cudaStreamDestroy(s->side_stream[k]);
+    for (int k = 0; k < kSideSlots; ++k)
+        if (s->side_ev[k]) cudaEventDestroy(s->side_ev[k]);
+    if (s->h_flags) cudaFreeHost(s->h_flags);
     delete s;
     return GS_OK;
 }
