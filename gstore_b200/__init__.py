@@ -47,7 +47,8 @@ ABI_SYMBOLS = [
     "gs_batch_create", "gs_batch_add", "gs_batch_run", "gs_batch_download", "gs_batch_result_count",
     "gs_batch_bfs_levels", "gs_batch_stats", "gs_batch_free",
     "gs_serve_create", "gs_serve_add_graph", "gs_serve_submit", "gs_serve_step", "gs_serve_poll",
-    "gs_serve_result", "gs_serve_clock", "gs_serve_stats", "gs_serve_free",
+    "gs_serve_result", "gs_serve_clock", "gs_serve_stats", "gs_serve_free", "gs_serve_completed",
+    "gs_serve_set_side_streams",
 ]
 
 
@@ -119,6 +120,8 @@ def lib():
             "gs_serve_clock": [vp, C.POINTER(C.c_double)],
             "gs_serve_stats": [vp, pu64, pu64, pu64, pu64],
             "gs_serve_free": [vp],
+            "gs_serve_completed": [vp, pu64, i32, C.POINTER(C.c_int)],
+            "gs_serve_set_side_streams": [vp, i32],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -375,6 +378,20 @@ class Server:
         na, nq = C.c_int(), C.c_int()
         self.ctx._check(lib().gs_serve_step(self._h, C.byref(na), C.byref(nq)))
         return na.value, nq.value
+
+    def completed(self, max_ids: int = 4096):
+        """Ids of requests finished since the last call, oldest first."""
+        buf = (C.c_uint64 * max_ids)()
+        n = C.c_int()
+        out = []
+        while True:
+            self.ctx._check(lib().gs_serve_completed(self._h, buf, max_ids, C.byref(n)))
+            out.extend(buf[: n.value])
+            if n.value < max_ids:
+                return out
+
+    def set_side_streams(self, n: int) -> None:
+        self.ctx._check(lib().gs_serve_set_side_streams(self._h, n))
 
     def poll(self, rid: int) -> int:
         st = C.c_int()

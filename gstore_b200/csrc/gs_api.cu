@@ -198,6 +198,7 @@ static void free_graph_arrays(gs_graph* g) {
     gs_dev_free(g->d_tile_rc);
     gs_dev_free(g->d_degree);
     gs_dev_free(g->d_runs);
+    gs_dev_free(g->d_runs_lpt);
     gs_dev_free(g->d_units);
     gs_dev_free(g->d_runs_blk);
     gs_dev_free(g->d_units_blk);
@@ -206,6 +207,7 @@ static void free_graph_arrays(gs_graph* g) {
     g->d_runs_blk2 = nullptr;
     g->d_units_blk2 = nullptr;
     g->d_runs = nullptr;
+    g->d_runs_lpt = nullptr;
     g->d_units = nullptr;
     g->d_runs_blk = nullptr;
     g->d_units_blk = nullptr;
@@ -364,6 +366,18 @@ static gs_status build_tables(gs_graph* g) {
     if (!runs.empty())
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_runs, runs.data(), runs.size() * sizeof(gs_tile_run),
                                            cudaMemcpyHostToDevice, ctx->stream));
+    // the BFS sweep's order: longest runs first, so that the runs drawn last
+    // (from the sweep's ticket) are the short ones
+    std::vector<gs_tile_run> lpt;
+    if (!g->stream && !runs.empty()) {
+        lpt = runs;
+        std::stable_sort(lpt.begin(), lpt.end(), [](const gs_tile_run& x, const gs_tile_run& y) {
+            return x.rec_end - x.rec_beg > y.rec_end - y.rec_beg;
+        });
+        GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_runs_lpt, lpt.size() * sizeof(gs_tile_run)));
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_runs_lpt, lpt.data(), lpt.size() * sizeof(gs_tile_run),
+                                           cudaMemcpyHostToDevice, ctx->stream));
+    }
     GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_tile_off, tile_off.size() * sizeof(uint64_t)));
     GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_tile_rc, std::max<size_t>(1, tile_rc.size()) * sizeof(uint32_t)));
     GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_tile_off, tile_off.data(), tile_off.size() * sizeof(uint64_t),
@@ -678,6 +692,7 @@ gs_status gs_state_free(gs_state* s) {
     gs_dev_free(s->d_kactive);
     gs_dev_free(s->d_lab);
     gs_dev_free(s->d_error);
+    gs_dev_free(s->d_ticket);
     gs_dev_free(s->d_fv);
     gs_dev_free(s->d_uflags);
     gs_dev_free(s->d_sel);

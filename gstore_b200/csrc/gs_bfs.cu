@@ -7,7 +7,9 @@
 //   depth[v]    u8, written by the finalize for new vertices
 //
 // A CTA sweeps one run at a time (consecutive tiles of one tile row inside
-// a group, <= kRunRecords records).  The row window's state (16 KB) is
+// a group, <= kRunRecords records), taking the next run from an atomic
+// ticket so that CTAs that drew short runs take more of them (run sizes
+// range from a few records to kRunRecords).  The row window's state (16 KB) is
 // brought into shared memory once per run with one cp.async.bulk copy; the
 // run's units (tile slices of <= kUnitRecords records) are spread over the
 // warps, each warp streaming its unit's records with 128-bit evict-first
@@ -39,6 +41,7 @@ struct __align__(128) BfsSmem {
     uint32_t nx[kNxWords];
     uint32_t dirty[kNxWords / 32];
     unsigned long long bar;
+    unsigned long long cur;   // the run drawn by thread 0
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -72,6 +75,9 @@ struct RunArgs {
     int directed;
     int* error;
     const gs_seg_run* seg;   // segment sweep: entries to sweep (records at rec + delta), else null
+    // [0] next run, [1] CTAs finished; zero at launch, the last CTA to
+    // finish zeroes them again for the next launch on the stream
+    unsigned int* ticket;
 };
 
 __global__ void __launch_bounds__(kThreads) bfs_run_kernel(RunArgs a) {
@@ -86,8 +92,14 @@ __global__ void __launch_bounds__(kThreads) bfs_run_kernel(RunArgs a) {
     if (tid < kNxWords / 32) m.dirty[tid] = 0;
     __syncthreads();
     uint32_t parity = 0;
+    auto draw = [&]() -> uint64_t {
+        // every thread has read the previous draw: a barrier lies between
+        if (tid == 0) m.cur = atomicAdd(a.ticket, 1u);
+        __syncthreads();
+        return m.cur;
+    };
 
-    for (uint64_t i = blockIdx.x; i < a.n_runs; i += gridDim.x) {
+    for (uint64_t i = draw(); i < a.n_runs; i = draw()) {
         uint32_t ub, ue;
         const uint32_t* rec = a.rec;
         if (a.seg) {
@@ -123,7 +135,7 @@ __global__ void __launch_bounds__(kThreads) bfs_run_kernel(RunArgs a) {
         parity ^= 1;
         if (!__syncthreads_and(got)) {
             if (tid == 0) atomicExch(a.error, 1);
-            return;   // uniform; nothing else in flight
+            break;   // uniform; nothing else in flight
         }
         const uint32_t mr = ar ? 1u : 0u;
         for (uint32_t ui = ub + warp; ui < ue; ui += kWarps) {
@@ -199,6 +211,11 @@ __global__ void __launch_bounds__(kThreads) bfs_run_kernel(RunArgs a) {
         }
         if (__syncthreads_or(any_row) && tid == 0) a.act_next[row] = 1;        // read_part_next->set_bit_atomic(i)
     }
+    if (tid == 0 && atomicAdd(a.ticket + 1, 1u) == gridDim.x - 1) {
+        // every CTA has drawn its last ticket
+        atomicExch(a.ticket, 0u);
+        atomicExch(a.ticket + 1, 0u);
+    }
 }
 
 // Bits 1,3,5,... of x gathered into bits 0..15.
@@ -273,6 +290,8 @@ gs_status bfs_init(gs_state* s) {
     if (!s->d_act) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_act, g->nw));
     if (!s->d_act_next) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_act_next, g->nw));
     if (!s->d_error) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_error, sizeof(uint64_t)));
+    if (!s->d_ticket) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_ticket, 2 * sizeof(uint32_t)));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_ticket, 0, 2 * sizeof(uint32_t), ctx->stream));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_depth, 0, g->N, ctx->stream));   // INFTY = 0
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_front, 0, words * 8, ctx->stream));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_visited, 0, words * 4, ctx->stream));
@@ -310,8 +329,9 @@ gs_status bfs_sweep_launch(gs_state* s) {
     // every run of the resident graph, or the entries of the current segment
     const uint64_t n_runs = g->seg.list ? g->seg.n : g->R;
     if (n_runs == 0) return GS_OK;
-    RunArgs a{g->d_runs, n_runs, g->d_units, g->seg.list ? g->seg.buf : g->d_rec, s->d_front, s->d_visited,
-              s->d_act, s->d_act_next, g->directed, (int*)s->d_error, g->seg.list};
+    RunArgs a{g->d_runs_lpt ? g->d_runs_lpt : g->d_runs, n_runs, g->d_units, g->seg.list ? g->seg.buf : g->d_rec,
+              s->d_front, s->d_visited,
+              s->d_act, s->d_act_next, g->directed, (int*)s->d_error, g->seg.list, s->d_ticket};
     const uint32_t grid = (uint32_t)std::min<uint64_t>(n_runs, gs_grid_size(ctx, 6));
     gs_timer_begin(ctx);
     bfs_run_kernel<<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
@@ -364,7 +384,7 @@ gs_status bfs_seed_into(gs_ctx* ctx, uint8_t* depth, uint32_t* st, uint8_t* act,
 
 gs_status bfs_level_into(gs_ctx* ctx, const gs_graph* g, uint8_t* depth, uint32_t* st, uint32_t* next,
                          uint8_t* act, uint8_t* act_next, unsigned long long* count, int* error,
-                         uint8_t next_level) {
+                         unsigned int* ticket, uint8_t next_level) {
     if (g->R) {
         static bool attr_set[64] = {false};
         if (!attr_set[ctx->device & 63]) {
@@ -372,7 +392,8 @@ gs_status bfs_level_into(gs_ctx* ctx, const gs_graph* g, uint8_t* depth, uint32_
                                                     (int)sizeof(BfsSmem)));
             attr_set[ctx->device & 63] = true;
         }
-        RunArgs a{g->d_runs, g->R, g->d_units, g->d_rec, st, next, act, act_next, g->directed, error, nullptr};
+        RunArgs a{g->d_runs_lpt ? g->d_runs_lpt : g->d_runs, g->R, g->d_units, g->d_rec, st, next, act, act_next,
+                  g->directed, error, nullptr, ticket};
         const uint32_t grid = (uint32_t)std::min<uint64_t>(g->R, gs_grid_size(ctx, 6));
         bfs_run_kernel<<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
         GS_CHECK_CUDA(ctx, cudaGetLastError());

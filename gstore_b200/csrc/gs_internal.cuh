@@ -143,6 +143,7 @@ struct gs_graph {
     gs_item* d_items = nullptr;
     gs_tile_run* d_runs = nullptr;
     gs_unit* d_units = nullptr;
+    gs_tile_run* d_runs_lpt = nullptr; // the R runs, longest first (resident graphs; BFS sweep order)
     uint64_t R_blk = 0;               // runs of the L2-blocked order (resident graphs)
     gs_tile_run* d_runs_blk = nullptr;
     gs_unit* d_units_blk = nullptr;
@@ -178,6 +179,7 @@ struct gs_state {
     uint32_t* d_front = nullptr;     // N/32 frontier words
     uint32_t* d_visited = nullptr;   // N/32 words: discovered-this-sweep bitmap
     uint64_t* d_error = nullptr;     // bounded-wait failure flag
+    uint32_t* d_ticket = nullptr;    // BFS sweep: run ticket, finished CTAs
     uint2* d_fv = nullptr;           // N/32 {frontier, visited} word pairs
     uint8_t* d_uflags = nullptr;     // 2 x U: per-unit activity flags, selection flags
     uint32_t* d_sel = nullptr;       // U + 1: selected unit indices, then their count
@@ -255,7 +257,8 @@ gs_status pr_init(gs_state* s);
 gs_status pr_layout_build(gs_graph* g);
 void pr_layout_free(gs_graph* g);
 gs_status pr_slice_launch(gs_state* s);
-gs_status pr_slice_sweep(gs_graph* g, cudaStream_t stream, const float* x, float* y, int* error);
+gs_status pr_slice_sweep(gs_graph* g, cudaStream_t stream, const float* x, float* y, int* error,
+                         bool item_ctas = false);
 gs_status pr_finalize_launch(gs_ctx* ctx, cudaStream_t stream, float* x, float* y, float* r, const int32_t* deg,
                              uint64_t N, uint64_t V, int compat);
 gs_status pr_sweep_launch(gs_state* s);
@@ -325,7 +328,7 @@ gs_status gs_graph_adopt(gs_ctx* ctx, uint64_t V, const uint64_t* d_start, uint6
 gs_status bfs_seed_into(gs_ctx* ctx, uint8_t* depth, uint32_t* st, uint8_t* act, uint64_t root);
 gs_status bfs_level_into(gs_ctx* ctx, const gs_graph* g, uint8_t* depth, uint32_t* st, uint32_t* next,
                          uint8_t* act, uint8_t* act_next, unsigned long long* count, int* error,
-                         uint8_t next_level);
+                         unsigned int* ticket, uint8_t next_level);
 
 // Timing helpers around the main sweep kernel of an algorithm.
 void gs_timer_begin(gs_ctx* ctx);

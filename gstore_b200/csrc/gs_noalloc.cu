@@ -40,7 +40,8 @@ constexpr size_t kActOff = kNextOff + kNoAllocMaxVertices / 8;           // wind
 constexpr size_t kActNextOff = kActOff + kNoAllocWindows;
 constexpr size_t kCountOff = kActNextOff + kNoAllocWindows;              // level count (u64)
 constexpr size_t kErrorOff = kCountOff + 8;                              // error flag (int)
-constexpr size_t kScratchBytes = kErrorOff + 8;
+constexpr size_t kTicketOff = kErrorOff + 8;                             // sweep run ticket (2 x u32)
+constexpr size_t kScratchBytes = kTicketOff + 8;
 
 static __device__ __align__(256) unsigned char g_bfs_scratch[kScratchBytes];
 
@@ -77,18 +78,20 @@ extern "C" gs_status gs_bfs_noalloc(gs_graph* g, uint64_t root, uint8_t* d_depth
     uint8_t* act_next = base + kActNextOff;
     unsigned long long* count = reinterpret_cast<unsigned long long*>(base + kCountOff);
     int* error = reinterpret_cast<int*>(base + kErrorOff);
+    unsigned int* ticket = reinterpret_cast<unsigned int*>(base + kTicketOff);
 
     // the array keeps the previous call's contents: clear what this call reads
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(st, 0, g->N / 4, ctx->stream));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(next, 0, g->N / 8, ctx->stream));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(act, 0, 2 * kNoAllocWindows + 16, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(ticket, 0, 8, ctx->stream));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(d_depth, 0, g->V, ctx->stream));   // INFTY = 0
     GS_TRY(bfs_seed_into(ctx, d_depth, st, act, root));
     uint8_t level = 1;
     int64_t sweeps = 0;
     while (true) {
         GS_CHECK_CUDA(ctx, cudaMemsetAsync(count, 0, 8, ctx->stream));
-        GS_TRY(bfs_level_into(ctx, g, d_depth, st, next, act, act_next, count, error, (uint8_t)(level + 1)));
+        GS_TRY(bfs_level_into(ctx, g, d_depth, st, next, act, act_next, count, error, ticket, (uint8_t)(level + 1)));
         ++sweeps;
         // swap(read_part, read_part_next); read_part_next->reset()
         std::swap(act, act_next);

@@ -275,7 +275,7 @@ gs_status pr_layout_build(gs_graph* g) {
     return GS_OK;
 }
 
-gs_status pr_slice_sweep(gs_graph* g, cudaStream_t stream, const float* x, float* y, int* error) {
+gs_status pr_slice_sweep(gs_graph* g, cudaStream_t stream, const float* x, float* y, int* error, bool item_ctas) {
     gs_ctx* ctx = g->ctx;
     const gs_pr_layout& L = g->pr;
     if (L.n_items == 0) return GS_OK;
@@ -285,7 +285,9 @@ gs_status pr_slice_sweep(gs_graph* g, cudaStream_t stream, const float* x, float
                                                 (int)sizeof(PrSmem)));
         attr_set[ctx->device & 63] = true;
     }
-    const uint32_t grid = (uint32_t)std::min<uint64_t>(L.n_items, gs_grid_size(ctx, 3));
+    // persistent (two CTAs per SM walking the items) or one CTA per item, so
+    // that a higher-priority stream's CTAs find free SMs between items
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(L.n_items, item_ctas ? 0x7FFFFFFFull : gs_grid_size(ctx, 3));
     pr_slice_kernel<<<grid, kPrThreads, sizeof(PrSmem), stream>>>(L.d_items, L.n_items, L.d_units, L.d_rec, x, y,
                                                                   g->directed, error);
     GS_CHECK_CUDA(ctx, cudaGetLastError());

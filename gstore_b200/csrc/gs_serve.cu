@@ -68,7 +68,7 @@ struct Job {
     int directed;
     Fv64* fv;
     unsigned long long* next;
-    uint8_t* depth;               // [N][64]
+    uint8_t* depth;               // [64][N]: one plane per slot
     uint8_t* act_cur;
     uint8_t* act_next;
     unsigned long long* cnt;      // kCounters per job
@@ -115,6 +115,8 @@ __global__ void __launch_bounds__(kThreads) serve_sweep_kernel(const Table* __re
     }
 }
 
+// Depth planes are written per warp and slot: the 32 lanes' vertices are
+// consecutive, so each write of a plane is one 32-byte sector.
 __global__ void __launch_bounds__(kThreads) serve_post_kernel(const Table* __restrict__ t) {
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t gwarp = (uint64_t)blockIdx.x * kWarps + warp;
@@ -124,30 +126,28 @@ __global__ void __launch_bounds__(kThreads) serve_post_kernel(const Table* __res
         const uint64_t v = (x - jb.word_beg) * 32 + lane;
         const unsigned long long nx = jb.next[v];
         const Fv64 s = load_fv(jb.fv + v);
-        unsigned long long fresh = 0, over = 0;
+        unsigned long long fresh = 0;
         if (nx || s.f) {
             if (nx) jb.next[v] = 0;
             fresh = nx & ~s.vis;
             store_fv(jb.fv + v, fresh, s.vis | fresh);
-            if (fresh) {
-                jb.act_next[v >> 16] = 1;
-                unsigned long long m = fresh;
-                while (m) {
-                    const int q = __ffsll((long long)m) - 1;
-                    const int d = jb.level[q] + 1;
-                    if (d >= 255) over |= 1ull << q;   // bfs.cpp level limit (u8 depth_t)
-                    else jb.depth[v * kSlots + q] = (uint8_t)d;
-                    m &= m - 1;
-                }
-            }
         }
+        unsigned long long any = fresh;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            fresh |= __shfl_xor_sync(kFull, fresh, o);
-            over |= __shfl_xor_sync(kFull, over, o);
+        for (int o = 16; o > 0; o >>= 1) any |= __shfl_xor_sync(kFull, any, o);
+        if (!any) continue;
+        const uint64_t N = jb.words * 32;
+        unsigned long long over = 0, m = any;
+        while (m) {
+            const int q = __ffsll((long long)m) - 1;
+            const int d = jb.level[q] + 1;
+            if (d >= 255) over |= 1ull << q;   // bfs.cpp level limit (u8 depth_t)
+            else if (fresh >> q & 1) jb.depth[(uint64_t)q * N + v] = (uint8_t)d;
+            m &= m - 1;
         }
         if (lane == 0) {
-            if (fresh) atomicOr(jb.cnt + 0, fresh);
+            jb.act_next[v >> 16] = 1;
+            atomicOr(jb.cnt + 0, any);
             if (over) atomicOr(jb.cnt + 1, over);
         }
     }
@@ -223,27 +223,22 @@ __global__ void side_kcore_round(int32_t* __restrict__ deg, uint32_t* __restrict
 }
 
 // Admission: request q of a BFS group starts at `root` (bfs.cpp:70).
-__global__ void serve_seed_bfs(Fv64* fv, uint8_t* depth, uint8_t* act_cur, uint64_t root, int q) {
+__global__ void serve_seed_bfs(Fv64* fv, uint8_t* depth, uint64_t N, uint8_t* act_cur, uint64_t root, int q) {
     fv[root].f |= 1ull << q;
     fv[root].vis |= 1ull << q;
-    depth[root * kSlots + q] = 1;
+    depth[(uint64_t)q * N + root] = 1;
     act_cur[root >> 16] = 1;
 }
 
-// Retirement of BFS slot q: its depth column out, column and visited bit
-// cleared for the next request in the slot.
-__global__ void serve_take_bfs(Fv64* fv, uint8_t* depth, int q, uint8_t* out, uint64_t V, uint64_t N) {
+// Retirement of BFS slots: their frontier and visited bits cleared for the
+// next requests in the slots (the depth planes are copied out and zeroed by
+// the host's stream operations).
+__global__ void serve_clear_slots(Fv64* fv, uint64_t N, unsigned long long keep) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
-    const unsigned long long keep = ~(1ull << q);
     for (uint64_t v = tid; v < N; v += nth) {
-        const uint8_t d = depth[v * kSlots + q];
-        if (v < V) out[v] = d;
-        if (d) {
-            depth[v * kSlots + q] = 0;
-            fv[v].vis &= keep;
-            fv[v].f &= keep;
-        }
+        const Fv64 s = load_fv(fv + v);
+        if ((s.f | s.vis) & ~keep) store_fv(fv + v, s.f & keep, s.vis & keep);
     }
 }
 
@@ -303,8 +298,6 @@ struct SrvGraph {
     int slot_start[kSlots];           // step whose sweep sees depth 1
     unsigned long long used = 0;
     size_t group_bytes = 0;
-    uint8_t* out = nullptr;           // BFS result staging (V bytes)
-    uint32_t* out32 = nullptr;        // WCC labels staging (4 V bytes)
 };
 
 struct Request {
@@ -353,6 +346,7 @@ struct gs_server {
     // kSideStreams lower-priority streams, an event and a pinned flag pair
     // per slot
     cudaStream_t side_stream[kSideStreams] = {};
+    int n_side = kSideStreams;           // side streams in use
     cudaEvent_t side_ev[kSideSlots] = {};
     int* h_flags = nullptr;              // pinned, kSideSlots x 2
     std::vector<int> side_free;
@@ -366,6 +360,7 @@ struct gs_server {
     std::unordered_map<uint64_t, Request> reqs;
     std::deque<uint64_t> queue;
     std::vector<uint64_t> active;
+    std::deque<uint64_t> completed;      // finished since the client last asked
     uint64_t next_id = 1;
     int step = 0;
     uint64_t steps_run = 0, graph_launches = 0, kernel_launches = 0;
@@ -376,6 +371,10 @@ struct gs_server {
 };
 
 namespace {
+
+inline cudaStream_t side_stream_of(const gs_server* s, const Request& r) {
+    return s->side_stream[r.side % s->n_side];
+}
 
 double now_s(const gs_server* s) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - s->t0).count();
@@ -427,8 +426,15 @@ inline uint32_t blocks_for(uint64_t n, const gs_ctx* ctx) {
     return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(b, gs_grid_size(ctx, 16)));
 }
 
+// Side kernels: one thread per element (one CTA per run for sweeps), so
+// their CTAs are short and the step's higher-priority CTAs get SMs between
+// them instead of waiting for a grid-stride kernel to drain.
+inline uint32_t short_blocks(uint64_t n) {
+    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((n + kThreads - 1) / kThreads, 0x7FFFFFFFull));
+}
+
 size_t group_bytes(const gs_graph* g) {
-    return g->N * (sizeof(Fv64) + 8 + kSlots) + 2 * (size_t)g->nw + g->V + 256;
+    return g->N * (sizeof(Fv64) + 8 + kSlots) + 2 * (size_t)g->nw + 256;
 }
 
 // HBM bytes a request adds when admitted.
@@ -452,7 +458,6 @@ gs_status open_group(gs_server* s, SrvGraph& sg) {
     GS_TRY(pool_dev(s, N * kSlots, (void**)&sg.depth));
     GS_TRY(pool_dev(s, g->nw, (void**)&sg.act[0]));
     GS_TRY(pool_dev(s, g->nw, (void**)&sg.act[1]));
-    GS_TRY(pool_dev(s, g->V + 16, (void**)&sg.out));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(sg.fv, 0, N * sizeof(Fv64), s->stream));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(sg.next, 0, N * 8, s->stream));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(sg.depth, 0, N * kSlots, s->stream));
@@ -472,12 +477,10 @@ void close_group(gs_server* s, SrvGraph& sg) {
     pool_dev_put(s, sg.depth, g->N * kSlots);
     pool_dev_put(s, sg.act[0], g->nw);
     pool_dev_put(s, sg.act[1], g->nw);
-    pool_dev_put(s, sg.out, g->V + 16);
     sg.fv = nullptr;
     sg.next = nullptr;
     sg.depth = nullptr;
     sg.act[0] = sg.act[1] = nullptr;
-    sg.out = nullptr;
     s->used -= sg.group_bytes;
     sg.group_bytes = 0;
 }
@@ -500,12 +503,12 @@ gs_status admit(gs_server* s, Request& r) {
         sg.slot_req[q] = (int64_t)r.id;
         sg.slot_start[q] = s->step;
         r.slot = q;
-        serve_seed_bfs<<<1, 1, 0, s->stream>>>(sg.fv, sg.depth, sg.act[sg.cur], (uint64_t)r.arg, q);
+        serve_seed_bfs<<<1, 1, 0, s->stream>>>(sg.fv, sg.depth, N, sg.act[sg.cur], (uint64_t)r.arg, q);
         s->kernel_launches++;
     } else {
         r.side = s->side_free.back();
         s->side_free.pop_back();
-        cudaStream_t st = s->side_stream[r.side % kSideStreams];
+        cudaStream_t st = side_stream_of(s, r);
         GS_TRY(pool_dev(s, 256, (void**)&r.flags));
         GS_TRY(pool_dev(s, 2 * sizeof(unsigned long long), (void**)&r.cnt));
         GS_CHECK_CUDA(ctx, cudaMemsetAsync(r.flags, 0, 256, st));
@@ -515,7 +518,7 @@ gs_status admit(gs_server* s, Request& r) {
                 GS_TRY(pool_dev(s, N * 4, (void**)&r.parent));
                 GS_TRY(pool_dev(s, N, (void**)&r.touched));
                 GS_TRY(pool_dev(s, g->V * 4 + 16, (void**)&r.labels));
-                serve_iota<<<blocks_for(N, ctx), kThreads, 0, st>>>(r.parent, N);
+                serve_iota<<<short_blocks(N), kThreads, 0, st>>>(r.parent, N);
                 s->kernel_launches++;
                 GS_CHECK_CUDA(ctx, cudaMemsetAsync(r.touched, 0, N, st));
                 break;
@@ -534,7 +537,7 @@ gs_status admit(gs_server* s, Request& r) {
                 GS_TRY(pool_dev(s, N * 4, (void**)&r.x));
                 GS_TRY(pool_dev(s, N * 4, (void**)&r.y));
                 GS_TRY(pool_dev(s, N * 4, (void**)&r.r));
-                serve_pr_init<<<blocks_for(N, ctx), kThreads, 0, st>>>(r.x, r.y, N, g->V);
+                serve_pr_init<<<short_blocks(N), kThreads, 0, st>>>(r.x, r.y, N, g->V);
                 s->kernel_launches++;
                 break;
         }
@@ -606,24 +609,16 @@ void fill_graph_tables(Job& j, const gs_graph* g) {
     j.directed = g->directed;
 }
 
-// Enqueues the copy of a finished request's result to pinned host memory
-// on the request's stream.
+// Enqueues the copy of a finished side request's result to pinned host
+// memory on the request's stream.
 gs_status take_result(gs_server* s, Request& r) {
     gs_ctx* ctx = s->ctx;
-    SrvGraph& sg = s->graphs[r.graph];
-    const gs_graph* g = sg.g;
+    const gs_graph* g = s->graphs[r.graph].g;
     const void* src = nullptr;
-    cudaStream_t stream = r.side >= 0 ? s->side_stream[r.side % kSideStreams] : s->stream;
+    cudaStream_t stream = side_stream_of(s, r);
     switch (r.algo) {
-        case GS_ALGO_BFS:
-            serve_take_bfs<<<blocks_for(g->N, ctx), kThreads, 0, stream>>>(sg.fv, sg.depth, r.slot, sg.out, g->V,
-                                                                                g->N);
-            s->kernel_launches++;
-            src = sg.out;
-            r.result_bytes = g->V;
-            break;
         case GS_ALGO_WCC:
-            serve_wcc_labels<<<blocks_for(g->V, ctx), kThreads, 0, stream>>>(r.parent, r.touched, r.labels,
+            serve_wcc_labels<<<short_blocks(g->V), kThreads, 0, stream>>>(r.parent, r.touched, r.labels,
                                                                                  g->V);
             s->kernel_launches++;
             src = r.labels;
@@ -670,24 +665,24 @@ bool same_query(const Request& a, const Request& b) {
 gs_status queue_chunk(gs_server* s, Request& r) {
     gs_ctx* ctx = s->ctx;
     gs_graph* g = s->graphs[r.graph].g;
-    cudaStream_t st = s->side_stream[r.side % kSideStreams];
+    cudaStream_t st = side_stream_of(s, r);
     const gs_tile_run* runs = g->d_runs_blk ? g->d_runs_blk : g->d_runs;
     const gs_unit* units = g->d_runs_blk ? g->d_units_blk : g->d_units;
     const uint64_t R = g->d_runs_blk ? g->R_blk : g->R;
-    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(R, gs_grid_size(ctx, 8)));
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(R, 0x7FFFFFFFull));
     switch (r.algo) {
         case GS_ALGO_WCC:
             for (int k = 0; k < kWccChunk; ++k, ++r.iter) {
                 const WccOp op{r.parent, r.iter == 0 ? r.touched : nullptr, r.cnt + (r.iter & 1)};
                 side_sweep_kernel<<<grid, kThreads, 0, st>>>(runs, R, units, g->d_rec, op, r.flags, nullptr);
-                side_wcc_post<<<blocks_for(g->N, ctx), kThreads, 0, st>>>(r.parent, g->N, r.cnt, r.iter, r.flags);
+                side_wcc_post<<<short_blocks(g->N), kThreads, 0, st>>>(r.parent, g->N, r.cnt, r.iter, r.flags);
                 s->kernel_launches += 2;
             }
             break;
         case GS_ALGO_KCORE:
             for (int k = 0; k < kKcoreChunk; ++k, ++r.iter) {
                 const int p = r.iter & 1;
-                side_kcore_round<<<blocks_for(g->N, ctx), kThreads, 0, st>>>(
+                side_kcore_round<<<short_blocks(g->N), kThreads, 0, st>>>(
                     r.deg, r.removed, r.act[p], r.act[p ^ 1], g->nw, g->N / 32, (int)r.arg, r.cnt, r.iter, r.flags);
                 const KcoreOp op{r.deg, r.removed, r.act[p]};
                 side_sweep_kernel<<<grid, kThreads, 0, st>>>(runs, R, units, g->d_rec, op, r.flags, r.cnt + p);
@@ -696,7 +691,7 @@ gs_status queue_chunk(gs_server* s, Request& r) {
             break;
         default:
             for (; r.iter < r.arg; ++r.iter) {
-                GS_TRY(pr_slice_sweep(g, st, r.x, r.y, r.flags + 1));
+                GS_TRY(pr_slice_sweep(g, st, r.x, r.y, r.flags + 1, true));
                 GS_TRY(pr_finalize_launch(ctx, st, r.x, r.y, r.r, g->d_degree, g->N, g->V, 0));
                 s->kernel_launches += 2;
             }
@@ -811,7 +806,9 @@ void retire(gs_server* s, const std::vector<uint64_t>& finished, double t) {
         r.state = r.status == GS_OK ? kDone : kFailed;
         r.t_done = t;
         release(s, r);
+        s->completed.push_back(id);
         for (uint64_t f : r.followers) {
+            s->completed.push_back(f);
             Request& fr = s->reqs[f];
             fr.state = r.state;
             fr.status = r.status;
@@ -887,17 +884,32 @@ gs_status bfs_step(gs_server* s) {
     }
     s->step += 1;
     if (finished.empty()) return GS_OK;
+    // per graph: the retiring slots' bits cleared in one pass; per request:
+    // its depth plane copied to pinned host memory, then zeroed
+    std::vector<unsigned long long> retiring(s->graphs.size(), 0);
     for (uint64_t id : finished) {
         Request& r = s->reqs[id];
+        retiring[r.graph] |= 1ull << r.slot;
+    }
+    for (int g = 0; g < (int)s->graphs.size(); ++g) {
+        if (!retiring[g]) continue;
+        const SrvGraph& sg = s->graphs[g];
+        serve_clear_slots<<<blocks_for(sg.g->N, ctx), kThreads, 0, s->stream>>>(sg.fv, sg.g->N, ~retiring[g]);
+        s->kernel_launches++;
+    }
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    for (uint64_t id : finished) {
+        Request& r = s->reqs[id];
+        const SrvGraph& sg = s->graphs[r.graph];
+        uint8_t* plane = sg.depth + (size_t)r.slot * sg.g->N;
         if (r.status == GS_OK) {
-            GS_TRY(take_result(s, r));
-        } else {
-            // clear the slot for its next request (result discarded)
-            SrvGraph& sg = s->graphs[r.graph];
-            serve_take_bfs<<<blocks_for(sg.g->N, ctx), kThreads, 0, s->stream>>>(sg.fv, sg.depth, r.slot, sg.out,
-                                                                                 sg.g->V, sg.g->N);
-            s->kernel_launches++;
+            gs_status st = GS_OK;
+            r.result_bytes = sg.g->V;
+            r.result = host_buf(s, r.result_bytes, &st);
+            if (st != GS_OK) return st;
+            GS_CHECK_CUDA(ctx, cudaMemcpyAsync(r.result->p, plane, r.result_bytes, cudaMemcpyDeviceToHost, s->stream));
         }
+        GS_CHECK_CUDA(ctx, cudaMemsetAsync(plane, 0, sg.g->N, s->stream));
     }
     GS_CHECK_CUDA(ctx, cudaStreamSynchronize(s->stream));
     retire(s, finished, now_s(s));
@@ -935,7 +947,7 @@ gs_status side_step(gs_server* s) {
             }
             if (done) {
                 GS_TRY(take_result(s, r));
-                GS_CHECK_CUDA(ctx, cudaEventRecord(s->side_ev[r.side], s->side_stream[r.side % kSideStreams]));
+                GS_CHECK_CUDA(ctx, cudaEventRecord(s->side_ev[r.side], side_stream_of(s, r)));
                 r.result_pending = true;
                 continue;
             }
@@ -968,6 +980,25 @@ gs_status gs_serve_step(gs_server* s, int* n_active, int* n_queued) {
     GS_TRY(bfs_step(s));
     if (n_active) *n_active = (int)s->active.size();
     if (n_queued) *n_queued = (int)s->queue.size();
+    return GS_OK;
+}
+
+gs_status gs_serve_completed(gs_server* s, uint64_t* ids, int max_ids, int* n) {
+    if (!s || !n || max_ids < 0 || (max_ids && !ids)) return GS_ERR_ARG;
+    int k = 0;
+    while (k < max_ids && !s->completed.empty()) {
+        ids[k++] = s->completed.front();
+        s->completed.pop_front();
+    }
+    *n = k;
+    return GS_OK;
+}
+
+gs_status gs_serve_set_side_streams(gs_server* s, int n) {
+    if (!s || n < 1 || n > kSideStreams) return GS_ERR_ARG;
+    for (uint64_t id : s->active)
+        if (s->reqs[id].side >= 0) return gs_fail(s->ctx, GS_ERR_STATE, "side requests in flight");
+    s->n_side = n;
     return GS_OK;
 }
 

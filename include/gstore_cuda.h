@@ -229,22 +229,30 @@ gs_status gs_batch_free(gs_batch* b);
 /* Replaces: one gstoreu process per query (gstore.cpp:250-333), as a
  * request loop.  Graphs are registered resident graphs; requests (BFS root,
  * k-core k, PageRank iterations, WCC) are queued by gs_serve_submit and
- * advanced by gs_serve_step: each step admits queued requests in arrival
- * order while their device state fits state_budget_bytes (0 = 32 GiB) and a
- * slot is free (64 BFS requests per graph share bit-parallel frontier
- * words), runs one iteration of every admitted request in one CUDA-graph
- * launch (a sweep kernel and a post kernel over all of them), and retires
- * finished ones into pinned host buffers.  A request identical to one
- * queued or running (same graph, algorithm and argument) shares its run.
- * Results equal gs_run's for the same query (BFS/WCC/k-core bit for bit,
- * PageRank within float rounding).  Times are seconds of the server's
- * steady clock (gs_serve_clock).  States: 0 queued, 1 running, 2 done,
- * 3 failed. */
+ * advanced by gs_serve_step, which never blocks on side work.  Each step
+ * admits queued requests in arrival order while their device state fits
+ * state_budget_bytes (0 = 32 GiB) and a slot is free; runs one level of
+ * every graph's BFS group (up to 64 BFS requests per graph share
+ * bit-parallel frontier words and join at any level) in one CUDA-graph
+ * launch; and advances the WCC / k-core / PageRank requests, which run to
+ * completion on lower-priority side streams in chunks of iterations (64
+ * slots).  Finished requests are retired into pinned host buffers and
+ * listed by gs_serve_completed.  A request identical to one queued or
+ * running (same graph, algorithm and argument) shares its run.  Results
+ * equal gs_run's for the same query (BFS/WCC/k-core bit for bit, PageRank
+ * within float rounding).  Times are seconds of the server's steady clock
+ * (gs_serve_clock).  States: 0 queued, 1 running, 2 done, 3 failed. */
 gs_status gs_serve_create(gs_ctx* ctx, uint64_t state_budget_bytes, gs_server** out);
 gs_status gs_serve_add_graph(gs_server* s, gs_graph* g, int* graph_id);
 gs_status gs_serve_submit(gs_server* s, int graph_id, gs_algo algo, int64_t arg, uint64_t* request_id);
 gs_status gs_serve_step(gs_server* s, int* n_active, int* n_queued);
 gs_status gs_serve_poll(gs_server* s, uint64_t request_id, int* state);
+/* Ids of requests finished (done or failed) since the last call, oldest
+ * first, at most max_ids of them; *n = how many were written. */
+gs_status gs_serve_completed(gs_server* s, uint64_t* ids, int max_ids, int* n);
+/* Side streams the WCC / k-core / PageRank requests spread over (1-8,
+ * default 8); only while none of those requests is running. */
+gs_status gs_serve_set_side_streams(gs_server* s, int n);
 /* Copies a finished request's result (gs_download's format; host_dst may be
  * NULL) and forgets the request.  A failed request returns its status. */
 gs_status gs_serve_result(gs_server* s, uint64_t request_id, void* host_dst, uint64_t bytes,
