@@ -366,14 +366,35 @@ static gs_status build_tables(gs_graph* g) {
     if (!runs.empty())
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_runs, runs.data(), runs.size() * sizeof(gs_tile_run),
                                            cudaMemcpyHostToDevice, ctx->stream));
-    // the BFS sweep's order: longest runs first, so that the runs drawn last
-    // (from the sweep's ticket) are the short ones
+    // The BFS sweep's runs, longest first, so that the runs drawn last from
+    // the sweep's ticket are the short ones.  A graph with fewer than
+    // kBfsRunsPerCta runs per CTA of the sweep has its runs cut into pieces
+    // of 32, 16 or 8 units (the largest cut that gives that many pieces):
+    // pieces spread a small grid over the machine, while on a large grid
+    // whole runs pay their per-run set-up (row state, flush) over more
+    // records.
     std::vector<gs_tile_run> lpt;
     if (!g->stream && !runs.empty()) {
-        lpt = runs;
+        const uint64_t want = kBfsRunsPerCta * gs_grid_size(ctx, kBfsCtasPerSm);
+        uint32_t cut = 0;   // whole runs
+        if (runs.size() < want)
+            for (cut = 32; cut > kBfsMinRunUnits; cut /= 2) {
+                uint64_t pieces = 0;
+                for (const gs_tile_run& r : runs) pieces += (r.unit_end - r.unit_beg + cut - 1) / cut;
+                if (pieces >= want) break;
+            }
+        if (cut == 0) cut = UINT32_MAX;
+        for (const gs_tile_run& r : runs)
+            for (uint32_t u = r.unit_beg; u < r.unit_end;) {
+                const uint32_t ue = (uint32_t)std::min<uint64_t>(r.unit_end, (uint64_t)u + cut);
+                lpt.push_back(gs_tile_run{units[u].rec_beg, units[ue - 1].rec_beg + units[ue - 1].n, r.tile_beg,
+                                          r.tile_end, u, ue});
+                u = ue;
+            }
         std::stable_sort(lpt.begin(), lpt.end(), [](const gs_tile_run& x, const gs_tile_run& y) {
             return x.rec_end - x.rec_beg > y.rec_end - y.rec_beg;
         });
+        g->R_lpt = lpt.size();
         GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_runs_lpt, lpt.size() * sizeof(gs_tile_run)));
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_runs_lpt, lpt.data(), lpt.size() * sizeof(gs_tile_run),
                                            cudaMemcpyHostToDevice, ctx->stream));

@@ -327,12 +327,12 @@ gs_status bfs_sweep_launch(gs_state* s) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
     // every run of the resident graph, or the entries of the current segment
-    const uint64_t n_runs = g->seg.list ? g->seg.n : g->R;
+    const uint64_t n_runs = g->seg.list ? g->seg.n : (g->d_runs_lpt ? g->R_lpt : g->R);
     if (n_runs == 0) return GS_OK;
     RunArgs a{g->d_runs_lpt ? g->d_runs_lpt : g->d_runs, n_runs, g->d_units, g->seg.list ? g->seg.buf : g->d_rec,
               s->d_front, s->d_visited,
               s->d_act, s->d_act_next, g->directed, (int*)s->d_error, g->seg.list, s->d_ticket};
-    const uint32_t grid = (uint32_t)std::min<uint64_t>(n_runs, gs_grid_size(ctx, 6));
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(n_runs, gs_grid_size(ctx, kBfsCtasPerSm));
     gs_timer_begin(ctx);
     bfs_run_kernel<<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
@@ -392,9 +392,10 @@ gs_status bfs_level_into(gs_ctx* ctx, const gs_graph* g, uint8_t* depth, uint32_
                                                     (int)sizeof(BfsSmem)));
             attr_set[ctx->device & 63] = true;
         }
-        RunArgs a{g->d_runs_lpt ? g->d_runs_lpt : g->d_runs, g->R, g->d_units, g->d_rec, st, next, act, act_next,
+        const uint64_t n_runs = g->d_runs_lpt ? g->R_lpt : g->R;
+        RunArgs a{g->d_runs_lpt ? g->d_runs_lpt : g->d_runs, n_runs, g->d_units, g->d_rec, st, next, act, act_next,
                   g->directed, error, nullptr, ticket};
-        const uint32_t grid = (uint32_t)std::min<uint64_t>(g->R, gs_grid_size(ctx, 6));
+        const uint32_t grid = (uint32_t)std::min<uint64_t>(n_runs, gs_grid_size(ctx, kBfsCtasPerSm));
         bfs_run_kernel<<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
         GS_CHECK_CUDA(ctx, cudaGetLastError());
         ctx->launches++;

@@ -51,6 +51,9 @@ constexpr uint32_t kBlockWindows = 64;
 constexpr uint32_t kBlockWindowsSmall = 32;
 // Units per run of the L2-blocked order.
 constexpr uint32_t kBlockRunUnits = 8;
+constexpr uint32_t kBfsMinRunUnits = 8;     // BFS sweep: smallest run piece
+constexpr uint64_t kBfsRunsPerCta = 4;      // BFS sweep: run pieces wanted per CTA
+constexpr int kBfsCtasPerSm = 6;            // BFS sweep: resident CTAs per SM
 
 // One unit: records [rec_beg, rec_beg + n) of the tile at row rc >> 16,
 // column rc & 0xFFFF (n <= kUnitRecords; units follow the file order).
@@ -143,7 +146,8 @@ struct gs_graph {
     gs_item* d_items = nullptr;
     gs_tile_run* d_runs = nullptr;
     gs_unit* d_units = nullptr;
-    gs_tile_run* d_runs_lpt = nullptr; // the R runs, longest first (resident graphs; BFS sweep order)
+    gs_tile_run* d_runs_lpt = nullptr; // BFS sweep: runs (maybe cut into pieces), longest first (resident)
+    uint64_t R_lpt = 0;
     uint64_t R_blk = 0;               // runs of the L2-blocked order (resident graphs)
     gs_tile_run* d_runs_blk = nullptr;
     gs_unit* d_units_blk = nullptr;
