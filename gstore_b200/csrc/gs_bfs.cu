@@ -13,7 +13,8 @@
 // brought into shared memory once per run with one cp.async.bulk copy; the
 // run's units (tile slices of <= kUnitRecords records) are spread over the
 // warps, each warp streaming its unit's records with 128-bit evict-first
-// loads.  Per record: the row end's state comes from shared memory, the
+// loads, each lane loading its next 2 x 16 bytes before it visits the
+// current ones.  Per record: the row end's state comes from shared memory, the
 // column end's from global memory through L1 — tiles written by the device
 // converter are sorted by column offset, so the 32 lookups of a warp fall
 // on a few neighbouring lines.  A discovered row end sets a bit in a
@@ -80,7 +81,9 @@ struct RunArgs {
     unsigned int* ticket;
 };
 
-__global__ void __launch_bounds__(kThreads) bfs_run_kernel(RunArgs a) {
+// Six CTAs per SM (48 warps): the register cap this sets (40) costs a few
+// spilled bytes, and measured faster than 48 registers at five CTAs.
+__global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     BfsSmem& m = *reinterpret_cast<BfsSmem*>(smem_raw);
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -173,21 +176,26 @@ __global__ void __launch_bounds__(kThreads) bfs_run_kernel(RunArgs a) {
             if (ae + lane < e) visit(__ldcs(rec + ae + lane));
             const uint4* r4 = reinterpret_cast<const uint4*>(rec + ab);
             const uint32_t n4 = (uint32_t)((ae - ab) >> 2);
+            // the next iteration's records are loaded before this one's are
+            // visited, so the loads overlap the lookups
+            const uint4 z = make_uint4(0, 0, 0, 0);
+            uint4 q0 = lane < n4 ? __ldcs(r4 + lane) : z;
+            uint4 q1 = lane + 32 < n4 ? __ldcs(r4 + lane + 32) : z;
             for (uint32_t k = lane; k < n4; k += 64) {
-                const uint4 q0 = __ldcs(r4 + k);
-                const bool two = k + 32 < n4;
-                uint4 q1 = make_uint4(0, 0, 0, 0);
-                if (two) q1 = __ldcs(r4 + k + 32);
+                const uint4 p0 = k + 64 < n4 ? __ldcs(r4 + k + 64) : z;
+                const uint4 p1 = k + 96 < n4 ? __ldcs(r4 + k + 96) : z;
                 visit(q0.x);
                 visit(q0.y);
                 visit(q0.z);
                 visit(q0.w);
-                if (two) {
+                if (k + 32 < n4) {
                     visit(q1.x);
                     visit(q1.y);
                     visit(q1.z);
                     visit(q1.w);
                 }
+                q0 = p0;
+                q1 = p1;
             }
             if (__any_sync(0xFFFFFFFFu, hit) && lane == 0) a.act_next[col] = 1;   // read_part_next->set_bit_atomic(j)
         }
