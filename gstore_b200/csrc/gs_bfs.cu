@@ -14,7 +14,9 @@
 // run's units (tile slices of <= kUnitRecords records) are spread over the
 // warps, each warp streaming its unit's records with 128-bit evict-first
 // loads, each lane loading its next 2 x 16 bytes before it visits the
-// current ones.  Per record: the row end's state comes from shared memory, the
+// current ones and classifying four records before it acts on any of them
+// (the discovery path is one branch per four records).  Per record: the row
+// end's state comes from shared memory, the
 // column end's from global memory through L1 — tiles written by the device
 // converter are sorted by column offset, so the 32 lookups of a warp fall
 // on a few neighbouring lines.  A discovered row end sets a bit in a
@@ -152,11 +154,14 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
             // bit 0: the column end is discovered (row end in the frontier,
             // column end unvisited, bfs.cpp:158-164); bit 1: the row end
             // (bfs.cpp:166-172)
-            auto visit = [&](uint32_t r) {
+            auto classify = [&](uint32_t r) -> uint32_t {
                 const uint32_t v0 = r & 0xFFFFu, v1 = r >> 16;
                 const uint32_t s0 = m.strow[v0 >> 4] >> ((v0 & 15) << 1);
                 const uint32_t s1 = __ldg(colst + (v1 >> 4)) >> ((v1 & 15) << 1);
-                const uint32_t c = (s0 & ~(s1 >> 1) & mr) | (((s1 & ~(s0 >> 1)) << 1) & mc);
+                return ((s0 & ~(s1 >> 1) & mr) | (((s1 & ~(s0 >> 1)) << 1) & mc)) & 3u;
+            };
+            auto discover = [&](uint32_t r, uint32_t c) {
+                const uint32_t v0 = r & 0xFFFFu, v1 = r >> 16;
                 if (c & 1u) {
                     atomicOr(next_col + (v1 >> 5), 1u << (v1 & 31));
                     hit = true;
@@ -165,6 +170,21 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
                     const uint32_t w = v0 >> 5, bit = 1u << (v0 & 31);
                     if (!(m.nx[w] & bit) && atomicOr(m.nx + w, bit) == 0)
                         atomicOr(m.dirty + (w >> 5), 1u << (w & 31));
+                }
+            };
+            auto visit = [&](uint32_t r) {
+                const uint32_t c = classify(r);
+                if (c) discover(r, c);
+            };
+            // four records classified before any is acted on: one branch
+            // per four records in a level that discovers little
+            auto visit4 = [&](const uint4 q) {
+                const uint32_t c0 = classify(q.x), c1 = classify(q.y), c2 = classify(q.z), c3 = classify(q.w);
+                if (c0 | c1 | c2 | c3) {
+                    if (c0) discover(q.x, c0);
+                    if (c1) discover(q.y, c1);
+                    if (c2) discover(q.z, c2);
+                    if (c3) discover(q.w, c3);
                 }
             };
             const uint64_t b = d.rec_beg, e = d.rec_beg + d.n;
@@ -184,16 +204,8 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
             for (uint32_t k = lane; k < n4; k += 64) {
                 const uint4 p0 = k + 64 < n4 ? __ldcs(r4 + k + 64) : z;
                 const uint4 p1 = k + 96 < n4 ? __ldcs(r4 + k + 96) : z;
-                visit(q0.x);
-                visit(q0.y);
-                visit(q0.z);
-                visit(q0.w);
-                if (k + 32 < n4) {
-                    visit(q1.x);
-                    visit(q1.y);
-                    visit(q1.z);
-                    visit(q1.w);
-                }
+                visit4(q0);
+                if (k + 32 < n4) visit4(q1);
                 q0 = p0;
                 q1 = p1;
             }
