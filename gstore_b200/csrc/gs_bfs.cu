@@ -154,11 +154,15 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
             // bit 0: the column end is discovered (row end in the frontier,
             // column end unvisited, bfs.cpp:158-164); bit 1: the row end
             // (bfs.cpp:166-172)
+            // a vertex's two state bits rotated down to bits 0-1 (the
+            // rotation takes its amount mod 32); the bits above them do not
+            // reach the class
             auto classify = [&](uint32_t r) -> uint32_t {
-                const uint32_t v0 = r & 0xFFFFu, v1 = r >> 16;
-                const uint32_t s0 = m.strow[v0 >> 4] >> ((v0 & 15) << 1);
-                const uint32_t s1 = __ldg(colst + (v1 >> 4)) >> ((v1 & 15) << 1);
-                return ((s0 & ~(s1 >> 1) & mr) | (((s1 & ~(s0 >> 1)) << 1) & mc)) & 3u;
+                const uint32_t w0 = m.strow[(r & 0xFFFFu) >> 4];
+                const uint32_t w1 = __ldg(colst + (r >> 20));
+                const uint32_t s0 = __funnelshift_r(w0, w0, r << 1);
+                const uint32_t s1 = __funnelshift_r(w1, w1, (r >> 16) << 1);
+                return (s0 & ~(s1 >> 1) & mr) | (((s1 & ~(s0 >> 1)) << 1) & mc);
             };
             auto discover = [&](uint32_t r, uint32_t c) {
                 const uint32_t v0 = r & 0xFFFFu, v1 = r >> 16;
