@@ -9,7 +9,9 @@
 //     next[v1] |= frontier[v0] & ~visited[v1]
 //     next[v0] |= frontier[v1] & ~visited[v0]     (half grid)
 // and the finalize turns next into the new frontier and writes depth level+1
-// for each new (vertex, query) bit (iteration_finalize, bfs.cpp:187-224).  A
+// for each new (vertex, query) bit (iteration_finalize, bfs.cpp:187-224)
+// into the query's depth plane ([bits][N], so a warp's 32 consecutive
+// vertices write one sector per query).  A
 // tile is swept when its row or column window holds a frontier vertex of any
 // query.  Per query the depths equal the single-root BFS bit for bit: a
 // vertex's depth is its level distance, whichever query shares the sweep.
@@ -97,7 +99,7 @@ struct MsArgs {
     uint32_t nw;
     FvPair<W>* fv;
     W* next;
-    uint8_t* depth;                  // [N][bits]
+    uint8_t* depth;                  // [bits][N]: one plane per query
     uint8_t* act;                    // 2 x nw, by level parity
     unsigned long long* total;       // fresh (vertex, query) pairs per level, [256]
     W* overflow;                     // queries that reached a depth over 254
@@ -107,11 +109,11 @@ struct MsArgs {
     int directed;
     const gs_pr_item* items;         // row-slice order: (row, slice, column block) items
     uint64_t n_items;
+    unsigned int* tickets;           // [256]: next run of each level's sweep
 };
 
 template <class W>
 __global__ void __launch_bounds__(kThreads) msbfs_kernel(MsArgs<W> a) {
-    constexpr int kBits = sizeof(W) * 8;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
@@ -121,10 +123,18 @@ __global__ void __launch_bounds__(kThreads) msbfs_kernel(MsArgs<W> a) {
         uint8_t* act_next = a.act + ((level + 1) & 1) * a.nw;
         // the flags of the next frontier start empty (last read one level ago)
         for (uint64_t w = tid; w < a.nw; w += nth) act_next[w] = 0;
-        // sweep: a CTA per run, a warp per unit; a tile is swept when its row
-        // (or, half grid, column) window holds a frontier vertex of any query
-        // (grid::bfs_mmap, gstore.cpp:2671-2698)
-        for (uint64_t i = blockIdx.x; i < a.R; i += gridDim.x) {
+        // sweep: a CTA per run (drawn from the level's ticket), a warp per
+        // unit; a tile is swept when its row (or, half grid, column) window
+        // holds a frontier vertex of any query (grid::bfs_mmap,
+        // gstore.cpp:2671-2698)
+        __shared__ unsigned long long s_run;
+        auto draw = [&]() -> uint64_t {
+            __syncthreads();   // every thread has read the previous draw
+            if (threadIdx.x == 0) s_run = atomicAdd(a.tickets + level, 1u);
+            __syncthreads();
+            return s_run;
+        };
+        for (uint64_t i = draw(); i < a.R; i = draw()) {
             const gs_tile_run run = a.runs[i];
             const uint32_t row = a.units[run.unit_beg].rc >> 16;
             const bool ar = __ldcg(act + row) != 0;
@@ -140,20 +150,26 @@ __global__ void __launch_bounds__(kThreads) msbfs_kernel(MsArgs<W> a) {
         for (uint64_t v = tid; v < a.N; v += nth) {
             const W nx = __ldcg(a.next + v);
             const FvPair<W> s = load_fv(a.fv + v);
-            if (nx == 0 && s.f == 0) continue;
-            if (nx) __stcg(a.next + v, (W)0);
-            const W fresh = nx & ~s.vis;
-            store_fv(a.fv + v, fresh, s.vis | fresh);
-            if (fresh) {
-                local += popc_w(fresh);
+            W fresh = 0;
+            if (nx != 0 || s.f != 0) {
+                if (nx) __stcg(a.next + v, (W)0);
+                fresh = nx & ~s.vis;
+                store_fv(a.fv + v, fresh, s.vis | fresh);
+            }
+            // depth planes written per query for the warp's 32 consecutive
+            // vertices at once (one sector per plane)
+            const W any = warp_or(fresh);
+            if (!any) continue;
+            if (fresh) local += popc_w(fresh);
+            if (lane == 0) {
                 act_next[v >> 16] = 1;
-                if (level == 254) atomicOr(a.overflow, fresh);
-                W x = fresh;
-                while (x) {
-                    const int q = ffs_w(x) - 1;
-                    a.depth[v * kBits + q] = (uint8_t)(level + 1);
-                    x &= x - 1;
-                }
+                if (level == 254) atomicOr(a.overflow, any);
+            }
+            W x = any;
+            while (x) {
+                const int q = ffs_w(x) - 1;
+                if (fresh >> q & 1) a.depth[(uint64_t)q * a.N + v] = (uint8_t)(level + 1);
+                x &= x - 1;
             }
         }
         warp_add_u64(a.total + level, local);
@@ -207,7 +223,6 @@ struct MsSliceOp {
 
 template <class W>
 __global__ void __launch_bounds__(kSliceThreads) msbfs_slice_kernel(MsArgs<W> a) {
-    constexpr int kBits = sizeof(W) * 8;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     FvPair<W>* fvs = reinterpret_cast<FvPair<W>*>(smem_raw);
     W* nxs = reinterpret_cast<W*>(smem_raw + kSliceV * sizeof(FvPair<W>));
@@ -250,20 +265,26 @@ __global__ void __launch_bounds__(kSliceThreads) msbfs_slice_kernel(MsArgs<W> a)
         for (uint64_t v = gtid; v < a.N; v += nth) {
             const W nx = __ldcg(a.next + v);
             const FvPair<W> s = load_fv(a.fv + v);
-            if (nx == 0 && s.f == 0) continue;
-            if (nx) __stcg(a.next + v, (W)0);
-            const W fresh = nx & ~s.vis;
-            store_fv(a.fv + v, fresh, s.vis | fresh);
-            if (fresh) {
-                local += popc_w(fresh);
+            W fresh = 0;
+            if (nx != 0 || s.f != 0) {
+                if (nx) __stcg(a.next + v, (W)0);
+                fresh = nx & ~s.vis;
+                store_fv(a.fv + v, fresh, s.vis | fresh);
+            }
+            // depth planes written per query for the warp's 32 consecutive
+            // vertices at once (one sector per plane)
+            const W any = warp_or(fresh);
+            if (!any) continue;
+            if (fresh) local += popc_w(fresh);
+            if (lane == 0) {
                 act_next[v >> 16] = 1;
-                if (level == 254) atomicOr(a.overflow, fresh);
-                W x = fresh;
-                while (x) {
-                    const int q = ffs_w(x) - 1;
-                    a.depth[v * kBits + q] = (uint8_t)(level + 1);
-                    x &= x - 1;
-                }
+                if (level == 254) atomicOr(a.overflow, any);
+            }
+            W x = any;
+            while (x) {
+                const int q = ffs_w(x) - 1;
+                if (fresh >> q & 1) a.depth[(uint64_t)q * a.N + v] = (uint8_t)(level + 1);
+                x &= x - 1;
             }
         }
         warp_add_u64(a.total + level, local);
@@ -279,35 +300,27 @@ __global__ void __launch_bounds__(kSliceThreads) msbfs_slice_kernel(MsArgs<W> a)
 // Root seeding: depth 1, frontier and visited bit of query q (bfs.cpp:70).
 // (one thread: several queries may share a root)
 template <class W>
-__global__ void msbfs_seed_kernel(const uint64_t* roots, int n, FvPair<W>* fv, uint8_t* depth, uint8_t* act1) {
-    constexpr int kBits = sizeof(W) * 8;
+__global__ void msbfs_seed_kernel(const uint64_t* roots, int n, FvPair<W>* fv, uint8_t* depth, uint64_t N,
+                                  uint8_t* act1) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     for (int q = 0; q < n; ++q) {
         const uint64_t r = roots[q];
         fv[r].f |= (W)1 << q;
         fv[r].vis |= (W)1 << q;
-        depth[r * kBits + q] = 1;
+        depth[(uint64_t)q * N + r] = 1;
         act1[r >> 16] = 1;   // calc_part_needed (bfs.cpp:324-338); level 1 has parity 1
     }
 }
 
-// Per query: depth column q of [N][bits] into a contiguous V-byte array.
-__global__ void gather_depth_kernel(const uint8_t* __restrict__ depth, int bits, int q, uint8_t* __restrict__ out,
-                                    uint64_t V) {
-    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t v = tid; v < V; v += nth) out[v] = depth[v * bits + q];
-}
-
-// Per query and depth: vertex counts (the per-level frontier counts).
-__global__ void depth_histogram_kernel(const uint8_t* __restrict__ depth, int bits, int n_queries, uint64_t V,
+// Per query and depth: vertex counts (the per-level frontier counts) of the
+// planes [n_queries][N] (first V bytes of each).
+__global__ void depth_histogram_kernel(const uint8_t* __restrict__ depth, uint64_t N, int n_queries, uint64_t V,
                                        unsigned long long* hist /* [n_queries][256] */) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = tid; i < V * bits; i += nth) {
-        const int q = (int)(i % bits);
-        if (q >= n_queries) continue;
-        const uint8_t d = depth[i];
+    for (uint64_t i = tid; i < V * (uint64_t)n_queries; i += nth) {
+        const uint64_t q = i / V, v = i - q * V;
+        const uint8_t d = depth[q * N + v];
         if (d) atomicAdd(hist + q * 256 + d, 1ull);
     }
 }
@@ -495,7 +508,7 @@ struct gs_bfs_group {
     int bits = 64;
     int order = 1;                     // 0 file order, 1 / 2: 64- / 32-window blocks, 3 row slices
     std::vector<int> queries;
-    uint8_t* depth = nullptr;          // [N][bits]
+    uint8_t* depth = nullptr;          // [bits][N]: one plane per query
     int levels = 0;
     unsigned long long overflow = 0;
     std::vector<uint64_t> hist;        // [queries][256], filled on demand
@@ -577,7 +590,7 @@ gs_status run_bfs_group(gs_batch* b, gs_bfs_group& grp) {
     // device scratch: fv (N pairs), next (N words), act (2 nw), totals, bar, err, levels, overflow, roots
     const size_t fv_b = N * sizeof(FvPair<W>), nx_b = N * sizeof(W);
     const size_t act_b = (2 * (size_t)g->nw + 255) & ~(size_t)255;
-    const size_t small_b = 256 * 8 + 64 + 8 * kMaxBatch + 64;
+    const size_t small_b = 256 * 8 + 64 + 8 * kMaxBatch + 64 + 256 * 4;
     void* base = nullptr;
     GS_TRY(scratch(b, fv_b + nx_b + act_b + small_b, &base));
     char* p = (char*)base;
@@ -591,13 +604,14 @@ gs_status run_bfs_group(gs_batch* b, gs_bfs_group& grp) {
     int* levels = (int*)(small + 256 * 8 + 32);
     W* overflow = (W*)(small + 256 * 8 + 48);
     uint64_t* roots = (uint64_t*)(small + 256 * 8 + 64);
+    unsigned int* tickets = (unsigned int*)(small + 256 * 8 + 64 + 8 * kMaxBatch + 64);
     GS_TRY(gs_pool_get(ctx, N * kBits, (void**)&grp.depth));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(base, 0, fv_b + nx_b + act_b + small_b, ctx->stream));
-    GS_CHECK_CUDA(ctx, cudaMemsetAsync(grp.depth, 0, N * kBits, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(grp.depth, 0, N * n, ctx->stream));   // the queries' planes
     std::vector<uint64_t> h_roots(n);
     for (int i = 0; i < n; ++i) h_roots[i] = (uint64_t)b->q[grp.queries[i]].arg;
     GS_CHECK_CUDA(ctx, cudaMemcpyAsync(roots, h_roots.data(), n * 8, cudaMemcpyHostToDevice, ctx->stream));
-    msbfs_seed_kernel<W><<<1, 1, 0, ctx->stream>>>(roots, n, fv, grp.depth, act + g->nw);
+    msbfs_seed_kernel<W><<<1, 1, 0, ctx->stream>>>(roots, n, fv, grp.depth, N, act + g->nw);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches += 1;
     const gs_tile_run* runs = grp.order == 1 ? g->d_runs_blk : grp.order == 2 ? g->d_runs_blk2 : g->d_runs;
@@ -620,7 +634,8 @@ gs_status run_bfs_group(gs_batch* b, gs_bfs_group& grp) {
                 levels,
                 g->directed,
                 nullptr,
-                0};
+                0,
+                tickets};
     void* args[] = {&a};
     GS_CHECK_CUDA(ctx, cudaEventRecord(b->e0, ctx->stream));
     if (grp.order == 3) {
@@ -900,10 +915,7 @@ gs_status gs_batch_download(gs_batch* b, int query_id, int what, void* host_dst,
     const void* src = nullptr;
     if (q->algo == GS_ALGO_BFS) {
         const gs_bfs_group& grp = b->groups[q->group];
-        gather_depth_kernel<<<blocks_for(g->V, ctx), kThreads, 0, ctx->stream>>>(grp.depth, grp.bits, q->lane,
-                                                                                 (uint8_t*)tmp, g->V);
-        ctx->launches++;
-        src = tmp;
+        src = grp.depth + (size_t)q->lane * g->N;   // the query's depth plane
     } else if (q->algo == GS_ALGO_WCC) {
         wk_labels_kernel<<<blocks_for(g->V, ctx), kThreads, 0, ctx->stream>>>(q->parent, q->touched, (uint32_t*)tmp,
                                                                               g->V, (unsigned long long*)ctx->d_scalars);
@@ -962,8 +974,8 @@ gs_status gs_batch_bfs_levels(gs_batch* b, int query_id, uint64_t* level_counts,
         void* tmp = nullptr;
         GS_TRY(scratch(b, (size_t)n * 256 * 8, &tmp));
         GS_CHECK_CUDA(ctx, cudaMemsetAsync(tmp, 0, (size_t)n * 256 * 8, ctx->stream));
-        depth_histogram_kernel<<<blocks_for(grp.g->V * grp.bits, ctx), kThreads, 0, ctx->stream>>>(
-            grp.depth, grp.bits, n, grp.g->V, (unsigned long long*)tmp);
+        depth_histogram_kernel<<<blocks_for(grp.g->V * n, ctx), kThreads, 0, ctx->stream>>>(
+            grp.depth, grp.g->N, n, grp.g->V, (unsigned long long*)tmp);
         ctx->launches++;
         GS_CHECK_CUDA(ctx, cudaGetLastError());
         grp.hist.resize((size_t)n * 256);

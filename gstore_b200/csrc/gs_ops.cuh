@@ -223,6 +223,12 @@ __device__ __forceinline__ void store_fv(FvPair<unsigned long long>* p, unsigned
 }
 __device__ __forceinline__ int popc_w(uint32_t x) { return __popc(x); }
 __device__ __forceinline__ int popc_w(unsigned long long x) { return __popcll(x); }
+template <class W>
+__device__ __forceinline__ W warp_or(W x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x |= __shfl_xor_sync(kFull, x, o);
+    return x;
+}
 __device__ __forceinline__ int ffs_w(uint32_t x) { return __ffs(x); }
 __device__ __forceinline__ int ffs_w(unsigned long long x) { return __ffsll((long long)x); }
 
