@@ -93,7 +93,10 @@ __device__ __forceinline__ int job_of(const Table* t, uint64_t x, bool by_words)
     return lo;
 }
 
-__global__ void __launch_bounds__(kThreads) serve_sweep_kernel(const Table* __restrict__ t) {
+// A CTA takes the next run of the concatenated lists from `ticket` (zeroed
+// by the step before the launch).
+__global__ void __launch_bounds__(kThreads) serve_sweep_kernel(const Table* __restrict__ t,
+                                                               unsigned long long* ticket) {
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n_jobs = t->n_jobs;
     // the flags the post kernel sets start empty
@@ -101,7 +104,14 @@ __global__ void __launch_bounds__(kThreads) serve_sweep_kernel(const Table* __re
         const Job& jb = t->jobs[j];
         for (uint32_t w = threadIdx.x; w < jb.nw; w += blockDim.x) jb.act_next[w] = 0;
     }
-    for (uint64_t x = blockIdx.x; x < t->total_runs; x += gridDim.x) {
+    __shared__ unsigned long long s_run;
+    auto draw = [&]() -> uint64_t {
+        __syncthreads();   // every thread has read the previous draw
+        if (threadIdx.x == 0) s_run = atomicAdd(ticket, 1ull);
+        __syncthreads();
+        return s_run;
+    };
+    for (uint64_t x = draw(); x < t->total_runs; x = draw()) {
         const Job& jb = t->jobs[job_of(t, x, false)];
         const gs_tile_run run = jb.runs[x - jb.run_beg];
         const uint32_t row = jb.units[run.unit_beg].rc >> 16;
@@ -355,7 +365,7 @@ struct gs_server {
     Table* h_table = nullptr;            // pinned
     Table* d_table = nullptr;
     unsigned long long* h_cnt = nullptr; // pinned, kMaxJobs x kCounters
-    unsigned long long* d_cnt = nullptr;
+    unsigned long long* d_cnt = nullptr; // kMaxJobs x kCounters, then the sweep ticket
     std::vector<SrvGraph> graphs;
     std::unordered_map<uint64_t, Request> reqs;
     std::deque<uint64_t> queue;
@@ -646,8 +656,9 @@ gs_status build_step_graph(gs_server* s) {
     const int grid = (int)gs_grid_size(ctx, 8);
     GS_CHECK_CUDA(ctx, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     cudaMemcpyAsync(s->d_table, s->h_table, sizeof(Table), cudaMemcpyHostToDevice, s->stream);
-    cudaMemsetAsync(s->d_cnt, 0, sizeof(unsigned long long) * kMaxJobs * kCounters, s->stream);
-    serve_sweep_kernel<<<grid, kThreads, 0, s->stream>>>(s->d_table);
+    // the job counters and, after them, the sweep's run ticket
+    cudaMemsetAsync(s->d_cnt, 0, sizeof(unsigned long long) * (kMaxJobs * kCounters + 1), s->stream);
+    serve_sweep_kernel<<<grid, kThreads, 0, s->stream>>>(s->d_table, s->d_cnt + kMaxJobs * kCounters);
     serve_post_kernel<<<grid, kThreads, 0, s->stream>>>(s->d_table);
     cudaMemcpyAsync(s->h_cnt, s->d_cnt, sizeof(unsigned long long) * kMaxJobs * kCounters, cudaMemcpyDeviceToHost,
                     s->stream);
@@ -731,7 +742,8 @@ gs_status gs_serve_create(gs_ctx* ctx, uint64_t state_budget_bytes, gs_server** 
                                             cudaHostAllocDefault);
     if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "server set-up");
     if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&s->d_table, sizeof(Table));
-    if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&s->d_cnt, sizeof(unsigned long long) * kMaxJobs * kCounters);
+    if (st == GS_OK)
+        st = gs_dev_alloc(ctx, (void**)&s->d_cnt, sizeof(unsigned long long) * (kMaxJobs * kCounters + 1));
     if (st == GS_OK) {
         std::memset(s->h_table, 0, sizeof(Table));
         st = build_step_graph(s);
