@@ -44,8 +44,9 @@ sys.path.insert(0, str(ROOT))
 
 HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes (read + write) per algorithmic byte of the BFS sweep kernel,
-# from one ncu capture of a full level at scale 22: 275.9 MB / 268.4 MB.
-BFS_DRAM_PER_ALG_BYTE = (271.015424 + 4.886016) / (67106947 * 4 / 1e6)
+# from one ncu capture of a full level at scale 25 (536,867,454 records):
+# 2,215.8 MB read + 22.4 MB written per 2,147.5 MB of records.
+BFS_DRAM_PER_ALG_BYTE = (2215.776 + 22.36288) / (536867454 * 4 / 1e6)
 
 
 def parse_args():
@@ -641,7 +642,7 @@ def main():
                 "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                 "traffic": BFS_DRAM_PER_ALG_BYTE * alg_per_launch,
                 "traffic_note": "bytes per launch: DRAM read+write per algorithmic byte from an ncu capture "
-                                "of a full level at scale 22, times this run's algorithmic bytes per launch",
+                                "of a full level at scale 25, times this run's algorithmic bytes per launch",
                 "algorithmic_bytes": "4 B x records in swept tiles per level",
                 "algorithmic_bytes_per_launch": alg_per_launch,
                 "launches": sweep_launches, "sweep_ms_total": sweep_ms}
