@@ -124,6 +124,8 @@ gs_status gs_create(gs_ctx** out, int device, uint64_t hbm_budget_bytes, int dir
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
     if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_scalars, 64 * sizeof(uint64_t));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_ticket, 4 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemset(ctx->d_ticket, 0, 4 * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->h_scalars, 64 * sizeof(uint64_t));
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) {
@@ -145,6 +147,7 @@ gs_status gs_destroy(gs_ctx* ctx) {
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->d_scalars) cudaFree(ctx->d_scalars);
+    if (ctx->d_ticket) cudaFree(ctx->d_ticket);
     if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);
     delete ctx;
     return GS_OK;

@@ -121,6 +121,9 @@ struct gs_ctx {
     KernelTimes ktime[8];
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint64_t* d_scalars = nullptr;   // small device scratch for counters/flags
+    // run tickets of the persistent sweeps on `stream` ([0..1] generic sweep,
+    // [2..3] PageRank sweep): zero at launch, zeroed again by the last CTA
+    unsigned int* d_ticket = nullptr;
     uint64_t* h_scalars = nullptr;   // pinned mirror
     int num_sms = 148;
     uint64_t launches = 0;           // kernels launched on this context

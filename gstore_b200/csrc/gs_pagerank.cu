@@ -102,7 +102,7 @@ struct PrSliceOp {
 __global__ void __launch_bounds__(kPrThreads, 2)
     pr_slice_kernel(const gs_pr_item* __restrict__ items, uint64_t n_items, const gs_unit* __restrict__ units,
                     const uint32_t* __restrict__ rec, const float* __restrict__ x, float* __restrict__ y,
-                    int directed, int* error) {
+                    int directed, int* error, unsigned int* ticket) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     PrSmem& m = *reinterpret_cast<PrSmem*>(smem_raw);
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -113,7 +113,16 @@ __global__ void __launch_bounds__(kPrThreads, 2)
     __syncthreads();
     const PrSliceOp op{m.xs, m.ys, x, y, directed};
     uint32_t parity = 0;
-    for (uint64_t i = blockIdx.x; i < n_items; i += gridDim.x) {
+    // the next item from `ticket` when one is given, else every gridDim.x-th
+    __shared__ unsigned long long s_item;
+    auto advance = [&](uint64_t i) -> uint64_t {
+        if (!ticket) return i + gridDim.x;
+        __syncthreads();   // every thread has read the previous draw
+        if (tid == 0) s_item = atomicAdd(ticket, 1u);
+        __syncthreads();
+        return s_item;
+    };
+    for (uint64_t i = ticket ? advance(0) : blockIdx.x; i < n_items; i = advance(i)) {
         const gs_pr_item it = items[i];
         const uint64_t base = ((uint64_t)it.row << kTileBits) + ((uint64_t)it.slice << kPrSliceBits);
         if (tid == 0) {
@@ -133,7 +142,7 @@ __global__ void __launch_bounds__(kPrThreads, 2)
         parity ^= 1;
         if (!__syncthreads_and(got)) {
             if (tid == 0) atomicExch(error, 1);
-            return;   // uniform; nothing else in flight
+            break;   // uniform; nothing else in flight
         }
         for (uint32_t ui = it.unit_beg + warp; ui < it.unit_end; ui += kPrWarps) sweep_unit(units[ui], rec, op, lane);
         __syncthreads();
@@ -146,6 +155,10 @@ __global__ void __launch_bounds__(kPrThreads, 2)
             }
         }
         __syncthreads();   // xs and ys are rewritten by the next item
+    }
+    if (ticket && tid == 0 && atomicAdd(ticket + 1, 1u) == gridDim.x - 1) {
+        atomicExch(ticket, 0u);   // every CTA has drawn its last ticket
+        atomicExch(ticket + 1, 0u);
     }
 }
 
@@ -288,8 +301,11 @@ gs_status pr_slice_sweep(gs_graph* g, cudaStream_t stream, const float* x, float
     // persistent (two CTAs per SM walking the items) or one CTA per item, so
     // that a higher-priority stream's CTAs find free SMs between items
     const uint32_t grid = (uint32_t)std::min<uint64_t>(L.n_items, item_ctas ? 0x7FFFFFFFull : gs_grid_size(ctx, 3));
+    // the persistent form runs on the context's stream only, which owns the
+    // PageRank ticket; one CTA per item needs none
+    unsigned int* ticket = item_ctas ? nullptr : ctx->d_ticket + 2;
     pr_slice_kernel<<<grid, kPrThreads, sizeof(PrSmem), stream>>>(L.d_items, L.n_items, L.d_units, L.d_rec, x, y,
-                                                                  g->directed, error);
+                                                                  g->directed, error, ticket);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
     return GS_OK;

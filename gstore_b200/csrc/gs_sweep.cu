@@ -23,7 +23,8 @@ constexpr int kThreads = 256;
 using namespace gsops;
 
 // Generic run sweep.  A CTA takes one run at a time (consecutive tiles of one
-// tile row inside a group), its warps take the run's units (tile slices of at
+// tile row inside a group; the next from `ticket` when one is given, else
+// every gridDim.x-th), its warps take the run's units (tile slices of at
 // most kUnitRecords records) and stream their records with 128-bit
 // evict-first loads.  When `seg` lists runs, only those are swept and their
 // units are read from a segment buffer (file record r at rec[r + delta]).
@@ -32,10 +33,19 @@ template <class Op>
 __global__ void __launch_bounds__(kThreads) sweep_runs(const gs_tile_run* __restrict__ runs, uint64_t n_runs,
                                                        const gs_unit* __restrict__ units,
                                                        const uint32_t* __restrict__ rec,
-                                                       const gs_seg_run* __restrict__ seg, Op op) {
+                                                       const gs_seg_run* __restrict__ seg, Op op,
+                                                       unsigned int* ticket) {
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr uint32_t kWarps = kThreads / 32;
-    for (uint64_t i = blockIdx.x; i < n_runs; i += gridDim.x) {
+    __shared__ unsigned long long s_run;
+    auto advance = [&](uint64_t i) -> uint64_t {
+        if (!ticket) return i + gridDim.x;
+        __syncthreads();   // every thread has read the previous draw
+        if (threadIdx.x == 0) s_run = atomicAdd(ticket, 1u);
+        __syncthreads();
+        return s_run;
+    };
+    for (uint64_t i = ticket ? advance(0) : blockIdx.x; i < n_runs; i = advance(i)) {
         uint32_t ub, ue;
         const uint32_t* base = rec;
         if (seg) {
@@ -48,6 +58,10 @@ __global__ void __launch_bounds__(kThreads) sweep_runs(const gs_tile_run* __rest
             ue = runs[i].unit_end;
         }
         for (uint32_t ui = ub + warp; ui < ue; ui += kWarps) sweep_unit(units[ui], base, op, lane);
+    }
+    if (ticket && threadIdx.x == 0 && atomicAdd(ticket + 1, 1u) == gridDim.x - 1) {
+        atomicExch(ticket, 0u);   // every CTA has drawn its last ticket
+        atomicExch(ticket + 1, 0u);
     }
 }
 
@@ -64,7 +78,8 @@ gs_status launch_sweep(gs_graph* g, const Op& op, int algo, uint64_t bytes, bool
     const uint32_t grid = (uint32_t)std::min<uint64_t>(n, gs_grid_size(ctx, 8));
     gs_timer_begin(ctx);
     sweep_runs<Op><<<grid, kThreads, 0, ctx->stream>>>(blocked ? g->d_runs_blk : g->d_runs, n,
-                                                        blocked ? g->d_units_blk : g->d_units, rec, seg, op);
+                                                        blocked ? g->d_units_blk : g->d_units, rec, seg, op,
+                                                        ctx->d_ticket);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
     gs_timer_end(ctx, algo, seg ? 0 : bytes);
