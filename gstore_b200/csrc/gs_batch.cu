@@ -351,37 +351,57 @@ struct BatchArgs {
     int nq;
     unsigned int* bar;
     int* err;
+    unsigned int* tickets;       // [4], zero at launch
 };
 
-__device__ __forceinline__ int find_query(const uint64_t* pre, int nq, uint64_t x) {
-    int q = 0;
-    while (q + 1 < nq && pre[q + 1] <= x) ++q;
-    return q;
+// Position of x among the prefix sums pre[0..n] (pre[0] = 0, x < pre[n]).
+__device__ __forceinline__ int find_query(const uint64_t* pre, int n, uint64_t x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
 
+// Both phases walk only the queries still running: after each decision step
+// every CTA rebuilds the same compact list (act_q) and its prefix sums of
+// runs and words.  Phase B draws runs from tickets[it & 3]; phase A of
+// iteration it zeroes tickets[(it + 2) & 3], last used two iterations before.
 __global__ void __launch_bounds__(kThreads) wk_batch_kernel(BatchArgs a) {
     __shared__ uint64_t run_pre[kMaxBatch + 1], word_pre[kMaxBatch + 1];
-    __shared__ unsigned long long done_mask;
+    __shared__ int act_q[kMaxBatch];
+    __shared__ int n_act;
+    __shared__ unsigned long long done_mask, s_run;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t gwarp = (uint64_t)blockIdx.x * kWarps + warp;
     const uint64_t nwarps = (uint64_t)gridDim.x * kWarps;
-    if (threadIdx.x == 0) {
+    auto rebuild = [&]() {   // thread 0
+        int n = 0;
         run_pre[0] = word_pre[0] = 0;
         for (int q = 0; q < a.nq; ++q) {
-            run_pre[q + 1] = run_pre[q] + a.q[q].R;
-            word_pre[q + 1] = word_pre[q] + a.q[q].words;
+            if (done_mask >> q & 1) continue;
+            act_q[n] = q;
+            run_pre[n + 1] = run_pre[n] + a.q[q].R;
+            word_pre[n + 1] = word_pre[n] + a.q[q].words;
+            ++n;
         }
+        n_act = n;
+    };
+    if (threadIdx.x == 0) {
         done_mask = 0;
+        rebuild();
     }
     __syncthreads();
     for (int it = 0;; ++it) {
         const int p = it & 1;
+        if (blockIdx.x == 0 && threadIdx.x == 0) a.tickets[(it + 2) & 3] = 0;
         // phase A: k-core round / WCC pointer jumping, per 32-vertex word
-        for (uint64_t x = gwarp; x < word_pre[a.nq]; x += nwarps) {
-            const int qi = find_query(word_pre, a.nq, x);
-            if (done_mask >> qi & 1) continue;
-            const BQuery& q = a.q[qi];
-            const uint64_t w = x - word_pre[qi];
+        for (uint64_t x = gwarp; x < word_pre[n_act]; x += nwarps) {
+            const int ai = find_query(word_pre, n_act, x);
+            const BQuery& q = a.q[act_q[ai]];
+            const uint64_t w = x - word_pre[ai];
             const uint32_t v = (uint32_t)(w * 32 + lane);
             if (lane == 0 && w < 1) {
                 q.cnt[(it + 2) & 3] = 0;
@@ -408,8 +428,8 @@ __global__ void __launch_bounds__(kThreads) wk_batch_kernel(BatchArgs a) {
         if (!grid_barrier(a.bar, a.err)) return;
         // decisions, identical in every CTA (counters are final here)
         if (threadIdx.x == 0) {
-            for (int qi = 0; qi < a.nq; ++qi) {
-                if (done_mask >> qi & 1) continue;
+            for (int ai = 0; ai < n_act; ++ai) {
+                const int qi = act_q[ai];
                 const BQuery& q = a.q[qi];
                 bool done;
                 if (q.algo == GS_ALGO_KCORE) done = __ldcg(q.cnt + (it & 3)) == 0;
@@ -419,15 +439,22 @@ __global__ void __launch_bounds__(kThreads) wk_batch_kernel(BatchArgs a) {
                     if (blockIdx.x == 0) *q.sweeps = it;
                 }
             }
+            rebuild();
         }
         __syncthreads();
-        if (done_mask == (a.nq == 64 ? ~0ull : ((1ull << a.nq) - 1))) return;
+        if (n_act == 0) return;
         // phase B: one sweep of every query still running
-        for (uint64_t x = blockIdx.x; x < run_pre[a.nq]; x += gridDim.x) {
-            const int qi = find_query(run_pre, a.nq, x);
-            if (done_mask >> qi & 1) continue;
-            const BQuery& q = a.q[qi];
-            const gs_tile_run run = q.runs[x - run_pre[qi]];
+        unsigned int* ticket = a.tickets + (it & 3);
+        auto draw = [&]() -> uint64_t {
+            __syncthreads();   // every thread has read the previous draw
+            if (threadIdx.x == 0) s_run = atomicAdd(ticket, 1u);
+            __syncthreads();
+            return s_run;
+        };
+        for (uint64_t x = draw(); x < run_pre[n_act]; x = draw()) {
+            const int ai = find_query(run_pre, n_act, x);
+            const BQuery& q = a.q[act_q[ai]];
+            const gs_tile_run run = q.runs[x - run_pre[ai]];
             if (q.algo == GS_ALGO_KCORE) {
                 const KcoreOpL2 op{q.deg, q.removed, q.act + p * q.nw};
                 for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps)
@@ -767,11 +794,12 @@ gs_status run_wk_queries(gs_batch* b, std::vector<int>& idx) {
         BQuery* d_q = (BQuery*)base;
         unsigned int* bar = (unsigned int*)((char*)base + qb);
         int* err = (int*)((char*)base + qb + 16);
+        unsigned int* tickets = (unsigned int*)((char*)base + qb + 32);   // 4, zeroed with bar and err
         int* sweeps = (int*)((char*)base + qb + 256);
         for (int k = 0; k < nq; ++k) dq[k].sweeps = sweeps + k;
         GS_CHECK_CUDA(ctx, cudaMemsetAsync((char*)base + qb, 0, 256 + nq * sizeof(int), ctx->stream));
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(d_q, dq.data(), nq * sizeof(BQuery), cudaMemcpyHostToDevice, ctx->stream));
-        BatchArgs a{d_q, nq, bar, err};
+        BatchArgs a{d_q, nq, bar, err, tickets};
         void* args[] = {&a};
         const int grid = coop_grid(ctx, (const void*)wk_batch_kernel);
         GS_CHECK_CUDA(ctx, cudaEventRecord(b->e0, ctx->stream));
