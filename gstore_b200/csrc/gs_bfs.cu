@@ -20,7 +20,7 @@
 // column end's from global memory through L1 — tiles written by the device
 // converter are sorted by column offset, so the 32 lookups of a warp fall
 // on a few neighbouring lines.  A discovered row end sets a bit in a
-// shared bitmap OR-ed into `next` once per run (its dirty words only); a
+// shared bitmap OR-ed into `next` once per run (its non-zero words); a
 // discovered column end goes straight to `next`.  No barrier between tiles.
 //
 // Reference rule kept: a tile is swept when its row window (or, half grid,
@@ -42,7 +42,6 @@ constexpr long long kWaitLimit = 1ll << 24;   // bounded mbarrier waits
 struct __align__(128) BfsSmem {
     uint32_t strow[kStWords];
     uint32_t nx[kNxWords];
-    uint32_t dirty[kNxWords / 32];
     unsigned long long bar;
     unsigned long long cur;   // the run drawn by thread 0
 };
@@ -94,7 +93,6 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (uint32_t w = tid; w < kNxWords; w += kThreads) m.nx[w] = 0;
-    if (tid < kNxWords / 32) m.dirty[tid] = 0;
     __syncthreads();
     uint32_t parity = 0;
     auto draw = [&]() -> uint64_t {
@@ -172,8 +170,7 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
                 }
                 if (c & 2u) {
                     const uint32_t w = v0 >> 5, bit = 1u << (v0 & 31);
-                    if (!(m.nx[w] & bit) && atomicOr(m.nx + w, bit) == 0)
-                        atomicOr(m.dirty + (w >> 5), 1u << (w & 31));
+                    if (!(m.nx[w] & bit)) atomicOr(m.nx + w, bit);
                 }
             };
             auto visit = [&](uint32_t r) {
@@ -216,20 +213,16 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
             if (__any_sync(0xFFFFFFFFu, hit) && lane == 0) a.act_next[col] = 1;   // read_part_next->set_bit_atomic(j)
         }
         __syncthreads();
-        // row side: OR the dirty words into next, clear them
+        // row side: OR the run's discovered words into next, clear them
         bool any_row = false;
-        if (tid < kNxWords / 32) {
-            uint32_t dw = m.dirty[tid];
-            if (dw) {
-                any_row = true;
-                m.dirty[tid] = 0;
-                uint32_t* dst = a.next + ((size_t)row << 11) + tid * 32;
-                uint32_t* src = m.nx + tid * 32;
-                while (dw) {
-                    const int k = __ffs(dw) - 1;
-                    atomicOr(dst + k, src[k]);
-                    src[k] = 0;
-                    dw &= dw - 1;
+        {
+            uint32_t* dst = a.next + ((size_t)row << 11);
+            for (uint32_t k = tid; k < kNxWords; k += kThreads) {
+                const uint32_t x = m.nx[k];
+                if (x) {
+                    any_row = true;
+                    atomicOr(dst + k, x);
+                    m.nx[k] = 0;
                 }
             }
         }
