@@ -168,10 +168,7 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
                     atomicOr(next_col + (v1 >> 5), 1u << (v1 & 31));
                     hit = true;
                 }
-                if (c & 2u) {
-                    const uint32_t w = v0 >> 5, bit = 1u << (v0 & 31);
-                    if (!(m.nx[w] & bit)) atomicOr(m.nx + w, bit);
-                }
+                if (c & 2u) atomicOr(m.nx + (v0 >> 5), 1u << (v0 & 31));
             };
             auto visit = [&](uint32_t r) {
                 const uint32_t c = classify(r);
