@@ -117,7 +117,6 @@ __global__ void __launch_bounds__(kThreads) msbfs_kernel(MsArgs<W> a) {
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
-    const MsOp<W> op{a.fv, a.next, a.directed};
     for (int level = 1; level < 255; ++level) {
         const uint8_t* act = a.act + (level & 1) * a.nw;
         uint8_t* act_next = a.act + ((level + 1) & 1) * a.nw;
@@ -141,7 +140,7 @@ __global__ void __launch_bounds__(kThreads) msbfs_kernel(MsArgs<W> a) {
             for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps) {
                 const gs_unit d = a.units[ui];
                 if (!ar && (a.directed || !__ldcg(act + (d.rc & 0xFFFFu)))) continue;
-                sweep_unit(d, a.rec, op, lane);
+                ms_sweep_unit<W>(d, a.rec, a.fv, a.next, a.directed, lane);
             }
         }
         if (!grid_barrier(a.bar, a.err)) return;

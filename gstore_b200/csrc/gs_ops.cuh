@@ -232,31 +232,52 @@ __device__ __forceinline__ W warp_or(W x) {
 __device__ __forceinline__ int ffs_w(uint32_t x) { return __ffs(x); }
 __device__ __forceinline__ int ffs_w(unsigned long long x) { return __ffsll((long long)x); }
 
+// Multi-source sweep of one unit: per record (v0, v1), for all queries of
+// the W-bit words at once, next[v1] |= f[v0] & ~vis[v1] and (half grid)
+// next[v0] |= f[v1] & ~vis[v0] (bfs.cpp:158-172).  The {frontier, visited}
+// pairs of a lane's four records are loaded before any of them is acted on,
+// so eight loads are in flight at once.
 template <class W>
-struct MsOp {
-    FvPair<W>* fv;
-    W* next;
-    int directed;
-    struct Item {
-        uint32_t rb, cb;
-    };
-    __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
-        c.rb = row << 16;
-        c.cb = col << 16;
-        return true;
-    }
-    __device__ void record(uint32_t r, Item& c) const {
-        const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
-        const FvPair<W> sa = load_fv(fv + a), sb = load_fv(fv + b);
+__device__ __forceinline__ void ms_sweep_unit(const gs_unit d, const uint32_t* __restrict__ base, FvPair<W>* fv,
+                                              W* next, int directed, uint32_t lane) {
+    const uint32_t rb = (d.rc >> 16) << 16, cb = (d.rc & 0xFFFFu) << 16;
+    auto act = [&](uint32_t a, uint32_t b, const FvPair<W>& sa, const FvPair<W>& sb) {
         const W nb = sa.f & ~sb.vis;
         if (nb) atomicOr(next + b, nb);
         if (!directed) {            // the half grid stores each edge once
             const W na = sb.f & ~sa.vis;
             if (na) atomicOr(next + a, na);
         }
+    };
+    auto one = [&](uint32_t r) {
+        const uint32_t a = rb + (r & 0xFFFFu), b = cb + (r >> 16);
+        act(a, b, load_fv(fv + a), load_fv(fv + b));
+    };
+    const uint64_t b = d.rec_beg, e = d.rec_beg + d.n;
+    uint64_t ab = (b + 3) & ~3ull;
+    if (ab > e) ab = e;
+    uint64_t ae = e & ~3ull;
+    if (ae < ab) ae = ab;
+    if (b + lane < ab) one(__ldcs(base + b + lane));
+    if (ae + lane < e) one(__ldcs(base + ae + lane));
+    const uint4* r4 = reinterpret_cast<const uint4*>(base + ab);
+    const uint32_t n4 = (uint32_t)((ae - ab) >> 2);
+    for (uint32_t k = lane; k < n4; k += 32) {
+        const uint4 q = load_stream(r4 + k);
+        const uint32_t a0 = rb + (q.x & 0xFFFFu), b0 = cb + (q.x >> 16);
+        const uint32_t a1 = rb + (q.y & 0xFFFFu), b1 = cb + (q.y >> 16);
+        const uint32_t a2 = rb + (q.z & 0xFFFFu), b2 = cb + (q.z >> 16);
+        const uint32_t a3 = rb + (q.w & 0xFFFFu), b3 = cb + (q.w >> 16);
+        const FvPair<W> sa0 = load_fv(fv + a0), sb0 = load_fv(fv + b0);
+        const FvPair<W> sa1 = load_fv(fv + a1), sb1 = load_fv(fv + b1);
+        const FvPair<W> sa2 = load_fv(fv + a2), sb2 = load_fv(fv + b2);
+        const FvPair<W> sa3 = load_fv(fv + a3), sb3 = load_fv(fv + b3);
+        act(a0, b0, sa0, sb0);
+        act(a1, b1, sa1, sb1);
+        act(a2, b2, sa2, sb2);
+        act(a3, b3, sa3, sb3);
     }
-    __device__ void end(uint32_t, uint32_t, Item&) const {}
-};
+}
 
 // KcoreOp for a persistent kernel: the removed bits and window flags change
 // between phases, so they are read through L2 (never the non-coherent path).

@@ -116,11 +116,10 @@ __global__ void __launch_bounds__(kThreads) serve_sweep_kernel(const Table* __re
         const gs_tile_run run = jb.runs[x - jb.run_beg];
         const uint32_t row = jb.units[run.unit_beg].rc >> 16;
         const bool ar = jb.act_cur[row] != 0;
-        const MsOp<unsigned long long> op{jb.fv, jb.next, jb.directed};
         for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps) {
             const gs_unit d = jb.units[ui];
             if (!ar && (jb.directed || !jb.act_cur[d.rc & 0xFFFFu])) continue;
-            sweep_unit(d, jb.rec, op, lane);
+            ms_sweep_unit<unsigned long long>(d, jb.rec, jb.fv, jb.next, jb.directed, lane);
         }
     }
 }
