@@ -61,6 +61,12 @@ void gs_pool_put(gs_ctx* ctx, void* ptr, size_t bytes) {
     ctx->pool_bytes += bytes;
 }
 
+gs_status gs_state_alloc(gs_state* s, void** ptr, size_t bytes) {
+    GS_TRY(gs_pool_get(s->g->ctx, bytes, ptr));
+    s->allocs.emplace_back(*ptr, bytes);
+    return GS_OK;
+}
+
 void gs_pool_clear(gs_ctx* ctx) {
     for (auto& kv : ctx->pool_free) gs_dev_free(kv.second);
     ctx->pool_free.clear();
@@ -701,26 +707,9 @@ gs_status gs_state_reset(gs_state* s, int64_t arg) {
 
 gs_status gs_state_free(gs_state* s) {
     if (!s) return GS_OK;
+    // the state's kernels are done before its buffers go back to the pool
     cudaStreamSynchronize(s->g->ctx->stream);
-    gs_dev_free(s->d_depth);
-    gs_dev_free(s->d_front);
-    gs_dev_free(s->d_visited);
-    gs_dev_free(s->d_act);
-    gs_dev_free(s->d_act_next);
-    gs_dev_free(s->d_x);
-    gs_dev_free(s->d_y);
-    gs_dev_free(s->d_r);
-    gs_dev_free(s->d_parent);
-    gs_dev_free(s->d_touched);
-    gs_dev_free(s->d_deg);
-    gs_dev_free(s->d_kactive);
-    gs_dev_free(s->d_lab);
-    gs_dev_free(s->d_error);
-    gs_dev_free(s->d_ticket);
-    gs_dev_free(s->d_fv);
-    gs_dev_free(s->d_uflags);
-    gs_dev_free(s->d_sel);
-    gs_dev_free(s->d_cub);
+    for (auto& pb : s->allocs) gs_pool_put(s->g->ctx, pb.first, pb.second);
     delete s;
     return GS_OK;
 }
@@ -831,44 +820,31 @@ gs_status gs_download(gs_state* s, int what, void* host_dst, uint64_t bytes) {
     gs_ctx* ctx = g->ctx;
     const void* src = nullptr;
     uint64_t need = 0;
-    uint32_t* tmp = nullptr;
+    if ((s->algo == GS_ALGO_BFS2 || s->algo == GS_ALGO_WCC) && !s->d_out)
+        GS_TRY(gs_state_alloc(s, (void**)&s->d_out, g->N * 4));
     switch (s->algo) {
         case GS_ALGO_BFS: src = s->d_depth; need = g->V; break;
         case GS_ALGO_PAGERANK: src = what == 1 ? s->d_x : s->d_r; need = g->V * 4; break;
         case GS_ALGO_KCORE: src = s->d_deg; need = g->V * 4; break;
         case GS_ALGO_TRAVERSE: src = s->d_lab; need = g->V * 4; break;
         case GS_ALGO_BFS2: {
-            GS_TRY(gs_dev_alloc(ctx, (void**)&tmp, g->N));
             uint64_t cnt;
-            gs_status st = lab_result(s, (uint8_t*)tmp, &cnt);
-            if (st != GS_OK) {
-                gs_dev_free(tmp);
-                return st;
-            }
-            src = tmp;
+            GS_TRY(lab_result(s, (uint8_t*)s->d_out, &cnt));
+            src = s->d_out;
             need = g->V;
             break;
         }
         case GS_ALGO_WCC: {
-            GS_TRY(gs_dev_alloc(ctx, (void**)&tmp, g->N * 4));
             uint64_t cnt;
-            gs_status st = gs_wcc_labels(s, tmp, &cnt);
-            if (st != GS_OK) {
-                gs_dev_free(tmp);
-                return st;
-            }
-            src = tmp;
+            GS_TRY(gs_wcc_labels(s, s->d_out, &cnt));
+            src = s->d_out;
             need = g->V * 4;
             break;
         }
     }
-    if (bytes < need) {
-        gs_dev_free(tmp);
-        return gs_fail(ctx, GS_ERR_ARG, "destination too small: need " + std::to_string(need));
-    }
+    if (bytes < need) return gs_fail(ctx, GS_ERR_ARG, "destination too small: need " + std::to_string(need));
     cudaError_t e = cudaMemcpyAsync(host_dst, src, need, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    gs_dev_free(tmp);
     if (e != cudaSuccess) return gs_cuda_fail(ctx, e, "download");
     return GS_OK;
 }
@@ -881,13 +857,9 @@ gs_status gs_result_count(gs_state* s, uint64_t* count) {
             return gs_count_reached(s, count, &e);
         }
         case GS_ALGO_KCORE: return gs_count_kcore(s, count);
-        case GS_ALGO_WCC: {
-            uint32_t* tmp = nullptr;
-            GS_TRY(gs_dev_alloc(s->g->ctx, (void**)&tmp, s->g->N * 4));
-            gs_status st = gs_wcc_labels(s, tmp, count);
-            gs_dev_free(tmp);
-            return st;
-        }
+        case GS_ALGO_WCC:
+            if (!s->d_out) GS_TRY(gs_state_alloc(s, (void**)&s->d_out, s->g->N * 4));
+            return gs_wcc_labels(s, s->d_out, count);
         case GS_ALGO_PAGERANK: *count = (uint64_t)s->step; return GS_OK;
         case GS_ALGO_BFS2:
         case GS_ALGO_TRAVERSE: return lab_result(s, nullptr, count);

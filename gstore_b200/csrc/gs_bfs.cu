@@ -298,13 +298,13 @@ gs_status bfs_init(gs_state* s) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
     const uint64_t words = g->N / 32;
-    if (!s->d_depth) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_depth, g->N));
-    if (!s->d_front) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_front, words * 8));    // 2-bit state
-    if (!s->d_visited) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_visited, words * 4)); // next bitmap
-    if (!s->d_act) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_act, g->nw));
-    if (!s->d_act_next) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_act_next, g->nw));
-    if (!s->d_error) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_error, sizeof(uint64_t)));
-    if (!s->d_ticket) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_ticket, 2 * sizeof(uint32_t)));
+    if (!s->d_depth) GS_TRY(gs_state_alloc(s, (void**)&s->d_depth, g->N));
+    if (!s->d_front) GS_TRY(gs_state_alloc(s, (void**)&s->d_front, words * 8));    // 2-bit state
+    if (!s->d_visited) GS_TRY(gs_state_alloc(s, (void**)&s->d_visited, words * 4)); // next bitmap
+    if (!s->d_act) GS_TRY(gs_state_alloc(s, (void**)&s->d_act, g->nw));
+    if (!s->d_act_next) GS_TRY(gs_state_alloc(s, (void**)&s->d_act_next, g->nw));
+    if (!s->d_error) GS_TRY(gs_state_alloc(s, (void**)&s->d_error, sizeof(uint64_t)));
+    if (!s->d_ticket) GS_TRY(gs_state_alloc(s, (void**)&s->d_ticket, 2 * sizeof(uint32_t)));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_ticket, 0, 2 * sizeof(uint32_t), ctx->stream));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_depth, 0, g->N, ctx->stream));   // INFTY = 0
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_front, 0, words * 8, ctx->stream));

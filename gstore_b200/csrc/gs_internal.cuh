@@ -187,11 +187,6 @@ struct gs_state {
     uint32_t* d_visited = nullptr;   // N/32 words: discovered-this-sweep bitmap
     uint64_t* d_error = nullptr;     // bounded-wait failure flag
     uint32_t* d_ticket = nullptr;    // BFS sweep: run ticket, finished CTAs
-    uint2* d_fv = nullptr;           // N/32 {frontier, visited} word pairs
-    uint8_t* d_uflags = nullptr;     // 2 x U: per-unit activity flags, selection flags
-    uint32_t* d_sel = nullptr;       // U + 1: selected unit indices, then their count
-    void* d_cub = nullptr;           // compaction scratch
-    size_t cub_bytes = 0;
     uint8_t* d_act = nullptr;        // nw window flags (current)
     uint8_t* d_act_next = nullptr;   // nw
     std::vector<uint64_t> level_counts;
@@ -209,6 +204,10 @@ struct gs_state {
     // bfs2 / traverse
     uint32_t* d_lab = nullptr;       // N: depth (bfs2) or colour (traverse)
     int64_t last_count = 0;
+    uint32_t* d_out = nullptr;       // N x 4 B: staging of derived results (WCC labels, bfs2 depth)
+    // every device buffer above, taken from the context's pool (gs_state_alloc)
+    // and returned to it by gs_state_free
+    std::vector<std::pair<void*, size_t>> allocs;
 };
 
 // ---------------------------------------------------------------- errors --
@@ -246,6 +245,8 @@ void gs_dev_free(void* ptr);
 // Context pool: a cached block of exactly `bytes` (rounded to 256), or a new
 // one; gs_pool_put returns it (blocks beyond kPoolMaxBytes are freed).
 gs_status gs_pool_get(gs_ctx* ctx, size_t bytes, void** out);
+// A buffer of a query state from the context's pool, recorded in s->allocs.
+gs_status gs_state_alloc(gs_state* s, void** ptr, size_t bytes);
 void gs_pool_put(gs_ctx* ctx, void* ptr, size_t bytes);
 void gs_pool_clear(gs_ctx* ctx);
 

@@ -315,7 +315,7 @@ gs_status pr_slice_launch(gs_state* s) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
     if (!s->d_error) {
-        GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_error, sizeof(uint64_t)));
+        GS_TRY(gs_state_alloc(s, (void**)&s->d_error, sizeof(uint64_t)));
         GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_error, 0, sizeof(uint64_t), ctx->stream));
     }
     gs_timer_begin(ctx);

@@ -411,9 +411,9 @@ gs_status gs_swept_records(gs_state* s, const uint8_t* act, uint64_t* swept) {
 gs_status pr_init(gs_state* s) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
-    if (!s->d_x) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_x, g->N * 4));
-    if (!s->d_y) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_y, g->N * 4));
-    if (!s->d_r) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_r, g->N * 4));
+    if (!s->d_x) GS_TRY(gs_state_alloc(s, (void**)&s->d_x, g->N * 4));
+    if (!s->d_y) GS_TRY(gs_state_alloc(s, (void**)&s->d_y, g->N * 4));
+    if (!s->d_r) GS_TRY(gs_state_alloc(s, (void**)&s->d_r, g->N * 4));
     pr_init_kernel<<<blocks_for(g->N, ctx), kThreads, 0, ctx->stream>>>(s->d_x, s->d_y, g->N, g->V);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
@@ -464,8 +464,8 @@ gs_status pr_finalize(gs_state* s, int64_t* frontier, int* done) {
 gs_status wcc_init(gs_state* s) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
-    if (!s->d_parent) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_parent, g->N * 4));
-    if (!s->d_touched) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_touched, g->N));
+    if (!s->d_parent) GS_TRY(gs_state_alloc(s, (void**)&s->d_parent, g->N * 4));
+    if (!s->d_touched) GS_TRY(gs_state_alloc(s, (void**)&s->d_touched, g->N));
     iota_kernel<<<blocks_for(g->N, ctx), kThreads, 0, ctx->stream>>>(s->d_parent, g->N);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
@@ -510,9 +510,9 @@ gs_status gs_wcc_labels(gs_state* s, uint32_t* d_out, uint64_t* count) {
 gs_status kcore_init(gs_state* s) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
-    if (!s->d_deg) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_deg, g->N * 4));
-    if (!s->d_kactive) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_kactive, g->N / 8));
-    if (!s->d_act) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_act, g->nw));
+    if (!s->d_deg) GS_TRY(gs_state_alloc(s, (void**)&s->d_deg, g->N * 4));
+    if (!s->d_kactive) GS_TRY(gs_state_alloc(s, (void**)&s->d_kactive, g->N / 8));
+    if (!s->d_act) GS_TRY(gs_state_alloc(s, (void**)&s->d_act, g->nw));
     GS_CHECK_CUDA(ctx, cudaMemcpyAsync(s->d_deg, g->d_degree, g->N * 4, cudaMemcpyDeviceToDevice, ctx->stream));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_kactive, 0, g->N / 8, ctx->stream));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_act, 0, g->nw, ctx->stream));
@@ -557,10 +557,10 @@ gs_status gs_count_kcore(gs_state* s, uint64_t* members) {
 gs_status lab_init(gs_state* s) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
-    if (!s->d_lab) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_lab, g->N * 4));
-    if (!s->d_act) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_act, g->nw));
-    if (!s->d_act_next) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_act_next, g->nw));
-    if (!s->d_error) GS_TRY(gs_dev_alloc(ctx, (void**)&s->d_error, sizeof(uint64_t)));
+    if (!s->d_lab) GS_TRY(gs_state_alloc(s, (void**)&s->d_lab, g->N * 4));
+    if (!s->d_act) GS_TRY(gs_state_alloc(s, (void**)&s->d_act, g->nw));
+    if (!s->d_act_next) GS_TRY(gs_state_alloc(s, (void**)&s->d_act_next, g->nw));
+    if (!s->d_error) GS_TRY(gs_state_alloc(s, (void**)&s->d_error, sizeof(uint64_t)));
     const uint64_t v = (uint64_t)s->arg;
     const bool bfs2 = s->algo == GS_ALGO_BFS2;
     // bfs2: every vertex unreached, root depth 1, every window active

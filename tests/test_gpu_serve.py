@@ -195,3 +195,39 @@ def test_serve_failure_is_per_request(gs, gpu_ctx_factory):
         with pytest.raises(gs.GStoreError, match="GS_ERR_ARG"):
             srv.submit(gid, "bfs", pg.V)
     pg.free()
+
+
+def test_serve_completion_queue_and_side_streams(gs, pool, gpu_ctx_factory, oracle_lib):
+    """A client that takes results as they land (gs_serve_completed) gets
+    every request exactly once, with the plain entry point's results, on one
+    side stream; the side-stream count can only change while no WCC /
+    k-core / PageRank request runs."""
+    ctx = gpu_ctx_factory(False)
+    reqs = _mix(pool, 30, 11) + [(3, "kcore", 6), (2, "wcc", 0), (1, "pagerank", 4)]
+    with gs.Server(ctx) as srv:
+        gids = [srv.add_graph(g) for g in pool]
+        srv.set_side_streams(1)
+        with pytest.raises(gs.GStoreError, match="GS_ERR_ARG"):
+            srv.set_side_streams(0)
+        ids = {}
+        for i, (gi, algo, arg) in enumerate(reqs):
+            ids[srv.submit(gids[gi], algo, arg)] = i
+        with pytest.raises(gs.GStoreError, match="GS_ERR_STATE"):
+            srv.step()
+            srv.set_side_streams(2)
+        seen = []
+        while True:
+            na, nq = srv.step()
+            for rid in srv.completed():
+                seen.append(rid)
+                gi, algo, arg = reqs[ids[rid]]
+                _check(algo, srv.result(rid)[0], _plain(pool[gi], algo, arg))
+            if na == 0 and nq == 0:
+                break
+        for rid in srv.completed():
+            seen.append(rid)
+            gi, algo, arg = reqs[ids[rid]]
+            _check(algo, srv.result(rid)[0], _plain(pool[gi], algo, arg))
+        assert sorted(seen) == sorted(ids)
+        assert srv.completed() == []
+        srv.set_side_streams(8)                  # nothing runs now
