@@ -879,10 +879,19 @@ gs_status gs_bfs_stats(gs_state* s, uint64_t* edges_in_component, uint64_t* swep
     if (level_counts)
         for (int l = 0; l < nl && l < max_levels; ++l) level_counts[l] = s->level_counts[l];
     if (swept_records) {
-        for (int l = 0; l < nl && l < max_levels; ++l) {
-            uint64_t sw = 0;
-            GS_TRY(gs_swept_records(s, s->level_act[l].data(), &sw));
-            swept_records[l] = sw;
+        const int nh = std::min(std::min(nl, max_levels), std::min(s->n_act_hist, 256));
+        if (nh > 0) {
+            gs_ctx* ctx = s->g->ctx;
+            const size_t nw = s->g->nw;
+            std::vector<uint8_t> hist((size_t)nh * nw);
+            GS_CHECK_CUDA(ctx, cudaMemcpyAsync(hist.data(), s->d_act_hist, hist.size(), cudaMemcpyDeviceToHost,
+                                               ctx->stream));
+            GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            for (int l = 0; l < nh; ++l) {
+                uint64_t sw = 0;
+                GS_TRY(gs_swept_records(s, hist.data() + (size_t)l * nw, &sw));
+                swept_records[l] = sw;
+            }
         }
     }
     return GS_OK;

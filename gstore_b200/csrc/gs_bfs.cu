@@ -317,17 +317,20 @@ gs_status bfs_init(gs_state* s) {
     ctx->launches++;
     s->level = 1;
     s->level_counts.clear();
-    s->level_act.clear();
+    s->n_act_hist = 0;
     return GS_OK;
 }
 
 gs_status bfs_sweep_begin(gs_state* s) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
-    // Window flags of this sweep, kept for the swept-record statistics.
-    s->level_act.emplace_back(g->nw);
-    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(s->level_act.back().data(), s->d_act, g->nw, cudaMemcpyDeviceToHost,
-                                       ctx->stream));
+    // Window flags of this sweep, kept on the device for the swept-record
+    // statistics (read back only when asked for: no host round trip here).
+    if (!s->d_act_hist) GS_TRY(gs_state_alloc(s, (void**)&s->d_act_hist, (size_t)g->nw * 256));
+    if (s->n_act_hist < 256)
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(s->d_act_hist + (size_t)s->n_act_hist * g->nw, s->d_act, g->nw,
+                                           cudaMemcpyDeviceToDevice, ctx->stream));
+    s->n_act_hist += 1;
     static bool attr_set[64] = {false};
     if (!attr_set[ctx->device & 63]) {
         GS_CHECK_CUDA(ctx, cudaFuncSetAttribute(bfs_run_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

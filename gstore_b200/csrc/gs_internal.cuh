@@ -190,7 +190,8 @@ struct gs_state {
     uint8_t* d_act = nullptr;        // nw window flags (current)
     uint8_t* d_act_next = nullptr;   // nw
     std::vector<uint64_t> level_counts;
-    std::vector<std::vector<uint8_t>> level_act;  // per level window flags (host)
+    uint8_t* d_act_hist = nullptr;   // 256 x nw: each level's window flags (swept-record statistics)
+    int n_act_hist = 0;              // levels recorded in d_act_hist
     // PageRank
     float* d_x = nullptr;            // N
     float* d_y = nullptr;            // N
