@@ -722,15 +722,26 @@ def main():
         graph.free()
         torch.cuda.empty_cache()
 
+        parts = {"upload": [], "bfs": [], "download": [], "free": []}
+
         def e2e_step(root):
+            t_a = time.perf_counter()
             g2 = ctx.upload(pin_start.numpy().view(np.uint64), pin_grid.numpy().view(np.uint32),
                             pin_deg.numpy(), V)
+            t_b = time.perf_counter()
             with g2.state("bfs", root) as s:
                 s.run()
+                t_c = time.perf_counter()
                 s.download_into(depth_out.numpy())
+                t_d = time.perf_counter()
             g2.free()
+            t_e = time.perf_counter()
+            for k, a, b in (("upload", t_a, t_b), ("bfs", t_b, t_c), ("download", t_c, t_d), ("free", t_d, t_e)):
+                parts[k].append((b - a) * 1e3)
 
         e2e_step(timed_roots[0])
+        for v in parts.values():
+            v.clear()
         dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -741,7 +752,8 @@ def main():
         line["e2e"] = {"value": e_total / e2e_s / 1e9, "unit": "GTEPS",
                        "h2d_bytes_per_step": int(pin_grid.numel() * 4 + pin_start.numel() * 8 + pin_deg.numel() * 4),
                        "d2h_bytes_per_step": V,
-                       "what": "per step: gs_upload_graph from pinned host tile arrays, BFS, depth download"}
+                       "what": "per step: gs_upload_graph from pinned host tile arrays, BFS, depth download",
+                       "ms_per_step_median": {k: float(np.median(v)) for k, v in parts.items()}}
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
     # ------------------------------------- batched / served / streamed forms

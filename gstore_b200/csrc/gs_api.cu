@@ -289,6 +289,16 @@ static gs_status build_blocked_order(gs_graph* g, uint32_t block, uint64_t* R_ou
     return GS_OK;
 }
 
+// The L2-blocked orders of a resident graph, built at their first use (the
+// BFS sweep and a plain upload do not need them).
+gs_status gs_ensure_blocked(gs_graph* g) {
+    if (g->stream || g->blocked_built) return GS_OK;
+    GS_TRY(build_blocked_order(g, kBlockWindows, &g->R_blk, &g->d_runs_blk, &g->d_units_blk));
+    GS_TRY(build_blocked_order(g, kBlockWindowsSmall, &g->R_blk2, &g->d_runs_blk2, &g->d_units_blk2));
+    g->blocked_built = true;
+    return GS_OK;
+}
+
 // Builds the non-empty tile table and the work items from the host .start
 // array, walking the stored tiles in file order (the loops of grid::*_mmap,
 // gstore.cpp:2520-2559), and uploads them.
@@ -363,10 +373,6 @@ static gs_status build_tables(gs_graph* g) {
     g->I = n_items;
     g->R = runs.size();
     g->U = units.size();
-    if (!g->stream) {
-        GS_TRY(build_blocked_order(g, kBlockWindows, &g->R_blk, &g->d_runs_blk, &g->d_units_blk));
-        GS_TRY(build_blocked_order(g, kBlockWindowsSmall, &g->R_blk2, &g->d_runs_blk2, &g->d_units_blk2));
-    }
     GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_units, std::max<size_t>(1, units.size()) * sizeof(gs_unit)));
     if (!units.empty())
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_units, units.data(), units.size() * sizeof(gs_unit),

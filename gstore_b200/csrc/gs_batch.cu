@@ -724,6 +724,7 @@ gs_status run_bfs_queries(gs_batch* b, std::vector<int>& idx) {
             if (b->q[i].g == g) mine.push_back(i);
         const int cand = pick_candidate(tune_of(g));
         const int bits = cand >= kOrders ? 64 : 32;
+        GS_TRY(gs_ensure_blocked(g));
         const int order = g->d_runs_blk ? cand % kOrders : 0;
         if (order == 3 && !g->pr.built) GS_TRY(pr_layout_build(g));
         for (size_t s = 0; s < mine.size(); s += bits) {
@@ -770,6 +771,7 @@ gs_status run_wk_queries(gs_batch* b, std::vector<int>& idx) {
             }
             BQuery d;
             std::memset(&d, 0, sizeof(d));
+            GS_TRY(gs_ensure_blocked(g));
             d.runs = g->d_runs_blk ? g->d_runs_blk : g->d_runs;
             d.units = g->d_runs_blk ? g->d_units_blk : g->d_units;
             d.rec = g->d_rec;

@@ -151,6 +151,7 @@ struct gs_graph {
     gs_unit* d_units = nullptr;
     gs_tile_run* d_runs_lpt = nullptr; // BFS sweep: runs (maybe cut into pieces), longest first (resident)
     uint64_t R_lpt = 0;
+    bool blocked_built = false;       // the two blocked orders below exist (gs_ensure_blocked)
     uint64_t R_blk = 0;               // runs of the L2-blocked order (resident graphs)
     gs_tile_run* d_runs_blk = nullptr;
     gs_unit* d_units_blk = nullptr;
@@ -248,6 +249,8 @@ void gs_dev_free(void* ptr);
 gs_status gs_pool_get(gs_ctx* ctx, size_t bytes, void** out);
 // A buffer of a query state from the context's pool, recorded in s->allocs.
 gs_status gs_state_alloc(gs_state* s, void** ptr, size_t bytes);
+// Builds the L2-blocked run orders of a resident graph on first use.
+gs_status gs_ensure_blocked(gs_graph* g);
 void gs_pool_put(gs_ctx* ctx, void* ptr, size_t bytes);
 void gs_pool_clear(gs_ctx* ctx);
 

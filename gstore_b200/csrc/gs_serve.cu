@@ -759,8 +759,10 @@ gs_status gs_serve_add_graph(gs_server* s, gs_graph* g, int* graph_id) {
     if (!s || !g || !graph_id) return GS_ERR_ARG;
     if (g->ctx != s->ctx) return gs_fail(s->ctx, GS_ERR_ARG, "graph belongs to another context");
     if (g->stream) return gs_fail(s->ctx, GS_ERR_UNSUPPORTED, "served graphs must be resident in HBM");
-    // the PageRank layout is built here, at set-up, not under a request
+    // the PageRank layout and the blocked orders are built here, at set-up,
+    // not under a request
     if (!g->pr.built && g->E) GS_TRY(pr_layout_build(g));
+    GS_TRY(gs_ensure_blocked(g));
     SrvGraph sg;
     sg.g = g;
     for (int q = 0; q < kSlots; ++q) sg.slot_req[q] = -1;

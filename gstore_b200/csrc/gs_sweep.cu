@@ -71,6 +71,7 @@ template <class Op>
 gs_status launch_sweep(gs_graph* g, const Op& op, int algo, uint64_t bytes, bool blocked = false) {
     gs_ctx* ctx = g->ctx;
     const gs_seg_run* seg = g->seg.list;
+    if (blocked && !seg) GS_TRY(gs_ensure_blocked(g));
     blocked = blocked && !seg && g->d_runs_blk;
     const uint64_t n = seg ? g->seg.n : (blocked ? g->R_blk : g->R);
     const uint32_t* rec = seg ? g->seg.buf : g->d_rec;
