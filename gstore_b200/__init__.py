@@ -43,7 +43,7 @@ ABI_SYMBOLS = [
     "gs_graph_degree", "gs_state_create", "gs_state_free", "gs_state_reset", "gs_sweep", "gs_finalize", "gs_run",
     "gs_download", "gs_result_count", "gs_bfs_stats", "gs_pagerank_compat",
     "gs_kron_generate_device", "gs_kron_generate", "gs_convert", "gs_graph_download",
-    "gs_bfs_noalloc", "gs_upload_graph_streamed", "gs_stream_stats",
+    "gs_bfs_noalloc", "gs_upload_graph_streamed", "gs_upload_graph_file", "gs_stream_stats",
     "gs_batch_create", "gs_batch_add", "gs_batch_run", "gs_batch_download", "gs_batch_result_count",
     "gs_batch_bfs_levels", "gs_batch_stats", "gs_batch_free",
     "gs_serve_create", "gs_serve_add_graph", "gs_serve_submit", "gs_serve_step", "gs_serve_poll",
@@ -101,6 +101,7 @@ def lib():
             "gs_graph_download": [vp, vp, vp, vp],
             "gs_bfs_noalloc": [vp, u64, vp, C.POINTER(C.c_int64)],
             "gs_upload_graph_streamed": [vp, vp, u64, vp, u64, vp, u64, u64, pvp],
+            "gs_upload_graph_file": [vp, vp, u64, C.c_char_p, u64, vp, u64, u64, pvp],
             "gs_stream_stats": [vp, pu64, pu64, pu64, pu64],
             "gs_batch_create": [vp, pvp],
             "gs_batch_add": [vp, vp, i32, i64, C.POINTER(C.c_int)],
@@ -255,6 +256,19 @@ class Context:
         self._check(lib().gs_upload_graph_streamed(self._h, _ptr(start), start.size, _ptr(grid), grid.size,
                                                    _ptr(degree), V, segment_bytes, C.byref(h)))
         return Graph(self, h, keep=grid)
+
+    def upload_file(self, start, grid_path, n_edges: int, degree, V: int, segment_bytes: int) -> "Graph":
+        """A graph whose records stay in the .grid file at grid_path and are
+        read into two pinned staging buffers, then copied through two HBM
+        segments of segment_bytes each, on every sweep."""
+        start = np.ascontiguousarray(start, np.uint64)
+        if degree is not None:
+            degree = np.ascontiguousarray(degree, np.int32)
+            assert degree.size >= V, "degree array shorter than V"
+        h = C.c_void_p()
+        self._check(lib().gs_upload_graph_file(self._h, _ptr(start), start.size, str(grid_path).encode(), n_edges,
+                                               _ptr(degree), V, segment_bytes, C.byref(h)))
+        return Graph(self, h)
 
     def upload_device(self, d_start: int, n_start: int, d_grid: int, n_edges: int, d_degree: int | None,
                       V: int) -> "Graph":

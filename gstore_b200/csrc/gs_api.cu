@@ -579,6 +579,27 @@ gs_status gs_upload_graph_streamed(gs_ctx* ctx, const uint64_t* start, uint64_t 
     return GS_OK;
 }
 
+gs_status gs_upload_graph_file(gs_ctx* ctx, const uint64_t* start, uint64_t n_start, const char* grid_path,
+                               uint64_t n_edges, const int32_t* degree, uint64_t V, uint64_t segment_bytes,
+                               gs_graph** out) {
+    if (!ctx || !start || !grid_path || !out) return gs_fail(ctx, GS_ERR_ARG, "null argument");
+    *out = nullptr;
+    gs_graph* g = nullptr;
+    GS_TRY(new_graph(ctx, V, &g));
+    g->h_start.assign(start, start + std::min<uint64_t>(n_start, g->T_all + 1));
+    gs_status st = check_start(g, n_start, n_edges);
+    g->E = n_edges;
+    if (st == GS_OK) st = gs_stream_open_file(g, grid_path, segment_bytes);
+    if (st == GS_OK) st = finish_upload(g, degree, false);
+    if (st != GS_OK) {
+        free_graph_arrays(g);
+        delete g;
+        return st;
+    }
+    *out = g;
+    return GS_OK;
+}
+
 gs_status gs_upload_graph_device(gs_ctx* ctx, const uint64_t* d_start, uint64_t n_start,
                                  const uint32_t* d_grid, uint64_t n_edges,
                                  const int32_t* d_degree, uint64_t V, gs_graph** out) {
@@ -645,7 +666,9 @@ gs_status gs_graph_download(const gs_graph* g, uint64_t* host_start, uint32_t* h
     gs_ctx* ctx = g->ctx;
     if (host_start) std::memcpy(host_start, g->h_start.data(), g->h_start.size() * 8);
     if (host_grid && g->E) {
-        if (g->stream) std::memcpy(host_grid, gs_stream_records(g), g->E * 4);
+        if (g->stream) {
+            if (!gs_stream_read_records(g, host_grid)) return gs_fail(ctx, GS_ERR_FORMAT, "reading the records failed");
+        }
         else GS_CHECK_CUDA(ctx, cudaMemcpyAsync(host_grid, g->d_rec, g->E * 4, cudaMemcpyDeviceToHost, ctx->stream));
     }
     if (host_degree)

@@ -313,7 +313,11 @@ gs_status gs_each_part(gs_graph* g, const gs_segment* segs, int n_segs, F launch
 }
 gs_status gs_stream_open(gs_graph* g, const uint32_t* host_grid, uint64_t segment_bytes);
 void gs_stream_close(gs_graph* g);
-const uint32_t* gs_stream_records(const gs_graph* g);   // host records of a streamed graph
+const uint32_t* gs_stream_records(const gs_graph* g);   // host records of a streamed graph (null: file-backed)
+// A graph whose records stream from the .grid file at `path` (from byte 0).
+gs_status gs_stream_open_file(gs_graph* g, const char* path, uint64_t segment_bytes);
+// Copies a streamed graph's records (from memory or the file) to dst.
+bool gs_stream_read_records(const gs_graph* g, uint32_t* dst);
 
 // bfs2 (-j 30) and traverse (-j 4): one u32 label per vertex in d_lab
 gs_status lab_init(gs_state* s);

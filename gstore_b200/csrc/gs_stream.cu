@@ -23,10 +23,20 @@
 //   * sweeps alternate direction, so the segment the previous sweep ended
 //     on is already in HBM when the next one starts (the reference's cache
 //     of segments already in memory, gstore.cpp:1494-1768).
+//
+// A file-backed graph (gs_upload_graph_file) keeps its records in the .grid
+// file instead, as the reference does: a segment's ranges are read with
+// pread into one of two pinned staging buffers (a staging buffer is reused
+// once its previous copy to HBM is done) and copied to HBM in one piece.
+// The host reads segment k+1 while the GPU sweeps segment k.
 #include "gs_internal.cuh"
 
 #include <algorithm>
+#include <cerrno>
 #include <cstring>
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 namespace {
 
@@ -53,6 +63,9 @@ inline uint64_t round4(uint64_t x) { return (x + 3) & ~3ull; }
 struct gs_streamer {
     const uint32_t* h_rec = nullptr;
     bool registered = false;       // cudaHostRegister'ed by the library
+    int fd = -1;                   // file-backed: the .grid file (records from byte 0)
+    uint32_t* h_stage[2] = {nullptr, nullptr};   // file-backed: pinned staging, one per buffer
+    bool staged[2] = {false, false};             // a copy from the staging buffer was queued
     uint64_t seg_records = 0;      // capacity of one segment buffer
     uint32_t* d_buf[2] = {nullptr, nullptr};
     bool used[2] = {false, false};
@@ -208,6 +221,21 @@ void pack(const gs_graph* g, std::vector<gs_seg_run>& ent, uint64_t cap, std::ve
     if (cur.list_n) segs.push_back(cur);
 }
 
+// Reads `bytes` at file offset `off` into dst (pread may return short counts).
+bool pread_full(int fd, void* dst, uint64_t bytes, uint64_t off) {
+    char* p = static_cast<char*>(dst);
+    while (bytes) {
+        const size_t chunk = (size_t)std::min<uint64_t>(bytes, 1ull << 30);
+        const ssize_t r = pread(fd, p, chunk, (off_t)off);
+        if (r < 0 && errno == EINTR) continue;
+        if (r <= 0) return false;
+        p += r;
+        off += (uint64_t)r;
+        bytes -= (uint64_t)r;
+    }
+    return true;
+}
+
 // Queues the copies of segment `sp` into a buffer and returns the buffer.
 gs_status stage(gs_graph* g, const SegPlan& sp, bool first, int prev, int* out) {
     gs_ctx* ctx = g->ctx;
@@ -224,11 +252,30 @@ gs_status stage(gs_graph* g, const SegPlan& sp, bool first, int prev, int* out) 
     }
     if (st->used[b]) GS_CHECK_CUDA(ctx, cudaStreamWaitEvent(st->copy, st->freed[b], 0));
     st->content[b].clear();
-    for (const CopyOp& c : sp.copies) {
-        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(st->d_buf[b] + c.dst, st->h_rec + c.src, c.n * 4,
-                                           cudaMemcpyHostToDevice, st->copy));
-        st->bytes += c.n * 4;
-        st->copies += 1;
+    if (st->fd >= 0) {
+        // the staging buffer's previous copy to HBM must be done before the
+        // file is read into it
+        if (st->staged[b]) GS_CHECK_CUDA(ctx, cudaEventSynchronize(st->ready[b]));
+        uint64_t extent = 0;
+        for (const CopyOp& c : sp.copies) {
+            if (!pread_full(st->fd, st->h_stage[b] + c.dst, c.n * 4, c.src * 4))
+                return gs_fail(ctx, GS_ERR_FORMAT, "reading the .grid file failed at record " + std::to_string(c.src));
+            extent = std::max(extent, c.dst + c.n);
+            st->bytes += c.n * 4;
+        }
+        if (extent) {
+            GS_CHECK_CUDA(ctx, cudaMemcpyAsync(st->d_buf[b], st->h_stage[b], extent * 4, cudaMemcpyHostToDevice,
+                                               st->copy));
+            st->copies += 1;
+        }
+        st->staged[b] = true;
+    } else {
+        for (const CopyOp& c : sp.copies) {
+            GS_CHECK_CUDA(ctx, cudaMemcpyAsync(st->d_buf[b] + c.dst, st->h_rec + c.src, c.n * 4,
+                                               cudaMemcpyHostToDevice, st->copy));
+            st->bytes += c.n * 4;
+            st->copies += 1;
+        }
     }
     st->content[b] = sp.copies;
     GS_CHECK_CUDA(ctx, cudaEventRecord(st->ready[b], st->copy));
@@ -251,12 +298,9 @@ gs_status run_streamed(gs_graph* g, std::vector<gs_seg_run>& ent, int direction,
     int b = 0;
     GS_TRY(stage(g, segs[0], true, st->last, &b));
     gs_status status = GS_OK;
+    // the sweep of segment k is queued before segment k+1 is staged, so a
+    // file-backed segment is read while the previous one sweeps
     for (size_t k = 0; k < segs.size(); ++k) {
-        int nb = b;
-        if (k + 1 < segs.size()) {
-            status = stage(g, segs[k + 1], false, b, &nb);
-            if (status != GS_OK) break;
-        }
         cudaError_t e = cudaStreamWaitEvent(ctx->stream, st->ready[b], 0);
         if (e != cudaSuccess) {
             status = gs_cuda_fail(ctx, e, "cudaStreamWaitEvent(ready)");
@@ -274,7 +318,12 @@ gs_status run_streamed(gs_graph* g, std::vector<gs_seg_run>& ent, int direction,
         st->last = b;
         st->segments += 1;
         if (status != GS_OK) break;
-        b = nb;
+        if (k + 1 < segs.size()) {
+            int nb = b;
+            status = stage(g, segs[k + 1], false, b, &nb);
+            if (status != GS_OK) break;
+            b = nb;
+        }
     }
     g->seg = SegView();
     gs_status st2 = list_done(g, slot);
@@ -350,6 +399,49 @@ gs_status gs_each_part_fn(gs_graph* g, const gs_segment* segs, int n_segs, gs_st
     return status != GS_OK ? status : st2;
 }
 
+namespace {
+
+// The segment buffers, their events and the copy stream of a streamer.
+gs_status open_buffers(gs_graph* g, gs_streamer* st) {
+    gs_ctx* ctx = g->ctx;
+    GS_CHECK_CUDA(ctx, cudaStreamCreateWithFlags(&st->copy, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+        GS_TRY(gs_dev_alloc(ctx, (void**)&st->d_buf[b], st->seg_records * 4 + 16));
+        GS_CHECK_CUDA(ctx, cudaEventCreateWithFlags(&st->ready[b], cudaEventDisableTiming));
+        GS_CHECK_CUDA(ctx, cudaEventCreateWithFlags(&st->freed[b], cudaEventDisableTiming));
+    }
+    return GS_OK;
+}
+
+}  // namespace
+
+gs_status gs_stream_open_file(gs_graph* g, const char* path, uint64_t segment_bytes) {
+    gs_ctx* ctx = g->ctx;
+    const uint64_t min_bytes = 2 * (kRunRecords + 8) * 4;
+    if (segment_bytes < min_bytes)
+        return gs_fail(ctx, GS_ERR_ARG, "segment_bytes must be at least " + std::to_string(min_bytes));
+    gs_streamer* st = new (std::nothrow) gs_streamer();
+    if (!st) return GS_ERR_OOM;
+    g->stream = st;
+    st->seg_records = (segment_bytes / 4) & ~3ull;
+    st->fd = open(path, O_RDONLY);
+    if (st->fd < 0) return gs_fail(ctx, GS_ERR_ARG, std::string("cannot open ") + path);
+    struct stat sb;
+    if (fstat(st->fd, &sb) != 0 || (uint64_t)sb.st_size < g->E * 4)
+        return gs_fail(ctx, GS_ERR_FORMAT, std::string(path) + " holds fewer than the records .start counts");
+    for (int b = 0; b < 2; ++b)
+        GS_CHECK_CUDA(ctx, cudaHostAlloc((void**)&st->h_stage[b], st->seg_records * 4 + 16, cudaHostAllocDefault));
+    return open_buffers(g, st);
+}
+
+bool gs_stream_read_records(const gs_graph* g, uint32_t* dst) {
+    const gs_streamer* st = g->stream;
+    if (!st) return false;
+    if (st->fd >= 0) return pread_full(st->fd, dst, g->E * 4, 0);
+    std::memcpy(dst, st->h_rec, g->E * 4);
+    return true;
+}
+
 gs_status gs_stream_open(gs_graph* g, const uint32_t* host_grid, uint64_t segment_bytes) {
     gs_ctx* ctx = g->ctx;
     const uint64_t min_bytes = 2 * (kRunRecords + 8) * 4;
@@ -376,13 +468,7 @@ gs_status gs_stream_open(gs_graph* g, const uint32_t* host_grid, uint64_t segmen
             }
         }
     }
-    GS_CHECK_CUDA(ctx, cudaStreamCreateWithFlags(&st->copy, cudaStreamNonBlocking));
-    for (int b = 0; b < 2; ++b) {
-        GS_TRY(gs_dev_alloc(ctx, (void**)&st->d_buf[b], st->seg_records * 4 + 16));
-        GS_CHECK_CUDA(ctx, cudaEventCreateWithFlags(&st->ready[b], cudaEventDisableTiming));
-        GS_CHECK_CUDA(ctx, cudaEventCreateWithFlags(&st->freed[b], cudaEventDisableTiming));
-    }
-    return GS_OK;
+    return open_buffers(g, st);
 }
 
 void gs_stream_close(gs_graph* g) {
@@ -397,6 +483,9 @@ void gs_stream_close(gs_graph* g) {
         }
         if (st->copy) cudaStreamDestroy(st->copy);
         if (st->registered) cudaHostUnregister((void*)st->h_rec);
+        for (int b = 0; b < 2; ++b)
+            if (st->h_stage[b]) cudaFreeHost(st->h_stage[b]);
+        if (st->fd >= 0) close(st->fd);
         delete st;
         g->stream = nullptr;
     }

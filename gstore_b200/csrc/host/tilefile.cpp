@@ -35,8 +35,10 @@ std::string write_all(const std::string& path, const T* data, uint64_t count) {
 
 }  // namespace
 
+std::string tile_file_size(const std::string& path, uint64_t* bytes) { return file_size(path, bytes); }
+
 std::string read_tile_files(const std::string& prefix, uint64_t expected_start_entries, uint64_t vert_count,
-                            bool want_degree, tile_files* out) {
+                            bool want_degree, tile_files* out, bool want_grid) {
     uint64_t sb = 0, gb = 0;
     std::string err = file_size(prefix + ".start", &sb);
     if (!err.empty()) return err;
@@ -52,8 +54,11 @@ std::string read_tile_files(const std::string& prefix, uint64_t expected_start_e
     if (out->start.back() != gb / 4)
         return "last .start entry (" + std::to_string(out->start.back()) + ") != records in .grid (" +
                std::to_string(gb / 4) + ")";
-    err = read_all(prefix + ".grid", gb / 4, &out->grid);
-    if (!err.empty()) return err;
+    out->grid.clear();
+    if (want_grid) {
+        err = read_all(prefix + ".grid", gb / 4, &out->grid);
+        if (!err.empty()) return err;
+    }
     out->degree.clear();
     if (want_degree) {
         uint64_t db = 0;

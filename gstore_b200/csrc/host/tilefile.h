@@ -15,9 +15,14 @@ struct tile_files {
 };
 
 // Returns "" on success, otherwise the reason (missing file, size not a
-// multiple of the element, entry count not matching the geometry).
+// multiple of the element, entry count not matching the geometry).  With
+// want_grid false the .grid file is checked but not read (out->grid stays
+// empty): the records then stream from the file.
 std::string read_tile_files(const std::string& prefix, uint64_t expected_start_entries,
-                            uint64_t vert_count, bool want_degree, tile_files* out);
+                            uint64_t vert_count, bool want_degree, tile_files* out, bool want_grid = true);
+
+// Size of a file in bytes ("" on success).
+std::string tile_file_size(const std::string& path, uint64_t* bytes);
 
 // Writes .grid/.start/.degree and the compressed .sdegree/.bdegree pair.
 std::string write_tile_files(const std::string& prefix, const tile_files& tf);

@@ -119,6 +119,17 @@ gs_status gs_upload_graph(gs_ctx* ctx, const uint64_t* start, uint64_t n_start,
 gs_status gs_upload_graph_streamed(gs_ctx* ctx, const uint64_t* start, uint64_t n_start,
                                    const uint32_t* grid, uint64_t n_edges, const int32_t* degree,
                                    uint64_t V, uint64_t segment_bytes, gs_graph** out);
+/* Replaces: the disk side of the same mode (records read from the .grid file
+ * by libaio into the IO segments, prep_read_aio_*, gstore.cpp:3130-3620).
+ * The records stay in the file at grid_path (uint32 records from byte 0,
+ * n_edges of them); every sweep plans the runs its skip rule needs, reads
+ * them with pread into two pinned staging buffers of segment_bytes each and
+ * copies each staged segment to one of two HBM buffers on a side stream: the
+ * host reads segment k+1 while the GPU sweeps segment k.  The file must stay
+ * unchanged until gs_graph_free.  segment_bytes >= 1 MiB + 64 bytes. */
+gs_status gs_upload_graph_file(gs_ctx* ctx, const uint64_t* start, uint64_t n_start, const char* grid_path,
+                               uint64_t n_edges, const int32_t* degree, uint64_t V, uint64_t segment_bytes,
+                               gs_graph** out);
 /* Host-to-device traffic of a streamed graph since upload: bytes copied,
  * cudaMemcpyAsync calls, segments swept, segments found already in HBM
  * (all 0 for a resident graph). */

@@ -75,3 +75,18 @@ def test_jobs_print_reference_results(kron16):
     ref_colored = 1 + sum(int(c) for c in re.findall(r"frontier count: (\d+)", ref))
     assert "coloured vertices = %d" % ref_colored in ours
     assert "Single color propagation time = " in ours
+
+
+def test_semi_external_jobs_stream_from_the_grid_file(kron16):
+    """Jobs 0-3 with a budget (-m 3: 3 MB) below the 4.2 MB grid leave the
+    records in the .grid file and stream them through two 1.5 MB segments;
+    the results are the resident jobs'."""
+    d = kron16
+    prefix = d / "ours"
+    bfs = run(OURS, "-s", 24, "-j", 0, "-a", 1, "-m", 3, "-i", prefix)
+    counts = [int(c) for c in re.findall(r"level: \d+ frontier count: (\d+)", bfs)]
+    assert counts == [4, 907, 35752, 10083, 67, 0]
+    kc = run(OURS, "-s", 24, "-j", 2, "-a", 8, "-m", 3, "-i", prefix)
+    assert re.search(r">= 8vertices count = (\d+)", kc).group(1) == "23418"
+    wcc = run(OURS, "-s", 24, "-j", 3, "-m", 3, "-i", prefix)
+    assert re.findall(r"WCC count = (\d+)", wcc)[-1] == "12"

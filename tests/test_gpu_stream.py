@@ -81,6 +81,47 @@ def test_streamed_kron20_matches_resident(seg_bytes, kron20, gpu_ctx_factory, or
     sg.free()
 
 
+@pytest.mark.parametrize("seg_bytes", [MIN_SEG, 4 << 20])
+def test_file_backed_kron20_matches_resident(seg_bytes, kron20, gpu_ctx_factory, oracle_lib, tmp_path):
+    """Records left in a .grid file, read segment by segment into pinned
+    staging and copied through two HBM buffers: the resident graph's results."""
+    k = kron20
+    ctx = gpu_ctx_factory(False)
+    path = tmp_path / "k20.grid"
+    k["grid"].tofile(path)
+    fg = ctx.upload_file(k["start"], path, k["grid"].size, k["degree"], k["V"], seg_bytes)
+    res = k["graph"]
+    for root in [1, *_roots(k["degree"], 2, 13)]:
+        assert np.array_equal(fg.bfs(root), res.bfs(root)), f"root {root}"
+    lab, n = fg.wcc()
+    lab_r, n_r = res.wcc()
+    assert np.array_equal(lab, lab_r) and n == n_r
+    for kk in (4, 32):
+        assert np.array_equal(fg.kcore(kk)[0], res.kcore(kk)[0]), f"k={kk}"
+    p, _, _ = oracle_lib.geometry(k["V"])
+    r64, _ = oracle_lib.pagerank(k["start"], k["grid"], k["degree"], p, False, k["V"], 3)
+    assert rel_l1(fg.pagerank(3)[0], r64) <= PR_TOL
+    stats = fg.stream_stats()
+    assert stats["segments"] > 0 and stats["bytes"] > 0
+    _, grid_back, _ = fg.download()                    # read back from the file
+    assert np.array_equal(grid_back, k["grid"])
+    fg.free()
+
+
+@pytest.mark.parametrize("name", ["spread18", "handmade_d"])
+def test_file_backed_golden(name, gpu_ctx_factory, tmp_path):
+    g = load_golden(name)
+    ctx = gpu_ctx_factory(g["directed"])
+    path = tmp_path / (name + ".grid")
+    np.asarray(g["grid"], np.uint32).tofile(path)
+    fg = ctx.upload_file(g["start"], path, g["grid"].size, g["degree"], g["V"], MIN_SEG)
+    for r, root in enumerate(g["bfs_roots"]):
+        assert np.array_equal(fg.bfs(int(root)), g["bfs_depth"][r]), f"root {root}"
+    labels, count = fg.wcc()
+    assert np.array_equal(labels, g["wcc_label"]) and count == int(g["wcc_count"])
+    fg.free()
+
+
 def test_streamed_traffic_and_reuse(kron20, gpu_ctx_factory):
     """A PageRank iteration copies every record once, less the segment the
     previous iteration left in HBM; a BFS level copies only the runs its
