@@ -48,7 +48,7 @@ ABI_SYMBOLS = [
     "gs_batch_bfs_levels", "gs_batch_stats", "gs_batch_free",
     "gs_serve_create", "gs_serve_add_graph", "gs_serve_submit", "gs_serve_step", "gs_serve_poll",
     "gs_serve_result", "gs_serve_clock", "gs_serve_stats", "gs_serve_free", "gs_serve_completed",
-    "gs_serve_set_side_streams",
+    "gs_serve_set_side_streams", "gs_serve_result_view", "gs_serve_release",
 ]
 
 
@@ -123,6 +123,9 @@ def lib():
             "gs_serve_free": [vp],
             "gs_serve_completed": [vp, pu64, i32, C.POINTER(C.c_int)],
             "gs_serve_set_side_streams": [vp, i32],
+            "gs_serve_result_view": [vp, u64, C.POINTER(C.c_void_p), pu64, C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), C.POINTER(C.c_int64)],
+            "gs_serve_release": [vp, u64],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -422,6 +425,26 @@ class Server:
         self.ctx._check(lib().gs_serve_result(self._h, rid, _ptr(out), 0 if out is None else out.nbytes,
                                               C.byref(ts), C.byref(td), C.byref(n)))
         return out, ts.value, td.value, n.value
+
+    def result_view(self, rid: int):
+        """(result array viewing the server's pinned buffer, t_submit, t_done,
+        steps) without a copy; the array is valid until release(rid)."""
+        gid, a = self._req[rid]
+        dt = np.dtype(_RESULT_DTYPE[a])
+        p, nb = C.c_void_p(), C.c_uint64()
+        ts, td, n = C.c_double(), C.c_double(), C.c_int64()
+        try:
+            self.ctx._check(lib().gs_serve_result_view(self._h, rid, C.byref(p), C.byref(nb), C.byref(ts),
+                                                       C.byref(td), C.byref(n)))
+        except GStoreError:
+            self._req.pop(rid)        # a failed request is forgotten by the server
+            raise
+        buf = (C.c_char * nb.value).from_address(p.value)
+        return np.frombuffer(buf, dt), ts.value, td.value, n.value
+
+    def release(self, rid: int) -> None:
+        self._req.pop(rid)
+        self.ctx._check(lib().gs_serve_release(self._h, rid))
 
     def clock(self) -> float:
         t = C.c_double()

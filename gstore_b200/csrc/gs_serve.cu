@@ -1047,6 +1047,36 @@ gs_status gs_serve_result(gs_server* s, uint64_t request_id, void* host_dst, uin
     return GS_OK;
 }
 
+gs_status gs_serve_result_view(gs_server* s, uint64_t request_id, const void** data, uint64_t* bytes,
+                               double* t_submit, double* t_done, int64_t* steps) {
+    if (!s || !data || !bytes) return GS_ERR_ARG;
+    auto it = s->reqs.find(request_id);
+    if (it == s->reqs.end()) return gs_fail(s->ctx, GS_ERR_ARG, "unknown request");
+    Request& r = it->second;
+    if (r.state == kQueued || r.state == kActive) return gs_fail(s->ctx, GS_ERR_STATE, "request not finished");
+    if (t_submit) *t_submit = r.t_submit;
+    if (t_done) *t_done = r.t_done;
+    if (steps) *steps = r.steps;
+    if (r.state == kFailed) {
+        const gs_status st = r.status;
+        s->reqs.erase(it);
+        return gs_fail(s->ctx, st, "request failed");
+    }
+    *data = r.result->p;
+    *bytes = r.result_bytes;
+    return GS_OK;
+}
+
+gs_status gs_serve_release(gs_server* s, uint64_t request_id) {
+    if (!s) return GS_ERR_ARG;
+    auto it = s->reqs.find(request_id);
+    if (it == s->reqs.end()) return gs_fail(s->ctx, GS_ERR_ARG, "unknown request");
+    if (it->second.state == kQueued || it->second.state == kActive)
+        return gs_fail(s->ctx, GS_ERR_STATE, "request not finished");
+    s->reqs.erase(it);   // the pinned buffer returns to the pool with its last holder
+    return GS_OK;
+}
+
 gs_status gs_serve_clock(const gs_server* s, double* seconds) {
     if (!s || !seconds) return GS_ERR_ARG;
     *seconds = now_s(s);

@@ -268,6 +268,13 @@ gs_status gs_serve_set_side_streams(gs_server* s, int n);
  * NULL) and forgets the request.  A failed request returns its status. */
 gs_status gs_serve_result(gs_server* s, uint64_t request_id, void* host_dst, uint64_t bytes,
                           double* t_submit, double* t_done, int64_t* steps);
+/* The same result without a copy: *data points to *bytes bytes in the
+ * server's pinned host buffer (gs_download's format), valid until
+ * gs_serve_release(s, request_id), which forgets the request.  A failed
+ * request returns its status and is forgotten at once. */
+gs_status gs_serve_result_view(gs_server* s, uint64_t request_id, const void** data, uint64_t* bytes,
+                               double* t_submit, double* t_done, int64_t* steps);
+gs_status gs_serve_release(gs_server* s, uint64_t request_id);
 gs_status gs_serve_clock(const gs_server* s, double* seconds);
 gs_status gs_serve_stats(const gs_server* s, uint64_t* steps, uint64_t* graph_launches,
                          uint64_t* kernel_launches, uint64_t* hbm_in_use);

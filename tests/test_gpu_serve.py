@@ -231,3 +231,31 @@ def test_serve_completion_queue_and_side_streams(gs, pool, gpu_ctx_factory, orac
         assert sorted(seen) == sorted(ids)
         assert srv.completed() == []
         srv.set_side_streams(8)                  # nothing runs now
+
+
+def test_serve_result_views(gs, pool, gpu_ctx_factory, oracle_lib):
+    """A result read in place (gs_serve_result_view) is the copied result;
+    release forgets the request; a failed request fails the view."""
+    ctx = gpu_ctx_factory(False)
+    reqs = [(0, "bfs", 1), (1, "wcc", 0), (3, "kcore", 5), (2, "pagerank", 3), (1, "bfs", 7)]
+    with gs.Server(ctx) as srv:
+        gids = [srv.add_graph(g) for g in pool]
+        ids = [srv.submit(gids[gi], algo, arg) for gi, algo, arg in reqs]
+        while srv.step() != (0, 0):
+            pass
+        for rid, (gi, algo, arg) in zip(ids, reqs):
+            view, t0, t1, steps = srv.result_view(rid)
+            _check(algo, view, _plain(pool[gi], algo, arg))
+            assert t1 >= t0 and steps >= 1
+            srv.release(rid)
+            with pytest.raises(gs.GStoreError, match="GS_ERR_ARG"):
+                ctx._check(gs.lib().gs_serve_release(srv._h, rid))   # already forgotten
+    path = np.arange(0, 301, dtype=np.uint32)
+    pg = ctx.convert(np.stack([path[:-1], path[1:]], 1), 1 << 16)
+    with gs.Server(ctx) as srv:
+        bad = srv.submit(srv.add_graph(pg), "bfs", 0)     # over 254 levels
+        while srv.step() != (0, 0):
+            pass
+        with pytest.raises(gs.GStoreError, match="GS_ERR_RANGE"):
+            srv.result_view(bad)
+    pg.free()
