@@ -835,13 +835,16 @@ void retire(gs_server* s, const std::vector<uint64_t>& finished, double t) {
     }
 }
 
-// One step of the BFS groups (the captured step graph).
-gs_status bfs_step(gs_server* s) {
+// One step of the BFS groups (the captured step graph), in two halves: the
+// launch, and the outcomes after the step has run.  `group_job` maps a graph
+// to its job in the step (-1: none); *launched says whether a step runs.
+gs_status bfs_launch(gs_server* s, std::vector<int>& group_job, bool* launched) {
     gs_ctx* ctx = s->ctx;
     Table* t = s->h_table;
     int nj = 0;
     uint64_t runs = 0, words = 0;
-    std::vector<int> group_job(s->graphs.size(), -1);
+    *launched = false;
+    group_job.assign(s->graphs.size(), -1);
     for (uint64_t id : s->active) {
         Request& r = s->reqs[id];
         if (r.algo != GS_ALGO_BFS) continue;
@@ -874,6 +877,12 @@ gs_status bfs_step(gs_server* s) {
     t->total_runs = runs;
     t->total_words = words;
     GS_CHECK_CUDA(ctx, cudaGraphLaunch(s->step_exec, s->stream));
+    *launched = true;
+    return GS_OK;
+}
+
+gs_status bfs_finish(gs_server* s, const std::vector<int>& group_job) {
+    gs_ctx* ctx = s->ctx;
     GS_CHECK_CUDA(ctx, cudaStreamSynchronize(s->stream));
     s->graph_launches++;
     s->kernel_launches += 2;
@@ -989,8 +998,17 @@ gs_status gs_serve_step(gs_server* s, int* n_active, int* n_queued) {
         s->active.push_back(r.id);
         s->queue.pop_front();
     }
-    GS_TRY(side_step(s));   // queue side chunks first: they run beside the step
-    GS_TRY(bfs_step(s));
+    // the step runs while the host tends the side requests (their chunks run
+    // beside it on the lower-priority streams)
+    std::vector<int> group_job;
+    bool launched = false;
+    GS_TRY(bfs_launch(s, group_job, &launched));
+    gs_status st = side_step(s);
+    if (launched) {
+        const gs_status st2 = bfs_finish(s, group_job);   // a launched step is always finished
+        if (st == GS_OK) st = st2;
+    }
+    if (st != GS_OK) return st;
     if (n_active) *n_active = (int)s->active.size();
     if (n_queued) *n_queued = (int)s->queue.size();
     return GS_OK;
