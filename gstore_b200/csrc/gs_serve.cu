@@ -24,10 +24,13 @@
 //     decrement sweep (kcore.cpp:63-177), done when a round removed
 //     nothing; PageRank: row-slice sweep + update, `arg` iterations.
 //
-// Between steps the host retires finished requests (results copied to
-// pinned host buffers), admits queued ones while their state fits the HBM
-// budget and a slot is free, and attaches a request to an identical one
-// already queued or running (same graph, algorithm and argument).
+// Each gs_serve_step admits queued requests while their state fits the HBM
+// budget and a slot is free (a request identical to one queued or running --
+// same graph, algorithm and argument -- attaches to it instead), launches the
+// BFS step, tends the side requests while it runs, then retires the finished
+// requests: results land in pinned host buffers, listed by
+// gs_serve_completed, taken with gs_serve_result (a copy) or read in place
+// with gs_serve_result_view until gs_serve_release.
 #include "gs_internal.cuh"
 #include "gs_ops.cuh"
 
