@@ -331,12 +331,7 @@ gs_status bfs_sweep_begin(gs_state* s) {
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(s->d_act_hist + (size_t)s->n_act_hist * g->nw, s->d_act, g->nw,
                                            cudaMemcpyDeviceToDevice, ctx->stream));
     s->n_act_hist += 1;
-    static bool attr_set[64] = {false};
-    if (!attr_set[ctx->device & 63]) {
-        GS_CHECK_CUDA(ctx, cudaFuncSetAttribute(bfs_run_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                (int)sizeof(BfsSmem)));
-        attr_set[ctx->device & 63] = true;
-    }
+    GS_CHECK_CUDA(ctx, gs_smem_limit_once<bfs_run_kernel>(ctx->device, (int)sizeof(BfsSmem)));
     return GS_OK;
 }
 
@@ -403,12 +398,7 @@ gs_status bfs_level_into(gs_ctx* ctx, const gs_graph* g, uint8_t* depth, uint32_
                          uint8_t* act, uint8_t* act_next, unsigned long long* count, int* error,
                          unsigned int* ticket, uint8_t next_level) {
     if (g->R) {
-        static bool attr_set[64] = {false};
-        if (!attr_set[ctx->device & 63]) {
-            GS_CHECK_CUDA(ctx, cudaFuncSetAttribute(bfs_run_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    (int)sizeof(BfsSmem)));
-            attr_set[ctx->device & 63] = true;
-        }
+        GS_CHECK_CUDA(ctx, gs_smem_limit_once<bfs_run_kernel>(ctx->device, (int)sizeof(BfsSmem)));
         const uint64_t n_runs = g->d_runs_lpt ? g->R_lpt : g->R;
         RunArgs a{g->d_runs_lpt ? g->d_runs_lpt : g->d_runs, n_runs, g->d_units, g->d_rec, st, next, act, act_next,
                   g->directed, error, nullptr, ticket};

@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -351,3 +352,18 @@ void gs_timer_begin(gs_ctx* ctx);
 void gs_timer_end(gs_ctx* ctx, int algo, uint64_t bytes);
 
 inline uint32_t gs_grid_size(const gs_ctx* ctx, int per_sm) { return (uint32_t)ctx->num_sms * per_sm; }
+
+// Raises Kernel's dynamic shared-memory limit to `bytes` once per device (the
+// device must be current).  Host threads that drive contexts on different
+// devices may call it concurrently: each device's attempt runs exactly once
+// and every caller sees its result.
+template <auto Kernel>
+inline cudaError_t gs_smem_limit_once(int device, int bytes) {
+    static std::once_flag once[64];
+    static cudaError_t result[64];
+    const int d = device & 63;
+    std::call_once(once[d], [&] {
+        result[d] = cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    });
+    return result[d];
+}

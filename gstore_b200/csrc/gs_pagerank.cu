@@ -292,12 +292,7 @@ gs_status pr_slice_sweep(gs_graph* g, cudaStream_t stream, const float* x, float
     gs_ctx* ctx = g->ctx;
     const gs_pr_layout& L = g->pr;
     if (L.n_items == 0) return GS_OK;
-    static bool attr_set[64] = {false};
-    if (!attr_set[ctx->device & 63]) {
-        GS_CHECK_CUDA(ctx, cudaFuncSetAttribute(pr_slice_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                (int)sizeof(PrSmem)));
-        attr_set[ctx->device & 63] = true;
-    }
+    GS_CHECK_CUDA(ctx, gs_smem_limit_once<pr_slice_kernel>(ctx->device, (int)sizeof(PrSmem)));
     // persistent (two CTAs per SM walking the items) or one CTA per item, so
     // that a higher-priority stream's CTAs find free SMs between items
     const uint32_t grid = (uint32_t)std::min<uint64_t>(L.n_items, item_ctas ? 0x7FFFFFFFull : gs_grid_size(ctx, 3));

@@ -522,8 +522,22 @@ gs_status kcore_init(gs_state* s) {
 
 gs_status kcore_sweep_launch(gs_state* s) {
     gs_graph* g = s->g;
+    gs_ctx* ctx = g->ctx;
+    // Algorithmic bytes of the round, counted only while kernel timing is on:
+    // the records of the tiles whose row or column window holds a vertex
+    // removed this round (the tiles kcore_mmap sweeps, gstore.cpp:2773-2782),
+    // plus the degree and removed-bit reads and the degree writes (8 B/vertex).
+    uint64_t bytes = 0;
+    if (ctx->profile && !g->seg.list) {
+        std::vector<uint8_t> act(g->nw);
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(act.data(), s->d_act, g->nw, cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        uint64_t swept = 0;
+        GS_TRY(gs_swept_records(s, act.data(), &swept));
+        bytes = 4 * swept + 8 * g->V;
+    }
     KcoreOp op{s->d_deg, s->d_kactive, s->d_act};
-    return launch_sweep(g, op, GS_ALGO_KCORE, 0, true);
+    return launch_sweep(g, op, GS_ALGO_KCORE, bytes, true);
 }
 
 gs_status kcore_finalize(gs_state* s, int64_t* frontier, int* done) {

@@ -203,8 +203,12 @@ gs_status gs_bfs_stats(gs_state* s, uint64_t* edges_in_component, uint64_t* swep
  * the caller's device buffer d_depth.  Limit: V <= 16777216 (else
  * GS_ERR_RANGE).  The first call on a device looks the array up; make it
  * before any stream capture.  Calls overlapping on one GPU share the array
- * and race: issue them one after another.  levels_out (may be NULL): sweeps
- * done. */
+ * and race: issue them one after another.  d_depth is cleared and written on
+ * the context's stream (gs_set_stream); the caller must have finished any
+ * other use of that buffer before the call, or ordered that use before it on
+ * the context's stream (for instance with an event the stream waits on).
+ * The call is synchronous: when it returns, d_depth holds the result.
+ * levels_out (may be NULL): sweeps done. */
 gs_status gs_bfs_noalloc(gs_graph* g, uint64_t root, uint8_t* d_depth, int64_t* levels_out);
 
 /* ------------------------------------------------------------ batching --- */

@@ -34,12 +34,17 @@ REF_DIR = HERE / "_ref"
 _lib = None
 
 
-def build(quiet: bool = True) -> None:
-    """Compile liboracle.so (and the reference under _ref when its sources exist)."""
+def build(quiet: bool = True, reference_dir: str | None = None) -> None:
+    """Compile liboracle.so, and the reference itself under _ref when the
+    directory of its sources is given (``reference_dir``, else the
+    ``GS_REFERENCE_DIR`` environment variable; there is no default).  A
+    directory that is given but holds no reference sources is an error."""
     out = subprocess.DEVNULL if quiet else None
     subprocess.run(["make", "-C", str(HERE), "all"], check=True, stdout=out)
-    ref = os.environ.get("GS_REFERENCE_DIR", "/root/reference")
-    if Path(ref).is_dir():
+    ref = reference_dir or os.environ.get("GS_REFERENCE_DIR")
+    if ref:
+        if not (Path(ref) / "gstore.cpp").is_file():
+            raise FileNotFoundError(f"oracle.build: {ref} holds no reference sources (gstore.cpp)")
         subprocess.run(["make", "-C", str(HERE), "ref", f"REF={ref}"], check=True, stdout=out)
 
 
@@ -66,6 +71,8 @@ def lib():
                                 C.c_void_p, u64p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
         L.orc_convert.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_int, C.c_uint64,
                                   C.c_void_p, C.c_void_p, C.c_void_p, u64p]
+        L.orc_edges_reached.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]
+        L.orc_edges_reached.restype = C.c_uint64
         L.orc_bfs2.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_uint64, C.c_uint64,
                                C.c_void_p, C.POINTER(C.c_int)]
         L.orc_traverse.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_uint64, C.c_uint64,
@@ -109,6 +116,14 @@ def bfs(start, grid, p, directed, n, root, max_levels=256):
     if st != 0:
         raise ValueError(f"orc_bfs status {st}")
     return depth, counts[: nl.value].copy(), swept[: nl.value].copy()
+
+
+def edges_reached(start, grid, p, directed, depth) -> int:
+    """Records with both ends reached (depth != 0): the GTEPS numerator."""
+    start = np.ascontiguousarray(start, np.uint64)
+    grid = np.ascontiguousarray(grid, np.uint32)
+    depth = np.ascontiguousarray(depth, np.uint8)
+    return int(lib().orc_edges_reached(_ptr(start), _ptr(grid), p, int(directed), _ptr(depth)))
 
 
 def bfs2(start, grid, p, directed, n, root):
@@ -230,9 +245,10 @@ def ref_convert(edge_file: Path, prefix: Path, V: int, directed: bool = False) -
 
 
 def ref_run(prefix: Path, V: int, algo: str, arg: int, directed: bool = False):
-    """Run the reference's own algorithm class on tile files; returns (array, stdout)."""
+    """Run the reference's own algorithm class on tile files; returns (array, stdout).
+    Runs with different (algo, arg) may go on concurrently."""
     exe = REF_DIR / ("ref_harness_d" if directed else "ref_harness_u")
-    out = Path(str(prefix) + f".{algo}.out")
+    out = Path(str(prefix) + f".{algo}.{arg}.out")
     r = subprocess.run([str(exe), str(prefix), str(V), algo, str(arg), str(out)],
                        check=True, capture_output=True, text=True)
     dt = {"bfs": np.uint8, "kcore": np.int32, "wcc": np.uint32, "pr": np.float32, "bfs2": np.uint8,

@@ -162,6 +162,22 @@ int orc_bfs(const uint64_t* start, const uint32_t* grid, uint32_t p,
     return status;
 }
 
+uint64_t orc_edges_reached(const uint64_t* start, const uint32_t* grid, uint32_t p,
+                           int directed, const uint8_t* depth)
+{
+    tiles_t tl;
+    if (tiles_make(p, directed, &tl)) return 0;
+    uint64_t total = 0;
+    for (uint64_t t = 0; t < tl.T; ++t) {
+        const uint8_t* d0 = depth + ((uint64_t)tl.row[t] << TILE_BITS);
+        const uint8_t* d1 = depth + ((uint64_t)tl.col[t] << TILE_BITS);
+        for (uint64_t e = start[t]; e < start[t + 1]; ++e)
+            total += (d0[grid[e] & 0xFFFF] != 0) & (d1[grid[e] >> 16] != 0);
+    }
+    tiles_free(&tl);
+    return total;
+}
+
 /* --------------------------------------------------------------- bfs2 --- */
 int orc_bfs2(const uint64_t* start, const uint32_t* grid, uint32_t p, int directed,
              uint64_t n, uint64_t root, uint8_t* depth, int* n_sweeps)

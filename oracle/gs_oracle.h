@@ -45,6 +45,12 @@ int orc_bfs(const uint64_t* start, const uint32_t* grid, uint32_t p,
             uint64_t* level_counts, uint64_t* swept, int max_levels,
             int* n_levels);
 
+/* Records whose two ends both have depth != 0: the GTEPS numerator of a
+ * BFS (the records of the root's component on an undirected grid).  The
+ * reference prints no such count; bfs.cpp:193-194 prints vertices per level. */
+uint64_t orc_edges_reached(const uint64_t* start, const uint32_t* grid, uint32_t p,
+                           int directed, const uint8_t* depth);
+
 /* Label-correcting BFS, "-j 30" (bfs2.cpp:56-181): every tile each sweep;
  * a record lowers the depth of an end to the other end's depth + 1 (u8,
  * root 1, 0 = unreached), until a sweep changes nothing.  The result is the

@@ -135,11 +135,13 @@ def test_kron_converter_matches_oracle(kron, oracle_lib):
             assert np.array_equal(np.sort(grid[a:b]), np.sort(k["grid"][a:b]))
 
 
-def test_survey_golden_numbers(kron):
-    """SURVEY golden numbers: Kron 16 has 1,048,067 records, 12 components,
-    23,418 k-core(8) members, BFS-from-1 level sizes 4/907/35752/10083/67;
-    Kron 20 has 16,776,020 records, 207 components, 294,079 k-core(8)
-    members."""
+def test_reference_printed_numbers(kron):
+    """The reference's own printed results on Graph500 Kron 16 / Kron 20
+    (seeds 1,2, edgefactor 16, converted with -c 1): "Total Edges again"
+    (gstore.cpp:2907) 1,048,067 / 16,776,020 records; "WCC count"
+    (wcc.cpp:336) 12 / 207; "vertices count" of -j 22 -a 8
+    (gstore.cpp:2796-2803) 23,418 / 294,079; and the BFS-from-1 "frontier
+    count" lines (bfs.cpp:193-194) 4/907/35752/10083/67 at Kron 16."""
     k16, k20 = kron[16]["graph"], kron[20]["graph"]
     assert k16.n_edges == 1048067 and k20.n_edges == 16776020
     with k16.state("bfs", 1) as s:

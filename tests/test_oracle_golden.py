@@ -114,10 +114,13 @@ def test_tile_index_roundtrip(oracle_lib):
             assert idx == list(range(0, T, 997))
 
 
-def test_survey_kron16_numbers(oracle_lib, tmp_path):
-    """SURVEY golden numbers for Graph500 Kron 16 (seeds 1,2, edgefactor 16):
-    1,048,067 records; BFS from 1 finds 4, 907, 35752, 10083, 67; 12
-    components; 23,418 vertices with degree != 0 after k-core k = 8."""
+def test_reference_kron16_numbers(oracle_lib, tmp_path):
+    """The reference's printed results for Graph500 Kron 16 (seeds 1,2,
+    edgefactor 16, -c 1): 1,048,067 records ("Total Edges again",
+    gstore.cpp:2907); BFS from 1 finds 4, 907, 35752, 10083, 67 ("frontier
+    count", bfs.cpp:193-194); 12 components ("WCC count", wcc.cpp:336);
+    23,418 vertices with degree != 0 after k-core k = 8 ("vertices count",
+    gstore.cpp:2796-2803)."""
     if not oracle_lib.ref_available():
         pytest.skip("reference generator not built here")
     pairs = oracle_lib.ref_generate(16, 16, tmp_path / "k16.bin")

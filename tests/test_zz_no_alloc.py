@@ -54,6 +54,33 @@ def test_noalloc_matches_regular_bfs_golden(env):
     graph.free()
 
 
+def test_noalloc_matches_regular_bfs_directed_golden(env):
+    """The directed grid (push v0 -> v1 only, every tile of the full grid)."""
+    gs, _, torch = env
+    g = load_golden("spread18d")
+    with gs.Context(0, directed=True) as dctx:
+        graph = dctx.upload(g["start"], g["grid"], g["degree"], g["V"])
+        roots = [int(r) for r in g["bfs_roots"][:2]]
+        _check_two_calls(gs, dctx, torch, graph, roots)
+        assert np.array_equal(graph.bfs(roots[0]), g["bfs_depth"][0])
+        graph.free()
+
+
+def test_noalloc_rejects_bad_root_and_streamed_graph(env):
+    gs, ctx, torch = env
+    g = load_golden("spread18")
+    V = int(g["V"])
+    out = torch.empty(V, dtype=torch.uint8, device="cuda")
+    graph = ctx.upload(g["start"], g["grid"], g["degree"], V)
+    with pytest.raises(gs.GStoreError, match="GS_ERR_ARG"):
+        graph.bfs_noalloc(V, out.data_ptr())          # root == V
+    graph.free()
+    streamed = ctx.upload_streamed(g["start"], g["grid"], g["degree"], V, segment_bytes=1 << 20)
+    with pytest.raises(gs.GStoreError, match="GS_ERR_UNSUPPORTED"):
+        streamed.bfs_noalloc(0, out.data_ptr())
+    streamed.free()
+
+
 def test_noalloc_matches_regular_bfs_kron20(env):
     gs, ctx, torch = env
     V = 1 << 20
