@@ -380,7 +380,8 @@ def run_reference_arm(args, dist: Dist):
         del start, grid, depth
         t = sum(timed) / len(timed)
         v = E / t / 1e9
-        sample = (f"reference gstoreu -s {scale} -j 20 (in-memory BFS from root 1) on Graph500 Kron {scale} "
+        sample = (f"reference gstoreu {' '.join(ref_geometry(scale, 20))} -j 20 (in-memory BFS from root 1) on "
+                  f"Graph500 Kron {scale} "
                   f"ef{ef} tile files of the reference generator and converter (-c 1); {len(timed)} timed jobs "
                   f"after {args.warmup} warm-up jobs; numerator {E} records with both ends reached (CPU oracle "
                   f"on the same files)")
@@ -657,7 +658,8 @@ def reference_leg(args, ctx, torch, gs, timer, ours: dict, checks: bool):
         t = statistics.median(bfs_t)
         res["cpu_baseline"] = dict({
             "value": E1 / t / 1e9 if E1 else None, "unit": "GTEPS", "kind": "reference",
-            "sample": (f"reference gstoreu -s {scale} -j 20 (in-memory BFS from root 1) on the reference converter's "
+            "sample": (f"reference gstoreu {' '.join(ref_geometry(scale, 20))} -j 20 (in-memory BFS from root 1) on "
+                       f"the reference converter's "
                        f"tile files of this Kron {scale} ef{ef} graph; median of {len(bfs_t)} jobs; numerator "
                        f"{E1} records with both ends reached"),
             "times_s": bfs_t, "kcore8_s": t_k, "wcc_s": t_w}, **ref_cores())
