@@ -130,8 +130,8 @@ gs_status gs_create(gs_ctx** out, int device, uint64_t hbm_budget_bytes, int dir
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
     if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_scalars, 64 * sizeof(uint64_t));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_ticket, 4 * sizeof(unsigned int));
-    if (e == cudaSuccess) e = cudaMemset(ctx->d_ticket, 0, 4 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_ticket, 8 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemset(ctx->d_ticket, 0, 8 * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->h_scalars, 64 * sizeof(uint64_t));
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) {
@@ -201,6 +201,7 @@ gs_status gs_kernel_time(gs_ctx* ctx, int algo, uint64_t* launches, double* tota
 static void free_graph_arrays(gs_graph* g) {
     gs_stream_close(g);
     pr_layout_free(g);
+    pb_layout_free(g);
     gs_dev_free(g->d_rec);
     gs_dev_free(g->d_items);
     gs_dev_free(g->d_tile_off);

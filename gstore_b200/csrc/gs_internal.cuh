@@ -102,6 +102,35 @@ struct gs_pr_layout {
     bool built = false;
 };
 
+// PageRank propagation-blocked layout (gs_pr_blocked.cu): one entry per
+// (record, direction), sorted by (source slice, destination bin); u16 offsets
+// of the source in its slice and of the destination in its bin, one float
+// value per entry written by the gather pass, and the (slice, bin) blocks in
+// bin-major order for the accumulate pass.
+constexpr int kPbSrcBits = 14;   // source slice: 16,384 vertices (x staged in shared memory)
+constexpr int kPbDstBits = 15;   // destination bin: 32,768 vertices (sums in shared memory)
+struct gs_pb_item1 {             // gather item: entries [e0, e0 + n) of source slice `slice`
+    uint64_t e0;
+    uint32_t n, slice;
+};
+struct gs_pb_item2 {             // accumulate item: blocks [b0, b1) of bin `bin`
+    uint32_t b0, b1, bin, whole;
+};
+struct gs_pb_block {             // entries [e0, e0 + n) of one (slice, bin) block
+    uint64_t e0;
+    uint32_t n, pad;
+};
+struct gs_pb_layout {
+    uint16_t* d_src = nullptr;
+    uint16_t* d_dst = nullptr;
+    float* d_val = nullptr;
+    gs_pb_block* d_blocks = nullptr;
+    gs_pb_item1* d_items1 = nullptr;
+    gs_pb_item2* d_items2 = nullptr;
+    uint64_t n_entries = 0, n_blocks = 0, n_items1 = 0, n_items2 = 0;
+    bool built = false;
+};
+
 struct gs_streamer;   // pinned-host record stream of a graph (gs_stream.cu)
 struct gs_seglists;   // double-buffered entry lists of segment sweeps (gs_stream.cu)
 
@@ -123,7 +152,9 @@ struct gs_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint64_t* d_scalars = nullptr;   // small device scratch for counters/flags
     // run tickets of the persistent sweeps on `stream` ([0..1] generic sweep,
-    // [2..3] PageRank sweep): zero at launch, zeroed again by the last CTA
+    // [2..3] PageRank row-slice sweep, [4..5] and [6..7] the two passes of the
+    // propagation-blocked PageRank sweep): zero at launch, zeroed again by the
+    // last CTA
     unsigned int* d_ticket = nullptr;
     uint64_t* h_scalars = nullptr;   // pinned mirror
     int num_sms = 148;
@@ -163,7 +194,8 @@ struct gs_graph {
     uint32_t* d_tile_rc = nullptr;    // T packed (row << 16 | col)
     int32_t* d_degree = nullptr;      // N
     SegView seg;                      // set during segment sweeps
-    gs_pr_layout pr;                  // built at the first PageRank on a resident graph
+    gs_pr_layout pr;                  // row-slice PageRank layout (serving, batches, smaller graphs)
+    gs_pb_layout pb;                  // propagation-blocked PageRank layout (gs_run on large graphs)
     gs_streamer* stream = nullptr;    // non-null: records stay in host memory
     gs_seglists* lists = nullptr;     // segment entry lists of segment sweeps
     std::vector<gs_tile_run> h_runs;  // host copies of the run and unit tables
@@ -275,6 +307,12 @@ gs_status pr_slice_sweep(gs_graph* g, cudaStream_t stream, const float* x, float
 gs_status pr_finalize_launch(gs_ctx* ctx, cudaStream_t stream, float* x, float* y, float* r, const int32_t* deg,
                              uint64_t N, uint64_t V, int compat);
 gs_status pr_sweep_launch(gs_state* s);
+// Propagation-blocked PageRank (gs_pr_blocked.cu): whether the layout is worth
+// building for this graph (and fits), building and freeing it, one sweep.
+bool pb_layout_wanted(const gs_graph* g);
+gs_status pb_layout_build(gs_graph* g);
+void pb_layout_free(gs_graph* g);
+gs_status pb_launch(gs_state* s);
 gs_status pr_finalize(gs_state* s, int64_t* frontier, int* done);
 
 gs_status wcc_init(gs_state* s);

@@ -1,0 +1,445 @@
+// PageRank sweep by propagation blocking (sm_100a): pagerank_onepart
+// (pr.cpp:119-154) for a large resident graph.
+//
+// Per record (v0, v1) of tile (i, j) the reference does
+//     rank[v1] += prior[v0];   rank[v0] += prior[v1]   (the second: half grid)
+// i.e. every record pushes x of one end into s of the other, once per
+// direction.  At Kronecker scale 26 both ends are random over 268 MB arrays,
+// so a sweep that touches x and s per record pays two random L2/DRAM
+// operations per record, and the L1 pipe that issues them is the limit.
+//
+// Here a sweep is two streaming passes over a layout built once per graph
+// (Beamer, Asanovic, Patterson, "Reducing PageRank Communication via
+// Propagation Blocking", IPDPS 2017, restated for the tile grid):
+//
+//   * entries: one per (record, direction), sorted by (source slice S =
+//     src >> 14, destination bin D = dst >> 15, dst, src).  Two u16 streams
+//     hold the source's offset in its slice and the destination's offset in
+//     its bin; the (S, D) blocks of the stream are contiguous;
+//   * gather (pass 1): a CTA stages x of one source slice (16,384 floats,
+//     64 KB) in shared memory with one bulk copy and streams the slice's
+//     entries: val[e] = x[src of e] -- a shared-memory gather, a coalesced
+//     16-bit read and a coalesced 32-bit write per entry;
+//   * accumulate (pass 2): a CTA owns one destination bin (32,768 floats,
+//     128 KB of shared memory), walks the bin's blocks (one per source slice,
+//     D-major block table) and adds val[e] into its shared-memory sums at
+//     the destination offset, then writes the bin's sums to y.
+//
+// Both passes stream; the random accesses stay in shared memory.  DRAM bytes
+// per entry and sweep: 2 (source offset) + 4 + 4 (value written and read) +
+// 2 (destination offset) = 12, plus x, y and the block table.  The sums are
+// re-associated per bin (FP32), which only changes rounding.
+#include "gs_internal.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <vector>
+
+namespace {
+
+constexpr uint32_t kSrcSlice = 1u << kPbSrcBits;   // 16,384
+constexpr uint32_t kDstBin = 1u << kPbDstBits;     // 32,768
+constexpr int kKeyLowBits = kPbSrcBits + kPbDstBits;
+constexpr int kGatherThreads = 512;
+constexpr int kAccThreads = 1024;
+constexpr long long kWaitLimit = 1ll << 24;
+
+struct __align__(128) GatherSmem {
+    float xs[kSrcSlice];
+    unsigned long long bar;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool wait_bar(unsigned long long* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (long long i = 0; i < kWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Pass 1.  Item: entries [e0, e0 + n) of source slice `slice`.
+__global__ void __launch_bounds__(kGatherThreads, 3)
+    pb_gather_kernel(const gs_pb_item1* __restrict__ items, uint64_t n_items, const uint16_t* __restrict__ src,
+                     const float* __restrict__ x, float* __restrict__ val, int* error, unsigned int* ticket) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    GatherSmem& m = *reinterpret_cast<GatherSmem*>(smem_raw);
+    const uint32_t tid = threadIdx.x;
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&m.bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t parity = 0;
+    __shared__ unsigned long long s_item;
+    auto advance = [&](uint64_t i) -> uint64_t {
+        if (!ticket) return i + gridDim.x;
+        __syncthreads();   // every thread has read the previous draw
+        if (tid == 0) s_item = atomicAdd(ticket, 1u);
+        __syncthreads();
+        return s_item;
+    };
+    for (uint64_t i = ticket ? advance(0) : blockIdx.x; i < n_items; i = advance(i)) {
+        const gs_pb_item1 it = items[i];
+        if (tid == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&m.bar)),
+                         "r"(kSrcSlice * 4)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_u32(m.xs)),
+                "l"(x + ((uint64_t)it.slice << kPbSrcBits)), "r"(kSrcSlice * 4), "r"(smem_u32(&m.bar))
+                : "memory");
+        }
+        const bool got = wait_bar(&m.bar, parity);
+        parity ^= 1;
+        if (!__syncthreads_and(got)) {
+            if (tid == 0) atomicExch(error, 1);
+            break;   // uniform; nothing else in flight
+        }
+        const uint64_t e0 = it.e0, end = it.e0 + it.n;
+        // head up to a multiple of 8 entries, 8-entry body (16-byte loads,
+        // two 16-byte stores), tail
+        const uint64_t a = ((e0 + 7) & ~7ull) < end ? ((e0 + 7) & ~7ull) : end;
+        const uint64_t b = (end & ~7ull) > a ? (end & ~7ull) : a;
+        for (uint64_t e = e0 + tid; e < a; e += kGatherThreads) val[e] = m.xs[src[e]];
+        for (uint64_t e = b + tid; e < end; e += kGatherThreads) val[e] = m.xs[src[e]];
+        const uint4* s8 = reinterpret_cast<const uint4*>(src);
+        float4* v4 = reinterpret_cast<float4*>(val);
+        const uint64_t c1 = b >> 3;
+        uint64_t c = (a >> 3) + tid;
+        for (; c + kGatherThreads < c1; c += 2 * kGatherThreads) {
+            const uint4 w0 = __ldcs(s8 + c), w1 = __ldcs(s8 + c + kGatherThreads);
+            v4[2 * c] = make_float4(m.xs[w0.x & 0xFFFFu], m.xs[w0.x >> 16], m.xs[w0.y & 0xFFFFu], m.xs[w0.y >> 16]);
+            v4[2 * c + 1] =
+                make_float4(m.xs[w0.z & 0xFFFFu], m.xs[w0.z >> 16], m.xs[w0.w & 0xFFFFu], m.xs[w0.w >> 16]);
+            const uint64_t d = c + kGatherThreads;
+            v4[2 * d] = make_float4(m.xs[w1.x & 0xFFFFu], m.xs[w1.x >> 16], m.xs[w1.y & 0xFFFFu], m.xs[w1.y >> 16]);
+            v4[2 * d + 1] =
+                make_float4(m.xs[w1.z & 0xFFFFu], m.xs[w1.z >> 16], m.xs[w1.w & 0xFFFFu], m.xs[w1.w >> 16]);
+        }
+        if (c < c1) {
+            const uint4 w0 = __ldcs(s8 + c);
+            v4[2 * c] = make_float4(m.xs[w0.x & 0xFFFFu], m.xs[w0.x >> 16], m.xs[w0.y & 0xFFFFu], m.xs[w0.y >> 16]);
+            v4[2 * c + 1] =
+                make_float4(m.xs[w0.z & 0xFFFFu], m.xs[w0.z >> 16], m.xs[w0.w & 0xFFFFu], m.xs[w0.w >> 16]);
+        }
+        __syncthreads();   // xs is rewritten by the next item
+    }
+    if (ticket && tid == 0 && atomicAdd(ticket + 1, 1u) == gridDim.x - 1) {
+        atomicExch(ticket, 0u);   // every CTA has drawn its last ticket
+        atomicExch(ticket + 1, 0u);
+    }
+}
+
+// Pass 2.  Item: blocks [b0, b1) of the D-major block table, all of bin
+// `bin`; `whole` when the item holds every block of the bin (its sums are
+// then stored, else added to y).
+__global__ void __launch_bounds__(kAccThreads, 1)
+    pb_accumulate_kernel(const gs_pb_item2* __restrict__ items, uint64_t n_items,
+                         const gs_pb_block* __restrict__ blocks, const uint16_t* __restrict__ dst,
+                         const float* __restrict__ val, float* __restrict__ y, unsigned int* ticket) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float* acc = reinterpret_cast<float*>(smem_raw);
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    constexpr uint32_t kWarps = kAccThreads / 32;
+    constexpr int kU = 8;   // entries in flight per lane
+    __shared__ unsigned long long s_item;
+    auto advance = [&](uint64_t i) -> uint64_t {
+        if (!ticket) return i + gridDim.x;
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(ticket, 1u);
+        __syncthreads();
+        return s_item;
+    };
+    float4* acc4 = reinterpret_cast<float4*>(acc);
+    for (uint64_t i = ticket ? advance(0) : blockIdx.x; i < n_items; i = advance(i)) {
+        const gs_pb_item2 it = items[i];
+        for (uint32_t k = tid; k < kDstBin / 4; k += kAccThreads) acc4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();
+        for (uint32_t bi = it.b0 + warp; bi < it.b1; bi += kWarps) {
+            const gs_pb_block blk = blocks[bi];
+            for (uint32_t k = lane; k < blk.n; k += 32 * kU) {
+                uint32_t d[kU];
+                float v[kU];
+#pragma unroll
+                for (int j = 0; j < kU; ++j) {
+                    const uint32_t q = k + 32u * j;
+                    d[j] = q < blk.n ? __ldcs(dst + blk.e0 + q) : 0u;
+                    v[j] = q < blk.n ? __ldcs(val + blk.e0 + q) : 0.f;
+                }
+#pragma unroll
+                for (int j = 0; j < kU; ++j)
+                    if (k + 32u * j < blk.n) atomicAdd(acc + d[j], v[j]);
+            }
+        }
+        __syncthreads();
+        float4* y4 = reinterpret_cast<float4*>(y + ((uint64_t)it.bin << kPbDstBits));
+        for (uint32_t k = tid; k < kDstBin / 4; k += kAccThreads) {
+            const float4 s = acc4[k];
+            if (it.whole) y4[k] = s;
+            else if (s.x != 0.f || s.y != 0.f || s.z != 0.f || s.w != 0.f) atomicAdd(y4 + k, s);
+        }
+        __syncthreads();   // acc is cleared by the next item
+    }
+    if (ticket && tid == 0 && atomicAdd(ticket + 1, 1u) == gridDim.x - 1) {
+        atomicExch(ticket, 0u);
+        atomicExch(ticket + 1, 0u);
+    }
+}
+
+// ------------------------------------------------------------------ build --
+// One key per (record, direction): (S * nD + D) above kKeyLowBits, then the
+// destination's and the source's offsets.
+__device__ __forceinline__ uint64_t pb_key(uint32_t src, uint32_t dst, uint32_t nD) {
+    const uint64_t blk = (uint64_t)(src >> kPbSrcBits) * nD + (dst >> kPbDstBits);
+    return (blk << kKeyLowBits) | ((uint64_t)(dst & (kDstBin - 1)) << kPbSrcBits) | (src & (kSrcSlice - 1));
+}
+
+__global__ void pb_keys_kernel(const gs_unit* __restrict__ units, uint64_t n_units, const uint32_t* __restrict__ rec,
+                               uint32_t nD, int directed, uint64_t* __restrict__ keys) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t n_warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t u = warp; u < n_units; u += n_warps) {
+        const gs_unit un = units[u];
+        const uint32_t rb = (un.rc >> 16) << 16, cb = (un.rc & 0xFFFFu) << 16;
+        for (uint32_t k = lane; k < un.n; k += 32) {
+            const uint64_t e = un.rec_beg + k;
+            const uint32_t r = rec[e];
+            const uint32_t a = rb + (r & 0xFFFFu), b = cb + (r >> 16);
+            if (directed) {
+                keys[e] = pb_key(a, b, nD);                  // push v0 -> v1 only (pr.cpp:141-146)
+            } else {
+                keys[2 * e] = pb_key(a, b, nD);              // rank[v1] += prior[v0]
+                keys[2 * e + 1] = pb_key(b, a, nD);          // rank[v0] += prior[v1]
+            }
+        }
+    }
+}
+
+__global__ void pb_split_kernel(const uint64_t* __restrict__ keys, uint64_t n, uint16_t* __restrict__ src,
+                                uint16_t* __restrict__ dst) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t e = tid; e < n; e += nth) {
+        const uint64_t k = keys[e];
+        src[e] = (uint16_t)(k & (kSrcSlice - 1));
+        dst[e] = (uint16_t)((k >> kPbSrcBits) & (kDstBin - 1));
+    }
+}
+
+// First entry of every block id in [0, n_blk] (n_blk: one past the last):
+// a binary search over the sorted keys.
+__global__ void pb_block_start_kernel(const uint64_t* __restrict__ keys, uint64_t n, uint64_t n_blk,
+                                      uint64_t* __restrict__ start) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t bid = tid; bid <= n_blk; bid += nth) {
+        uint64_t lo = 0, hi = n;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if ((keys[mid] >> kKeyLowBits) < bid) lo = mid + 1;
+            else hi = mid;
+        }
+        start[bid] = lo;
+    }
+}
+
+// The D-major block table: blocks[D * nS + S] = block (S, D).
+__global__ void pb_block_table_kernel(const uint64_t* __restrict__ start, uint32_t nS, uint32_t nD,
+                                      gs_pb_block* __restrict__ blocks) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t n_blk = (uint64_t)nS * nD;
+    for (uint64_t p = tid; p < n_blk; p += nth) {
+        const uint64_t D = p / nS, S = p % nS, bid = S * nD + D;
+        blocks[p] = gs_pb_block{start[bid], (uint32_t)(start[bid + 1] - start[bid]), 0u};
+    }
+}
+
+inline uint32_t grid_for(uint64_t n, const gs_ctx* ctx) {
+    const uint64_t b = (n + 255) / 256;
+    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(b, gs_grid_size(ctx, 16)));
+}
+
+}  // namespace
+
+void pb_layout_free(gs_graph* g) {
+    gs_pb_layout& L = g->pb;
+    gs_dev_free(L.d_src);
+    gs_dev_free(L.d_dst);
+    gs_dev_free(L.d_val);
+    gs_dev_free(L.d_blocks);
+    gs_dev_free(L.d_items1);
+    gs_dev_free(L.d_items2);
+    L = gs_pb_layout();
+}
+
+bool pb_layout_wanted(const gs_graph* g) {
+    if (g->stream || g->E == 0) return false;
+    const uint64_t n_ent = g->directed ? g->E : 2 * g->E;
+    const uint64_t nS = g->N >> kPbSrcBits, nD = g->N >> kPbDstBits;
+    // the block table is dense (every (S, D) pair): worth it when blocks hold
+    // many entries on average
+    if (nS * nD * 64 > n_ent || nS * nD >= (1ull << 31)) return false;
+    // under an HBM budget the layout (8 B per entry) must fit beside the records
+    if (g->ctx->budget && 4 * g->E + 8 * n_ent > g->ctx->budget) return false;
+    // building needs the sort's two key buffers too
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return false;
+    const uint64_t need = n_ent * (8 + 16) + (nS * nD + 1) * 24 + (2ull << 30);
+    return free_b > need;
+}
+
+gs_status pb_layout_build(gs_graph* g) {
+    gs_ctx* ctx = g->ctx;
+    gs_pb_layout& L = g->pb;
+    pb_layout_free(g);
+    const uint64_t n_ent = g->directed ? g->E : 2 * g->E;
+    const uint32_t nS = (uint32_t)(g->N >> kPbSrcBits), nD = (uint32_t)(g->N >> kPbDstBits);
+    const uint64_t n_blk = (uint64_t)nS * nD;
+    int end_bit = kKeyLowBits;
+    while ((1ull << (end_bit - kKeyLowBits)) < n_blk) ++end_bit;
+
+    uint64_t *d_k0 = nullptr, *d_k1 = nullptr, *d_start = nullptr;
+    void* d_tmp = nullptr;
+    size_t tmp_bytes = 0;
+    gs_status st = gs_dev_alloc(ctx, (void**)&d_k0, n_ent * 8);
+    if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&d_k1, n_ent * 8);
+    if (st == GS_OK) {
+        pb_keys_kernel<<<gs_grid_size(ctx, 8), 256, 0, ctx->stream>>>(g->d_units, g->U, g->d_rec, nD, g->directed,
+                                                                       d_k0);
+        ctx->launches++;
+        cudaError_t e = cudaGetLastError();
+        cub::DoubleBuffer<uint64_t> keys(d_k0, d_k1);
+        if (e == cudaSuccess)
+            e = cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, keys, n_ent, 0, end_bit, ctx->stream);
+        if (e == cudaSuccess) st = gs_dev_alloc(ctx, &d_tmp, tmp_bytes);
+        if (e == cudaSuccess && st == GS_OK)
+            e = cub::DeviceRadixSort::SortKeys(d_tmp, tmp_bytes, keys, n_ent, 0, end_bit, ctx->stream);
+        ctx->launches++;
+        if (e != cudaSuccess && st == GS_OK) st = gs_cuda_fail(ctx, e, "propagation-blocking key sort");
+        const uint64_t* sorted = keys.Current();
+        gs_dev_free(d_tmp);
+        d_tmp = nullptr;
+        if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_src, n_ent * 2);
+        if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_dst, n_ent * 2);
+        if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&d_start, (n_blk + 1) * 8);
+        if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_blocks, std::max<uint64_t>(1, n_blk) * sizeof(gs_pb_block));
+        if (st == GS_OK) {
+            pb_split_kernel<<<grid_for(n_ent, ctx), 256, 0, ctx->stream>>>(sorted, n_ent, L.d_src, L.d_dst);
+            pb_block_start_kernel<<<grid_for(n_blk + 1, ctx), 256, 0, ctx->stream>>>(sorted, n_ent, n_blk, d_start);
+            pb_block_table_kernel<<<grid_for(n_blk, ctx), 256, 0, ctx->stream>>>(d_start, nS, nD, L.d_blocks);
+            ctx->launches += 3;
+            e = cudaGetLastError();
+            if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "propagation-blocking layout");
+        }
+    }
+    gs_dev_free(d_k0);
+    gs_dev_free(d_k1);
+    std::vector<gs_pb_block> blocks(n_blk);
+    std::vector<uint64_t> slice_start(nS + 1);
+    if (st == GS_OK) {
+        cudaError_t e = cudaMemcpyAsync(blocks.data(), L.d_blocks, n_blk * sizeof(gs_pb_block),
+                                        cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        // entries of slice S start at block (S, 0), the first of the bin-major table
+        for (uint32_t s = 0; s < nS; ++s) slice_start[s] = blocks[s].e0;
+        slice_start[nS] = n_ent;
+        if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "propagation-blocking tables");
+    }
+    gs_dev_free(d_start);
+    if (st != GS_OK) {
+        pb_layout_free(g);
+        return st;
+    }
+    // Items: entry chunks of every slice (pass 1) and block ranges of every
+    // bin (pass 2), sized so that each pass has a few items per resident CTA.
+    const uint64_t per1 = std::clamp<uint64_t>(n_ent / ((uint64_t)ctx->num_sms * 12), 32768, 1ull << 20);
+    const uint64_t per2 = std::clamp<uint64_t>(n_ent / ((uint64_t)ctx->num_sms * 4), 65536, 1ull << 22);
+    std::vector<gs_pb_item1> items1;
+    for (uint32_t s = 0; s < nS; ++s)
+        for (uint64_t e = slice_start[s]; e < slice_start[s + 1]; e += per1)
+            items1.push_back(gs_pb_item1{e, (uint32_t)std::min<uint64_t>(per1, slice_start[s + 1] - e), s});
+    std::vector<gs_pb_item2> items2;
+    for (uint32_t d = 0; d < nD; ++d) {
+        const uint32_t first = (uint32_t)items2.size();
+        uint64_t acc = 0, bin_total = 0;
+        uint32_t b0 = d * nS;
+        for (uint32_t b = d * nS; b < (d + 1) * nS; ++b) {
+            bin_total += blocks[b].n;
+            if (acc > 0 && acc + blocks[b].n > per2) {
+                items2.push_back(gs_pb_item2{b0, b, d, 0u});
+                b0 = b;
+                acc = 0;
+            }
+            acc += blocks[b].n;
+        }
+        if (acc > 0) items2.push_back(gs_pb_item2{b0, (d + 1) * nS, d, 0u});
+        if (bin_total > 0 && items2.size() == first + 1) items2.back().whole = 1;
+    }
+    L.n_entries = n_ent;
+    L.n_blocks = n_blk;
+    L.n_items1 = items1.size();
+    L.n_items2 = items2.size();
+    st = gs_dev_alloc(ctx, (void**)&L.d_val, n_ent * 4);
+    if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_items1, std::max<size_t>(1, items1.size()) * sizeof(gs_pb_item1));
+    if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_items2, std::max<size_t>(1, items2.size()) * sizeof(gs_pb_item2));
+    cudaError_t e = cudaSuccess;
+    if (st == GS_OK && !items1.empty())
+        e = cudaMemcpyAsync(L.d_items1, items1.data(), items1.size() * sizeof(gs_pb_item1), cudaMemcpyHostToDevice,
+                            ctx->stream);
+    if (st == GS_OK && e == cudaSuccess && !items2.empty())
+        e = cudaMemcpyAsync(L.d_items2, items2.data(), items2.size() * sizeof(gs_pb_item2), cudaMemcpyHostToDevice,
+                            ctx->stream);
+    if (st == GS_OK && e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (st == GS_OK && e != cudaSuccess) st = gs_cuda_fail(ctx, e, "propagation-blocking items");
+    if (st != GS_OK) {
+        pb_layout_free(g);
+        return st;
+    }
+    L.built = true;
+    return GS_OK;
+}
+
+gs_status pb_sweep(gs_graph* g, const float* x, float* y, int* error) {
+    gs_ctx* ctx = g->ctx;
+    const gs_pb_layout& L = g->pb;
+    if (L.n_items1 == 0) return GS_OK;
+    GS_CHECK_CUDA(ctx, gs_smem_limit_once<pb_gather_kernel>(ctx->device, (int)sizeof(GatherSmem)));
+    GS_CHECK_CUDA(ctx, gs_smem_limit_once<pb_accumulate_kernel>(ctx->device, (int)(kDstBin * 4)));
+    const uint32_t g1 = (uint32_t)std::min<uint64_t>(L.n_items1, gs_grid_size(ctx, 3));
+    pb_gather_kernel<<<g1, kGatherThreads, sizeof(GatherSmem), ctx->stream>>>(L.d_items1, L.n_items1, L.d_src, x,
+                                                                             L.d_val, error, ctx->d_ticket + 4);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    const uint32_t g2 = (uint32_t)std::min<uint64_t>(L.n_items2, gs_grid_size(ctx, 1));
+    pb_accumulate_kernel<<<g2, kAccThreads, kDstBin * 4, ctx->stream>>>(L.d_items2, L.n_items2, L.d_blocks, L.d_dst,
+                                                                       L.d_val, y, ctx->d_ticket + 6);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    ctx->launches += 2;
+    return GS_OK;
+}
+
+gs_status pb_launch(gs_state* s) {
+    gs_graph* g = s->g;
+    gs_ctx* ctx = g->ctx;
+    if (!s->d_error) {
+        GS_TRY(gs_state_alloc(s, (void**)&s->d_error, sizeof(uint64_t)));
+        GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_error, 0, sizeof(uint64_t), ctx->stream));
+    }
+    gs_timer_begin(ctx);
+    GS_TRY(pb_sweep(g, s->d_x, s->d_y, (int*)s->d_error));
+    // algorithmic bytes per iteration: 4E + 12V (records, x, s, inv)
+    gs_timer_end(ctx, GS_ALGO_PAGERANK, 4 * g->E + 12 * g->V);
+    return GS_OK;
+}

@@ -420,13 +420,18 @@ gs_status pr_init(gs_state* s) {
     ctx->launches++;
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_r, 0, g->N * 4, ctx->stream));
     if (s->d_error) GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_error, 0, sizeof(uint64_t), ctx->stream));
-    // resident graphs sweep the row-slice layout (built once per graph)
-    if (!g->stream && g->E && !g->pr.built) GS_TRY(pr_layout_build(g));
+    // resident graphs sweep the propagation-blocked layout when it is worth
+    // building and fits, else the row-slice layout (each built once per graph)
+    if (!g->stream && g->E && !g->pb.built && !g->pr.built) {
+        if (pb_layout_wanted(g)) GS_TRY(pb_layout_build(g));
+        else GS_TRY(pr_layout_build(g));
+    }
     return GS_OK;
 }
 
 gs_status pr_sweep_launch(gs_state* s) {
     gs_graph* g = s->g;
+    if (!g->seg.list && g->pb.built) return pb_launch(s);
     if (!g->seg.list && g->pr.built) return pr_slice_launch(s);
     PrOp op{s->d_x, s->d_y, g->directed};
     // algorithmic bytes per iteration: 4E + 12V (records, x, s, inv)
