@@ -611,7 +611,7 @@ def reference_leg(args, ctx, torch, gs, timer, ours: dict, checks: bool):
         roots = ours["bfs_roots"]
         g = ctx.upload(start, grid, degree, V)
         ms_b, e_b = time_bfs_roots(g, timer, roots, theirs["bfs"])
-        ms_pr, _, _, _ = time_algo(g, timer, "pagerank", 5)
+        ms_pr, _, _, _ = time_algo(g, timer, "pagerank", 5, theirs)
         ms_wcc, _, n_wcc, _ = time_algo(g, timer, "wcc", 0, theirs)
         ms_k, _, n_k, _ = time_algo(g, timer, "kcore", 8, theirs, key="kcore8")
         g.free()
@@ -639,6 +639,7 @@ def reference_leg(args, ctx, torch, gs, timer, ours: dict, checks: bool):
             jobs = {("bfs", r): (lambda r=r: oracle.bfs(start, grid, p, False, V, r)[0]) for r in roots}
             jobs["wcc"] = lambda: oracle.wcc(start, grid, p, False, V)[0]
             jobs["kcore8"] = lambda: oracle.kcore(start, grid, degree, p, V, 8)[0]
+            jobs["pagerank"] = lambda: oracle.pagerank(start, grid, degree, p, False, V, 5)[0]
             t0 = time.perf_counter()
             with ThreadPoolExecutor(len(jobs)) as ex:          # the oracle's C calls release the GIL
                 futs = {k: ex.submit(f) for k, f in jobs.items()}
@@ -651,6 +652,10 @@ def reference_leg(args, ctx, torch, gs, timer, ours: dict, checks: bool):
                                           "reference_tiles": bool(np.array_equal(theirs["wcc"], orc["wcc"]))}
             par["kcore_deg_equal"] = {"engine_tiles": bool(np.array_equal(ours["kcore8"], orc["kcore8"])),
                                       "reference_tiles": bool(np.array_equal(theirs["kcore8"], orc["kcore8"]))}
+            e_own, e_ref = rel_l1(ours["pagerank"], orc["pagerank"]), rel_l1(theirs["pagerank"], orc["pagerank"])
+            par["pagerank_rel_l1_vs_fp64_oracle"] = {"engine_tiles": e_own, "reference_tiles": e_ref,
+                                                     "iterations": 5, "tolerance": PR_TOL,
+                                                     "within": bool(max(e_own, e_ref) <= PR_TOL)}
             E1 = oracle.edges_reached(start, grid, p, False, orc[("bfs", 1)]) if 1 in roots else None
         else:
             E1 = e_b[roots.index(1)] if 1 in roots else None
@@ -1120,7 +1125,8 @@ def main():
     # ------------------------------------------------------ secondary metrics
     if not args.no_secondary:
         sec = {}
-        pr_ms, _, _, (n, kms, kbytes) = time_algo(graph, timer, "pagerank", 5, kernel=gs.GS_ALGO_PAGERANK)
+        pr_ms, _, _, (n, kms, kbytes) = time_algo(graph, timer, "pagerank", 5, ours if leg else None,
+                                                  kernel=gs.GS_ALGO_PAGERANK)
         sec["pagerank"] = {"metric": "PR edge records/s/iteration", "iterations": 5,
                            "ms_per_iter": pr_ms / 5, "value": graph.n_edges / (pr_ms / 5 / 1e3),
                            "sweep_ms_per_iter": kms / max(n, 1),
@@ -1152,7 +1158,7 @@ def main():
         graph.free()
         torch.cuda.empty_cache()
 
-        parts = {"upload": [], "bfs": [], "download": [], "free": []}
+        parts = {"upload": [], "bfs": [], "download": [], "free": [], "step": []}
 
         def e2e_step(root):
             t_a = time.perf_counter()
@@ -1166,7 +1172,8 @@ def main():
                 t_d = time.perf_counter()
             g2.free()
             t_e = time.perf_counter()
-            for k, a, b in (("upload", t_a, t_b), ("bfs", t_b, t_c), ("download", t_c, t_d), ("free", t_d, t_e)):
+            for k, a, b in (("upload", t_a, t_b), ("bfs", t_b, t_c), ("download", t_c, t_d), ("free", t_d, t_e),
+                            ("step", t_a, t_e)):
                 parts[k].append((b - a) * 1e3)
 
         e2e_step(timed_roots[0])
@@ -1183,7 +1190,8 @@ def main():
                        "h2d_bytes_per_step": int(pin_grid.numel() * 4 + pin_start.numel() * 8 + pin_deg.numel() * 4),
                        "d2h_bytes_per_step": V,
                        "what": "per step: gs_upload_graph from pinned host tile arrays, BFS, depth download",
-                       "ms_per_step_median": {k: float(np.median(v)) for k, v in parts.items()}}
+                       "ms_per_step_median": {k: float(np.median(v)) for k, v in parts.items()},
+                       "ms_per_step_max": {k: float(np.max(v)) for k, v in parts.items()}}
         del pin_grid
     else:
         ours["start"], _, ours["degree"] = graph.download()

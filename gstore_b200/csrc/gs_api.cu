@@ -550,6 +550,8 @@ gs_status gs_upload_graph(gs_ctx* ctx, const uint64_t* start, uint64_t n_start,
         }
     }
     if (st == GS_OK) st = finish_upload(g, degree, false);
+    bool sorted_now = false;
+    if (st == GS_OK) st = gs_order_tiles(g, &sorted_now);
     if (st != GS_OK) {
         free_graph_arrays(g);
         delete g;
@@ -626,6 +628,8 @@ gs_status gs_upload_graph_device(gs_ctx* ctx, const uint64_t* d_start, uint64_t 
         }
     }
     if (st == GS_OK) st = finish_upload(g, d_degree, true);
+    bool sorted_now = false;
+    if (st == GS_OK) st = gs_order_tiles(g, &sorted_now);
     if (st != GS_OK) {
         free_graph_arrays(g);
         delete g;

@@ -82,7 +82,45 @@ __global__ void rebase_offsets_kernel(const uint64_t* __restrict__ start, uint64
         out[i] = (int)(start[t0 + i] - base);
 }
 
+// Flags a tile whose records are not in ascending order (a warp per unit;
+// a unit's first record is compared with the last one of the previous unit
+// when both lie in the same tile).
+__global__ void tiles_unsorted_kernel(const gs_unit* __restrict__ units, uint64_t n_units,
+                                      const uint32_t* __restrict__ rec, int* flag) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t n_warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t u = warp; u < n_units; u += n_warps) {
+        const gs_unit un = units[u];
+        const bool joined = u > 0 && units[u - 1].rc == un.rc && units[u - 1].rec_beg + units[u - 1].n == un.rec_beg;
+        bool bad = false;
+        for (uint32_t k = lane; k < un.n; k += 32) {
+            const uint64_t e = un.rec_beg + k;
+            if ((k > 0 || joined) && rec[e] < rec[e - 1]) bad = true;
+        }
+        if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicExch(flag, 1);
+    }
+}
+
 }  // namespace
+
+gs_status gs_order_tiles(gs_graph* g, bool* sorted_now) {
+    gs_ctx* ctx = g->ctx;
+    *sorted_now = false;
+    if (!g->d_rec || g->E < 2 || g->U == 0) return GS_OK;
+    int* d_flag = (int*)ctx->d_scalars;
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(d_flag, 0, sizeof(int), ctx->stream));
+    tiles_unsorted_kernel<<<gs_grid_size(ctx, 8), 256, 0, ctx->stream>>>(g->d_units, g->U, g->d_rec, d_flag);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    ctx->launches++;
+    int h_flag = 0;
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(&h_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (!h_flag) return GS_OK;
+    GS_TRY(gs_sort_tiles(ctx, g->d_tile_off, g->T, g->d_rec, g->E));
+    *sorted_now = true;
+    return GS_OK;
+}
 
 // Sorts the records of every tile in place (segments = tiles of `start`).
 gs_status gs_sort_tiles(gs_ctx* ctx, const uint64_t* d_start, uint64_t n_tiles, uint32_t* d_rec, uint64_t n_rec) {

@@ -377,6 +377,11 @@ gs_status gs_convert_launch(gs_ctx* ctx, const uint32_t* d_pairs, uint64_t n_pai
                             int32_t** d_degree_out, uint64_t* n_start, uint64_t* n_rec);
 
 gs_status gs_sort_tiles(gs_ctx* ctx, const uint64_t* d_start, uint64_t n_tiles, uint32_t* d_rec, uint64_t n_rec);
+// A resident graph whose tiles hold their records out of ascending order
+// (the reference converter leaves them in its threads' order) gets every
+// tile sorted: the sweeps' column-side state lookups then walk neighbouring
+// words.  Results do not depend on the in-tile order.
+gs_status gs_order_tiles(gs_graph* g, bool* sorted_now);
 gs_status gs_graph_adopt(gs_ctx* ctx, uint64_t V, const uint64_t* d_start, uint64_t n_start, uint32_t* d_rec,
                          uint64_t n_edges, const int32_t* d_degree, gs_graph** out);
 

@@ -44,6 +44,7 @@ constexpr int kKeyLowBits = kPbSrcBits + kPbDstBits;
 constexpr int kGatherThreads = 512;
 constexpr int kAccThreads = 1024;
 constexpr long long kWaitLimit = 1ll << 24;
+constexpr unsigned gsops_full_mask = 0xFFFFFFFFu;
 
 struct __align__(128) GatherSmem {
     float xs[kSrcSlice];
@@ -168,18 +169,32 @@ __global__ void __launch_bounds__(kAccThreads, 1)
         __syncthreads();
         for (uint32_t bi = it.b0 + warp; bi < it.b1; bi += kWarps) {
             const gs_pb_block blk = blocks[bi];
-            for (uint32_t k = lane; k < blk.n; k += 32 * kU) {
+            for (uint32_t k0 = 0; k0 < blk.n; k0 += 32 * kU) {   // warp-uniform: the shuffles need every lane
+                const uint32_t k = k0 + lane;
                 uint32_t d[kU];
                 float v[kU];
 #pragma unroll
                 for (int j = 0; j < kU; ++j) {
                     const uint32_t q = k + 32u * j;
-                    d[j] = q < blk.n ? __ldcs(dst + blk.e0 + q) : 0u;
+                    d[j] = q < blk.n ? __ldcs(dst + blk.e0 + q) : ~0u - lane;   // past the end: distinct keys
                     v[j] = q < blk.n ? __ldcs(val + blk.e0 + q) : 0.f;
                 }
 #pragma unroll
-                for (int j = 0; j < kU; ++j)
-                    if (k + 32u * j < blk.n) atomicAdd(acc + d[j], v[j]);
+                for (int j = 0; j < kU; ++j) {
+                    // 32 consecutive entries, sorted by destination: equal
+                    // destinations sit in adjacent lanes.  Sum each run as a
+                    // tree (segmented suffix sums) and add it once: fewer
+                    // atomics on high-degree vertices and shorter FP32 chains.
+                    float t = v[j];
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const float to = __shfl_down_sync(gsops_full_mask, t, o);
+                        const uint32_t dd = __shfl_down_sync(gsops_full_mask, d[j], o);
+                        if (lane + o < 32 && dd == d[j]) t += to;
+                    }
+                    const uint32_t dp = __shfl_up_sync(gsops_full_mask, d[j], 1);
+                    if ((lane == 0 || dp != d[j]) && d[j] < kDstBin) atomicAdd(acc + d[j], t);
+                }
             }
         }
         __syncthreads();

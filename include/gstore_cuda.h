@@ -100,7 +100,12 @@ gs_status gs_geometry(uint64_t V, int directed, uint32_t* p, uint32_t* p_s,
  * Copies host start[n_start], grid[n_edges] and degree[V] (degree may be NULL:
  * it is then counted on the device from the records) into HBM and builds the
  * tile tables.  Checks: n_start matches the geometry, start is monotone,
- * start[last] == n_edges, every record addresses a vertex below V. */
+ * start[last] == n_edges, every record addresses a vertex below V.  A
+ * resident graph whose tiles hold their records out of ascending order (the
+ * reference converter writes them in its threads' order, gstore.cpp:1403-1447)
+ * has every tile sorted on the device after the copy (the sweeps run about
+ * twice as fast on sorted tiles; results do not depend on the order), so
+ * gs_graph_download then returns the records sorted inside each tile. */
 gs_status gs_upload_graph(gs_ctx* ctx, const uint64_t* start, uint64_t n_start,
                           const uint32_t* grid, uint64_t n_edges,
                           const int32_t* degree, uint64_t V, gs_graph** out);

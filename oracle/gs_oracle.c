@@ -247,6 +247,19 @@ int orc_traverse(const uint64_t* start, const uint32_t* grid, uint32_t p, int di
 }
 
 /* ----------------------------------------------------------- PageRank --- */
+/* Tiles grouped by one of their windows (counting sort of tile indices by
+ * row or by column), so that one thread can own a window's sums. */
+static void tiles_by_window(const tiles_t* tl, uint64_t nw, int by_col, uint64_t* off, uint64_t* idx)
+{
+    memset(off, 0, (nw + 1) * sizeof(uint64_t));
+    for (uint64_t t = 0; t < tl->T; ++t) ++off[(by_col ? tl->col[t] : tl->row[t]) + 1];
+    for (uint64_t w = 0; w < nw; ++w) off[w + 1] += off[w];
+    uint64_t* pos = (uint64_t*)malloc(nw * sizeof(uint64_t));
+    memcpy(pos, off, nw * sizeof(uint64_t));
+    for (uint64_t t = 0; t < tl->T; ++t) idx[pos[by_col ? tl->col[t] : tl->row[t]]++] = t;
+    free(pos);
+}
+
 int orc_pagerank(const uint64_t* start, const uint32_t* grid,
                  const int32_t* degree, uint32_t p, int directed, uint64_t n,
                  int iterations, int compat, double* r_out, double* x_out)
@@ -254,9 +267,16 @@ int orc_pagerank(const uint64_t* start, const uint32_t* grid,
     tiles_t tl;
     if (n == 0 || iterations < 1 || tiles_make(p, directed, &tl)) return -1;
     if (check_range(start, grid, &tl, n)) { tiles_free(&tl); return -1; }
+    const uint64_t nw = (uint64_t)p * GROUP_TILES;
     double* x = (double*)malloc(n * sizeof(double));
     double* s = (double*)malloc(n * sizeof(double));
     double* inv = (double*)malloc(n * sizeof(double));
+    uint64_t* col_off = (uint64_t*)malloc((nw + 1) * sizeof(uint64_t));
+    uint64_t* row_off = (uint64_t*)malloc((nw + 1) * sizeof(uint64_t));
+    uint64_t* col_idx = (uint64_t*)malloc((tl.T + 1) * sizeof(uint64_t));
+    uint64_t* row_idx = (uint64_t*)malloc((tl.T + 1) * sizeof(uint64_t));
+    tiles_by_window(&tl, nw, 1, col_off, col_idx);
+    tiles_by_window(&tl, nw, 0, row_off, row_idx);
     for (uint64_t v = 0; v < n; ++v) {
         x[v] = 1.0 / (double)n;                /* pr.cpp:105-110 */
         int32_t d = degree[v];
@@ -266,15 +286,30 @@ int orc_pagerank(const uint64_t* start, const uint32_t* grid,
     }
     for (int it = 0; it < iterations; ++it) {
         memset(s, 0, n * sizeof(double));
-        for (uint64_t t = 0; t < tl.T; ++t) {
-            uint64_t b0 = (uint64_t)tl.row[t] << TILE_BITS;
-            uint64_t b1 = (uint64_t)tl.col[t] << TILE_BITS;
-            for (uint64_t e = start[t]; e < start[t + 1]; ++e) {
-                uint64_t a = b0 + (grid[e] & 0xFFFF), b = b1 + (grid[e] >> 16);
-                s[b] += x[a];                  /* pr.cpp:145-146 */
-                if (!directed) s[a] += x[b];   /* pr.cpp:147-150 */
+        /* s[v1] += x[v0] (pr.cpp:145-146): a thread owns the sums of one
+         * column window; deterministic order (tiles in file order) */
+        #pragma omp parallel for schedule(dynamic, 1)
+        for (uint64_t w = 0; w < nw; ++w) {
+            for (uint64_t k = col_off[w]; k < col_off[w + 1]; ++k) {
+                const uint64_t t = col_idx[k];
+                const uint64_t b0 = (uint64_t)tl.row[t] << TILE_BITS, b1 = w << TILE_BITS;
+                for (uint64_t e = start[t]; e < start[t + 1]; ++e)
+                    s[b1 + (grid[e] >> 16)] += x[b0 + (grid[e] & 0xFFFF)];
             }
         }
+        /* s[v0] += x[v1] (pr.cpp:147-150, half grid): one row window each */
+        if (!directed) {
+            #pragma omp parallel for schedule(dynamic, 1)
+            for (uint64_t w = 0; w < nw; ++w) {
+                for (uint64_t k = row_off[w]; k < row_off[w + 1]; ++k) {
+                    const uint64_t t = row_idx[k];
+                    const uint64_t b0 = w << TILE_BITS, b1 = (uint64_t)tl.col[t] << TILE_BITS;
+                    for (uint64_t e = start[t]; e < start[t + 1]; ++e)
+                        s[b0 + (grid[e] & 0xFFFF)] += x[b1 + (grid[e] >> 16)];
+                }
+            }
+        }
+        #pragma omp parallel for
         for (uint64_t v = 0; v < n; ++v) {     /* pr.cpp:281-302 */
             double r = 0.15 + 0.85 * s[v];
             if (r_out) r_out[v] = r;
@@ -282,7 +317,8 @@ int orc_pagerank(const uint64_t* start, const uint32_t* grid,
         }
     }
     if (x_out) memcpy(x_out, x, n * sizeof(double));
-    free(x); free(s); free(inv); tiles_free(&tl);
+    free(x); free(s); free(inv); free(col_off); free(row_off); free(col_idx); free(row_idx);
+    tiles_free(&tl);
     return 0;
 }
 

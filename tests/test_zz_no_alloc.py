@@ -75,7 +75,7 @@ def test_noalloc_rejects_bad_root_and_streamed_graph(env):
     with pytest.raises(gs.GStoreError, match="GS_ERR_ARG"):
         graph.bfs_noalloc(V, out.data_ptr())          # root == V
     graph.free()
-    streamed = ctx.upload_streamed(g["start"], g["grid"], g["degree"], V, segment_bytes=1 << 20)
+    streamed = ctx.upload_streamed(g["start"], g["grid"], g["degree"], V, segment_bytes=2 << 20)
     with pytest.raises(gs.GStoreError, match="GS_ERR_UNSUPPORTED"):
         streamed.bfs_noalloc(0, out.data_ptr())
     streamed.free()
