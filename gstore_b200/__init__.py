@@ -44,6 +44,7 @@ ABI_SYMBOLS = [
     "gs_download", "gs_result_count", "gs_bfs_stats", "gs_pagerank_compat",
     "gs_kron_generate_device", "gs_kron_generate", "gs_convert", "gs_graph_download",
     "gs_bfs_noalloc", "gs_upload_graph_streamed", "gs_upload_graph_file", "gs_stream_stats",
+    "gs_read_tile_files", "gs_upload_graph_files",
     "gs_batch_create", "gs_batch_add", "gs_batch_run", "gs_batch_download", "gs_batch_result_count",
     "gs_batch_bfs_levels", "gs_batch_stats", "gs_batch_free",
     "gs_serve_create", "gs_serve_add_graph", "gs_serve_submit", "gs_serve_step", "gs_serve_poll",
@@ -103,6 +104,8 @@ def lib():
             "gs_upload_graph_streamed": [vp, vp, u64, vp, u64, vp, u64, u64, pvp],
             "gs_upload_graph_file": [vp, vp, u64, C.c_char_p, u64, vp, u64, u64, pvp],
             "gs_stream_stats": [vp, pu64, pu64, pu64, pu64],
+            "gs_read_tile_files": [vp, C.c_char_p, u64, i32, vp, u64, vp, u64, vp, pu64],
+            "gs_upload_graph_files": [vp, C.c_char_p, u64, u64, pvp],
             "gs_batch_create": [vp, pvp],
             "gs_batch_add": [vp, vp, i32, i64, C.POINTER(C.c_int)],
             "gs_batch_run": [vp],
@@ -166,6 +169,29 @@ def read_tile_files(prefix, V: int | None = None, with_degree: bool = True):
     if with_degree and os.path.exists(prefix + ".degree"):
         degree = np.fromfile(prefix + ".degree", np.int32, count=-1 if V is None else V)
     return start, grid, degree
+
+
+def read_tiles(prefix, V: int, directed: bool = False, with_grid: bool = True, ctx=None):
+    """(start, grid, degree) of the tile files at `prefix` through the C ABI
+    (gs_read_tile_files): the single .start/.grid layout, or the per-file
+    .start.N/.grid.N layout of the reference's "-c 3" converter decoded into
+    the single-file .start and record order.  Host-only: needs no GPU."""
+    n = C.c_uint64()
+    pre = str(prefix).encode()
+    h = ctx._h if ctx is not None else None
+
+    def check(st):
+        if st != 0:
+            msg = lib().gs_last_error(h).decode() if h else "see the status"
+            raise GStoreError(st, f"reading {prefix}: {msg}")
+
+    check(lib().gs_read_tile_files(h, pre, V, int(directed), None, 0, None, 0, None, C.byref(n)))
+    start = np.empty(geometry(V, directed)[2], np.uint64)
+    grid = np.empty(n.value if with_grid else 0, np.uint32)
+    degree = np.empty(V, np.int32)
+    check(lib().gs_read_tile_files(h, pre, V, int(directed), _ptr(start), start.size,
+                                   _ptr(grid) if with_grid else None, grid.size, _ptr(degree), C.byref(n)))
+    return start, (grid if with_grid else None), degree
 
 
 def write_tile_files(prefix, start, grid, degree):
@@ -271,6 +297,17 @@ class Context:
         h = C.c_void_p()
         self._check(lib().gs_upload_graph_file(self._h, _ptr(start), start.size, str(grid_path).encode(), n_edges,
                                                _ptr(degree), V, segment_bytes, C.byref(h)))
+        return Graph(self, h)
+
+    def read_tile_files(self, prefix, V: int, with_grid: bool = True):
+        """read_tiles(prefix, V, directed=this context's grid kind)."""
+        return read_tiles(prefix, V, self.directed, with_grid, ctx=self)
+
+    def upload_files(self, prefix, V: int, segment_bytes: int) -> "Graph":
+        """A graph whose records stay in the tile file(s) at `prefix` (either
+        layout) and stream through two HBM segments (gs_upload_graph_files)."""
+        h = C.c_void_p()
+        self._check(lib().gs_upload_graph_files(self._h, str(prefix).encode(), V, segment_bytes, C.byref(h)))
         return Graph(self, h)
 
     def upload_device(self, d_start: int, n_start: int, d_grid: int, n_edges: int, d_degree: int | None,

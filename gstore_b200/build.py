@@ -25,7 +25,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SOURCES = ["gs_api.cu", "gs_sweep.cu", "gs_bfs.cu", "gs_gen.cu", "gs_convert.cu", "gs_noalloc.cu",
                 "gs_stream.cu", "gs_batch.cu",
-                "gs_serve.cu", "gs_pagerank.cu", "gs_pr_blocked.cu"]
+                "gs_serve.cu", "gs_pagerank.cu", "gs_pr_blocked.cu", "gs_files.cpp"]
 HOST_SOURCES = ["gstore_main.cpp", "tilefile.cpp", "algo.cpp"]
 
 

@@ -2,6 +2,8 @@
 // algo_t-style state machine (init / sweep / finalize / download).
 #include "gs_internal.cuh"
 
+#include <sys/stat.h>
+
 #include <algorithm>
 #include <cstring>
 #include <new>
@@ -594,6 +596,35 @@ gs_status gs_upload_graph_file(gs_ctx* ctx, const uint64_t* start, uint64_t n_st
     g->E = n_edges;
     if (st == GS_OK) st = gs_stream_open_file(g, grid_path, segment_bytes);
     if (st == GS_OK) st = finish_upload(g, degree, false);
+    if (st != GS_OK) {
+        free_graph_arrays(g);
+        delete g;
+        return st;
+    }
+    *out = g;
+    return GS_OK;
+}
+
+gs_status gs_upload_graph_files(gs_ctx* ctx, const char* prefix, uint64_t V, uint64_t segment_bytes,
+                                gs_graph** out) {
+    if (!ctx || !prefix || !out) return gs_fail(ctx, GS_ERR_ARG, "null argument");
+    *out = nullptr;
+    gs_tile_layout L;
+    GS_TRY(gs_read_layout(ctx, prefix, V, ctx->directed, &L));
+    // .degree when present (the converters write it), else counted on the device
+    std::vector<int32_t> degree;
+    struct stat sb;
+    if (stat((std::string(prefix) + ".degree").c_str(), &sb) == 0) {
+        degree.resize(V);
+        GS_TRY(gs_read_degree(ctx, prefix, V, degree.data()));
+    }
+    gs_graph* g = nullptr;
+    GS_TRY(new_graph(ctx, V, &g));
+    g->h_start = L.start;
+    gs_status st = check_start(g, L.start.size(), L.start.back());
+    g->E = L.start.back();
+    if (st == GS_OK) st = gs_stream_open_layout(g, L, segment_bytes);
+    if (st == GS_OK) st = finish_upload(g, degree.empty() ? nullptr : degree.data(), false);
     if (st != GS_OK) {
         free_graph_arrays(g);
         delete g;

@@ -351,6 +351,29 @@ gs_status gs_each_part(gs_graph* g, const gs_segment* segs, int n_segs, F launch
                            [](void* a) -> gs_status { return (*static_cast<F*>(a))(); }, &launch);
 }
 gs_status gs_stream_open(gs_graph* g, const uint32_t* host_grid, uint64_t segment_bytes);
+// Where a graph's records lie on disk: records [rec_beg, rec_beg + n) of the
+// file order (the order of one .grid file) sit contiguously at record
+// offset file_rec of file `file`.  One piece for a .grid file; one per
+// (file, group row) for the multi-file layout of "-c 3".
+struct gs_grid_piece {
+    uint64_t rec_beg, n, file_rec;
+    uint32_t file, pad;
+};
+struct gs_tile_layout {
+    std::vector<uint64_t> start;          // the .start of the single-file layout
+    std::vector<std::string> files;
+    std::vector<gs_grid_piece> pieces;    // ascending rec_beg, covering [0, start.back())
+};
+// Reads <prefix>.start / .grid (the single-file layout) or the per-file
+// <prefix>.start.N / .grid.N of "-c 3" (gs_files.cpp).
+gs_status gs_read_layout(gs_ctx* ctx, const std::string& prefix, uint64_t V, int directed, gs_tile_layout* L);
+// Reads `degree` entries (<= V) of <prefix>.degree; missing entries stay 0.
+gs_status gs_read_degree(gs_ctx* ctx, const std::string& prefix, uint64_t V, int32_t* degree);
+// Records [rec, rec + n) of a layout's files into dst.
+bool gs_read_pieces(const std::vector<int>& fds, const std::vector<gs_grid_piece>& pieces, uint32_t* dst,
+                    uint64_t rec, uint64_t n);
+// A graph whose records stay in the files of `L`.
+gs_status gs_stream_open_layout(gs_graph* g, const gs_tile_layout& L, uint64_t segment_bytes);
 void gs_stream_close(gs_graph* g);
 const uint32_t* gs_stream_records(const gs_graph* g);   // host records of a streamed graph (null: file-backed)
 // A graph whose records stream from the .grid file at `path` (from byte 0).

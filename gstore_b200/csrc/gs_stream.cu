@@ -63,7 +63,8 @@ inline uint64_t round4(uint64_t x) { return (x + 3) & ~3ull; }
 struct gs_streamer {
     const uint32_t* h_rec = nullptr;
     bool registered = false;       // cudaHostRegister'ed by the library
-    int fd = -1;                   // file-backed: the .grid file (records from byte 0)
+    std::vector<int> fds;          // file-backed: the layout's files
+    std::vector<gs_grid_piece> pieces;   // file-backed: where each record range lies
     uint32_t* h_stage[2] = {nullptr, nullptr};   // file-backed: pinned staging, one per buffer
     bool staged[2] = {false, false};             // a copy from the staging buffer was queued
     uint64_t seg_records = 0;      // capacity of one segment buffer
@@ -252,14 +253,14 @@ gs_status stage(gs_graph* g, const SegPlan& sp, bool first, int prev, int* out) 
     }
     if (st->used[b]) GS_CHECK_CUDA(ctx, cudaStreamWaitEvent(st->copy, st->freed[b], 0));
     st->content[b].clear();
-    if (st->fd >= 0) {
+    if (!st->fds.empty()) {
         // the staging buffer's previous copy to HBM must be done before the
-        // file is read into it
+        // files are read into it
         if (st->staged[b]) GS_CHECK_CUDA(ctx, cudaEventSynchronize(st->ready[b]));
         uint64_t extent = 0;
         for (const CopyOp& c : sp.copies) {
-            if (!pread_full(st->fd, st->h_stage[b] + c.dst, c.n * 4, c.src * 4))
-                return gs_fail(ctx, GS_ERR_FORMAT, "reading the .grid file failed at record " + std::to_string(c.src));
+            if (!gs_read_pieces(st->fds, st->pieces, st->h_stage[b] + c.dst, c.src, c.n))
+                return gs_fail(ctx, GS_ERR_FORMAT, "reading the grid files failed at record " + std::to_string(c.src));
             extent = std::max(extent, c.dst + c.n);
             st->bytes += c.n * 4;
         }
@@ -415,7 +416,28 @@ gs_status open_buffers(gs_graph* g, gs_streamer* st) {
 
 }  // namespace
 
-gs_status gs_stream_open_file(gs_graph* g, const char* path, uint64_t segment_bytes) {
+bool gs_read_pieces(const std::vector<int>& fds, const std::vector<gs_grid_piece>& pieces, uint32_t* dst,
+                    uint64_t rec, uint64_t n) {
+    // the first piece holding `rec` (pieces are sorted by rec_beg)
+    size_t lo = 0, hi = pieces.size();
+    while (lo < hi) {
+        const size_t mid = (lo + hi) / 2;
+        if (pieces[mid].rec_beg + pieces[mid].n <= rec) lo = mid + 1;
+        else hi = mid;
+    }
+    for (size_t i = lo; n > 0; ++i) {
+        if (i >= pieces.size() || pieces[i].rec_beg > rec) return false;
+        const gs_grid_piece& p = pieces[i];
+        const uint64_t k = std::min<uint64_t>(n, p.rec_beg + p.n - rec);
+        if (!pread_full(fds[p.file], dst, k * 4, (p.file_rec + (rec - p.rec_beg)) * 4)) return false;
+        dst += k;
+        rec += k;
+        n -= k;
+    }
+    return true;
+}
+
+gs_status gs_stream_open_layout(gs_graph* g, const gs_tile_layout& L, uint64_t segment_bytes) {
     gs_ctx* ctx = g->ctx;
     const uint64_t min_bytes = 2 * (kRunRecords + 8) * 4;
     if (segment_bytes < min_bytes)
@@ -424,20 +446,33 @@ gs_status gs_stream_open_file(gs_graph* g, const char* path, uint64_t segment_by
     if (!st) return GS_ERR_OOM;
     g->stream = st;
     st->seg_records = (segment_bytes / 4) & ~3ull;
-    st->fd = open(path, O_RDONLY);
-    if (st->fd < 0) return gs_fail(ctx, GS_ERR_ARG, std::string("cannot open ") + path);
-    struct stat sb;
-    if (fstat(st->fd, &sb) != 0 || (uint64_t)sb.st_size < g->E * 4)
-        return gs_fail(ctx, GS_ERR_FORMAT, std::string(path) + " holds fewer than the records .start counts");
+    st->pieces = L.pieces;
+    for (const std::string& path : L.files) {
+        const int fd = open(path.c_str(), O_RDONLY);
+        if (fd < 0) return gs_fail(ctx, GS_ERR_ARG, "cannot open " + path);
+        st->fds.push_back(fd);
+    }
+    for (const gs_grid_piece& p : L.pieces) {
+        struct stat sb;
+        if (fstat(st->fds[p.file], &sb) != 0 || (uint64_t)sb.st_size < (p.file_rec + p.n) * 4)
+            return gs_fail(ctx, GS_ERR_FORMAT, L.files[p.file] + " holds fewer than the records .start counts");
+    }
     for (int b = 0; b < 2; ++b)
         GS_CHECK_CUDA(ctx, cudaHostAlloc((void**)&st->h_stage[b], st->seg_records * 4 + 16, cudaHostAllocDefault));
     return open_buffers(g, st);
 }
 
+gs_status gs_stream_open_file(gs_graph* g, const char* path, uint64_t segment_bytes) {
+    gs_tile_layout L;
+    L.files.push_back(path);
+    if (g->E) L.pieces.push_back(gs_grid_piece{0, g->E, 0, 0, 0});
+    return gs_stream_open_layout(g, L, segment_bytes);
+}
+
 bool gs_stream_read_records(const gs_graph* g, uint32_t* dst) {
     const gs_streamer* st = g->stream;
     if (!st) return false;
-    if (st->fd >= 0) return pread_full(st->fd, dst, g->E * 4, 0);
+    if (!st->fds.empty()) return g->E == 0 || gs_read_pieces(st->fds, st->pieces, dst, 0, g->E);
     std::memcpy(dst, st->h_rec, g->E * 4);
     return true;
 }
@@ -485,7 +520,7 @@ void gs_stream_close(gs_graph* g) {
         if (st->registered) cudaHostUnregister((void*)st->h_rec);
         for (int b = 0; b < 2; ++b)
             if (st->h_stage[b]) cudaFreeHost(st->h_stage[b]);
-        if (st->fd >= 0) close(st->fd);
+        for (int fd : st->fds) close(fd);
         delete st;
         g->stream = nullptr;
     }

@@ -54,10 +54,35 @@ struct options {
     uint64_t total_size = 8192ull << 20;   // -m default, gstore.cpp:79
 };
 
+// The multi-file layout of "-c 3" (<prefix>.grid.N / .start.N): no
+// <prefix>.grid, but a <prefix>.grid.0.
+static bool multi_file_layout(const options& o) {
+    uint64_t b = 0;
+    return !tile_file_size(o.edgefile + ".grid", &b).empty() && tile_file_size(o.edgefile + ".grid.0", &b).empty();
+}
+
 static int read_graph_files(const options& o, bool want_degree, bool want_grid, tile_files* tf) {
     uint32_t p, ps;
     uint64_t n_start;
     gs_geometry(o.vert_count, kDirected, &p, &ps, &n_start);
+    if (multi_file_layout(o)) {
+        // decoded by the engine library into the single-file .start and order
+        uint64_t n = 0;
+        tf->start.resize(n_start);
+        if (gs_read_tile_files(nullptr, o.edgefile.c_str(), o.vert_count, kDirected, tf->start.data(), n_start,
+                               nullptr, 0, nullptr, &n) != GS_OK)
+            return fail(nullptr, "reading the multi-file layout " + o.edgefile + ".start.N / .grid.N");
+        tf->grid.clear();
+        tf->degree.clear();
+        if (want_grid) tf->grid.resize(n);
+        if (want_degree) tf->degree.resize(o.vert_count);
+        if ((want_grid || want_degree) &&
+            gs_read_tile_files(nullptr, o.edgefile.c_str(), o.vert_count, kDirected, nullptr, 0,
+                               want_grid ? tf->grid.data() : nullptr, n,
+                               want_degree ? tf->degree.data() : nullptr, &n) != GS_OK)
+            return fail(nullptr, "reading the multi-file layout " + o.edgefile + ".grid.N");
+        return 0;
+    }
     std::string err = read_tile_files(o.edgefile, n_start, o.vert_count, want_degree, tf, want_grid);
     if (!err.empty()) return fail(nullptr, err);
     return 0;
@@ -70,7 +95,9 @@ static int upload_graph(gs_ctx* ctx, const options& o, const tile_files& tf, boo
                         gs_graph** g) {
     const int32_t* degree = want_degree ? tf.degree.data() : nullptr;
     gs_status st;
-    if (tf.grid.empty() && tf.start.back() > 0)
+    if (tf.grid.empty() && tf.start.back() > 0 && multi_file_layout(o))
+        st = gs_upload_graph_files(ctx, o.edgefile.c_str(), o.vert_count, (budget / 2) & ~15ull, g);
+    else if (tf.grid.empty() && tf.start.back() > 0)
         st = gs_upload_graph_file(ctx, tf.start.data(), tf.start.size(), (o.edgefile + ".grid").c_str(),
                                   tf.start.back(), degree, o.vert_count, (budget / 2) & ~15ull, g);
     else
@@ -282,7 +309,15 @@ int main(int argc, char* argv[]) {
     // in-memory jobs (1x, 2x) keep the grid resident.
     const uint64_t budget = (job < 10 || job == 30) ? o.total_size : 0;
     uint64_t grid_bytes = 0;
-    const bool on_disk = budget && tile_file_size(o.edgefile + ".grid", &grid_bytes).empty() && grid_bytes > budget;
+    if (multi_file_layout(o)) {
+        if (gs_read_tile_files(nullptr, o.edgefile.c_str(), o.vert_count, kDirected, nullptr, 0, nullptr, 0, nullptr,
+                               &grid_bytes) != GS_OK)
+            return fail(nullptr, "reading the multi-file layout " + o.edgefile + ".start.N / .grid.N");
+        grid_bytes *= 4;
+    } else if (!tile_file_size(o.edgefile + ".grid", &grid_bytes).empty()) {
+        grid_bytes = 0;
+    }
+    const bool on_disk = budget && grid_bytes > budget;
     tile_files tf;
     int rc = read_graph_files(o, want_degree, !on_disk, &tf);
     if (rc) return rc;

@@ -135,6 +135,31 @@ gs_status gs_upload_graph_streamed(gs_ctx* ctx, const uint64_t* start, uint64_t 
 gs_status gs_upload_graph_file(gs_ctx* ctx, const uint64_t* start, uint64_t n_start, const char* grid_path,
                                uint64_t n_edges, const int32_t* degree, uint64_t V, uint64_t segment_bytes,
                                gs_graph** out);
+
+/* Replaces: read_start_in_mem + read_grid_in_mem + read_degree_in_mem
+ * (gstore.cpp:2953-3011, 3799-3813) for both layouts the reference's
+ * converters write: the single <prefix>.start / <prefix>.grid of "-c 1" and
+ * "-c 2", and the directory layout of "-c 3" -- <prefix>.start.N and
+ * <prefix>.grid.N per block of file groups (grid::post_grid_dir,
+ * save_start_files(is_odir), gstore.cpp:688-879, 2837-2898), which the
+ * reference writes but never reads back.  Their per-file .start.N entries
+ * (a running sum of per-row prefix sums) are decoded back to tile counts.
+ * Fills start[n_start] (the single-file .start; n_start from gs_geometry),
+ * grid[grid_capacity] with the records in single-file order, and degree[V]
+ * (.degree, zero past its end); each may be NULL.  *n_edges: the record
+ * count.  directed: the full grid of gstored, else the half grid.  No device
+ * work: ctx may be NULL (then only the status reports a failure). */
+gs_status gs_read_tile_files(gs_ctx* ctx, const char* prefix, uint64_t V, int directed, uint64_t* start,
+                             uint64_t n_start, uint32_t* grid, uint64_t grid_capacity, int32_t* degree,
+                             uint64_t* n_edges);
+
+/* Replaces: read_aio_init + read_degree_in_mem (gstore.cpp:3044-3119,
+ * 2971-3011) over either layout: a graph whose records stay in the file(s)
+ * at `prefix` and stream through two HBM segments of segment_bytes each, as
+ * gs_upload_graph_file does for one .grid file.  <prefix>.degree is read when
+ * present, else the degrees are counted from the records. */
+gs_status gs_upload_graph_files(gs_ctx* ctx, const char* prefix, uint64_t V, uint64_t segment_bytes,
+                                gs_graph** out);
 /* Host-to-device traffic of a streamed graph since upload: bytes copied,
  * cudaMemcpyAsync calls, segments swept, segments found already in HBM
  * (all 0 for a resident graph). */
