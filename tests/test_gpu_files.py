@@ -61,6 +61,6 @@ def test_cli_reads_multi_file_layout(reference_layouts):
     pat_k, pat_w = r">= 8vertices count = (\d+)", r"WCC count = (\d+)"
     want_k = re.search(pat_k, run(ref, "-s", 26, "-j", 22, "-a", 8, "-i", single)).group(1)
     want_w = re.search(pat_w, run(ref, "-s", 26, "-j", 23, "-i", single)).group(1)
-    for j_k, j_w, extra in ((22, 23, []), (2, 3, ["-m", 2])):
+    for j_k, j_w, extra in ((22, 23, []), (2, 3, ["-m", 3])):
         assert re.search(pat_k, run(ours, "-s", 26, "-j", j_k, "-a", 8, "-i", multi, *extra)).group(1) == want_k
         assert re.search(pat_w, run(ours, "-s", 26, "-j", j_w, "-i", multi, *extra)).group(1) == want_w
