@@ -67,9 +67,15 @@ __device__ __forceinline__ void warp_add_u64(unsigned long long* dst, uint64_t v
 }
 
 // --------------------------------------------------------------- PageRank --
+// Acc: the type of the sums in y.  The sweep of a streamed graph adds in
+// double: its per-record atomics reach high-degree vertices in file order,
+// one add per record, and FP32 sums drift past the 1e-6 tolerance at
+// Kronecker scale 28; that sweep waits on PCIe, so the wider adds cost no
+// time.  x stays FP32.
+template <class Acc>
 struct PrOp {
     const float* x;
-    float* y;
+    Acc* y;
     int directed;
     // Tiles sorted by v1 (the device converter's order) give runs of equal
     // column ends per lane: one add to y per run (fewer atomics, shorter
@@ -77,15 +83,15 @@ struct PrOp {
     struct Item {
         uint32_t rb, cb;
         uint32_t pb;     // column end of the open run, ~0 = none
-        float xb;        // x[pb]
-        float sum;       // sum of x[a] over the open run
+        Acc xb;          // x[pb]
+        Acc sum;         // sum of x[a] over the open run
     };
     __device__ bool begin(uint32_t row, uint32_t col, Item& c) const {
         c.rb = row << 16;
         c.cb = col << 16;
         c.pb = ~0u;
-        c.xb = 0.f;
-        c.sum = 0.f;
+        c.xb = 0;
+        c.sum = 0;
         return true;
     }
     __device__ void record(uint32_t r, Item& c) const {
@@ -93,10 +99,10 @@ struct PrOp {
         if (b != c.pb) {
             if (c.pb != ~0u) atomicAdd(y + c.pb, c.sum);   // pr.cpp:145-146
             c.pb = b;
-            c.sum = 0.f;
-            if (!directed) c.xb = __ldg(x + b);
+            c.sum = 0;
+            if (!directed) c.xb = (Acc)__ldg(x + b);
         }
-        c.sum += __ldg(x + a);
+        c.sum += (Acc)__ldg(x + a);
         if (!directed) atomicAdd(y + a, c.xb);             // pr.cpp:147-150
     }
     __device__ void end(uint32_t, uint32_t, Item& c) const {

@@ -172,7 +172,8 @@ __global__ void pr_init_kernel(float* x, float* y, uint64_t N, uint64_t V) {
 // rank = 0.15 + 0.85 s; x = rank * inv_degree; s := 0 (pr.cpp:281-302).  The
 // expression is evaluated in double as the reference does (double literals)
 // and stored as float.
-__global__ void pr_finalize_kernel(float* __restrict__ x, float* __restrict__ y, float* __restrict__ r_out,
+template <class Acc>
+__global__ void pr_finalize_kernel(float* __restrict__ x, Acc* __restrict__ y, float* __restrict__ r_out,
                                    const int32_t* __restrict__ deg, uint64_t N, uint64_t V, int compat) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
@@ -185,7 +186,7 @@ __global__ void pr_finalize_kernel(float* __restrict__ x, float* __restrict__ y,
         else xn = r / (double)d;
         r_out[v] = v < V ? (float)r : 0.f;
         x[v] = (float)xn;
-        y[v] = 0.f;
+        y[v] = 0;
     }
 }
 
@@ -413,9 +414,11 @@ gs_status pr_init(gs_state* s) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
     if (!s->d_x) GS_TRY(gs_state_alloc(s, (void**)&s->d_x, g->N * 4));
-    if (!s->d_y) GS_TRY(gs_state_alloc(s, (void**)&s->d_y, g->N * 4));
+    // the sums of a streamed graph's sweep are doubles (PrOp<double>)
+    if (!s->d_y) GS_TRY(gs_state_alloc(s, (void**)&s->d_y, g->N * (g->stream ? 8 : 4)));
     if (!s->d_r) GS_TRY(gs_state_alloc(s, (void**)&s->d_r, g->N * 4));
     pr_init_kernel<<<blocks_for(g->N, ctx), kThreads, 0, ctx->stream>>>(s->d_x, s->d_y, g->N, g->V);
+    if (g->stream) GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_y, 0, g->N * 8, ctx->stream));
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_r, 0, g->N * 4, ctx->stream));
@@ -433,14 +436,18 @@ gs_status pr_sweep_launch(gs_state* s) {
     gs_graph* g = s->g;
     if (!g->seg.list && g->pb.built) return pb_launch(s);
     if (!g->seg.list && g->pr.built) return pr_slice_launch(s);
-    PrOp op{s->d_x, s->d_y, g->directed};
+    if (g->stream) {
+        PrOp<double> op{s->d_x, reinterpret_cast<double*>(s->d_y), g->directed};
+        return launch_sweep(g, op, GS_ALGO_PAGERANK, 4 * g->E + 12 * g->V, true);
+    }
+    PrOp<float> op{s->d_x, s->d_y, g->directed};
     // algorithmic bytes per iteration: 4E + 12V (records, x, s, inv)
     return launch_sweep(g, op, GS_ALGO_PAGERANK, 4 * g->E + 12 * g->V, true);
 }
 
 gs_status pr_finalize_launch(gs_ctx* ctx, cudaStream_t stream, float* x, float* y, float* r, const int32_t* deg,
                              uint64_t N, uint64_t V, int compat) {
-    pr_finalize_kernel<<<blocks_for(N, ctx), kThreads, 0, stream>>>(x, y, r, deg, N, V, compat);
+    pr_finalize_kernel<float><<<blocks_for(N, ctx), kThreads, 0, stream>>>(x, y, r, deg, N, V, compat);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
     return GS_OK;
@@ -449,8 +456,12 @@ gs_status pr_finalize_launch(gs_ctx* ctx, cudaStream_t stream, float* x, float* 
 gs_status pr_finalize(gs_state* s, int64_t* frontier, int* done) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
-    pr_finalize_kernel<<<blocks_for(g->N, ctx), kThreads, 0, ctx->stream>>>(
-        s->d_x, s->d_y, s->d_r, g->d_degree, g->N, g->V, s->compat ? 1 : 0);
+    if (g->stream)
+        pr_finalize_kernel<double><<<blocks_for(g->N, ctx), kThreads, 0, ctx->stream>>>(
+            s->d_x, reinterpret_cast<double*>(s->d_y), s->d_r, g->d_degree, g->N, g->V, s->compat ? 1 : 0);
+    else
+        pr_finalize_kernel<float><<<blocks_for(g->N, ctx), kThreads, 0, ctx->stream>>>(
+            s->d_x, s->d_y, s->d_r, g->d_degree, g->N, g->V, s->compat ? 1 : 0);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
     *frontier = s->step;
