@@ -23,7 +23,8 @@
 //   * accumulate (pass 2): a CTA owns one destination bin (32,768 floats,
 //     128 KB of shared memory), walks the bin's blocks (one per source slice,
 //     D-major block table) and adds val[e] into its shared-memory sums at
-//     the destination offset, then writes the bin's sums to y.
+//     the destination offset (a lane merges equal destinations among its 8
+//     consecutive entries first), then writes the bin's sums to y.
 //
 // Both passes stream; the random accesses stay in shared memory.  DRAM bytes
 // per entry and sweep: 2 (source offset) + 4 + 4 (value written and read) +
@@ -44,7 +45,6 @@ constexpr int kKeyLowBits = kPbSrcBits + kPbDstBits;
 constexpr int kGatherThreads = 512;
 constexpr int kAccThreads = 1024;
 constexpr long long kWaitLimit = 1ll << 24;
-constexpr unsigned gsops_full_mask = 0xFFFFFFFFu;
 
 struct __align__(128) GatherSmem {
     float xs[kSrcSlice];
@@ -153,7 +153,6 @@ __global__ void __launch_bounds__(kAccThreads, 1)
     float* acc = reinterpret_cast<float*>(smem_raw);
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     constexpr uint32_t kWarps = kAccThreads / 32;
-    constexpr int kU = 8;   // entries in flight per lane
     __shared__ unsigned long long s_item;
     auto advance = [&](uint64_t i) -> uint64_t {
         if (!ticket) return i + gridDim.x;
@@ -169,32 +168,38 @@ __global__ void __launch_bounds__(kAccThreads, 1)
         __syncthreads();
         for (uint32_t bi = it.b0 + warp; bi < it.b1; bi += kWarps) {
             const gs_pb_block blk = blocks[bi];
-            for (uint32_t k0 = 0; k0 < blk.n; k0 += 32 * kU) {   // warp-uniform: the shuffles need every lane
-                const uint32_t k = k0 + lane;
-                uint32_t d[kU];
-                float v[kU];
+            const uint64_t e0 = blk.e0, e1 = blk.e0 + blk.n;
+            // head up to a multiple of 8 entries and tail: one entry per lane
+            const uint64_t a = ((e0 + 7) & ~7ull) < e1 ? ((e0 + 7) & ~7ull) : e1;
+            const uint64_t b = (e1 & ~7ull) > a ? (e1 & ~7ull) : a;
+            if (e0 + lane < a) atomicAdd(acc + __ldcs(dst + e0 + lane), __ldcs(val + e0 + lane));
+            if (b + lane < e1) atomicAdd(acc + __ldcs(dst + b + lane), __ldcs(val + b + lane));
+            // body: a lane takes 8 consecutive entries (one 16-byte load of
+            // offsets, two of values).  They are sorted by destination, so
+            // equal destinations are adjacent: the lane sums each run in a
+            // register and adds it once (fewer shared atomics on
+            // high-degree vertices, shorter FP32 chains).
+            const uint4* d8 = reinterpret_cast<const uint4*>(dst);
+            const float4* v4 = reinterpret_cast<const float4*>(val);
+            for (uint64_t c = (a >> 3) + lane; c < (b >> 3); c += 32) {
+                const uint4 d = __ldcs(d8 + c);
+                const float4 lo = __ldcs(v4 + 2 * c), hi = __ldcs(v4 + 2 * c + 1);
+                const uint32_t o[8] = {d.x & 0xFFFFu, d.x >> 16, d.y & 0xFFFFu, d.y >> 16,
+                                       d.z & 0xFFFFu, d.z >> 16, d.w & 0xFFFFu, d.w >> 16};
+                const float v[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+                uint32_t cur = o[0];
+                float sum = v[0];
 #pragma unroll
-                for (int j = 0; j < kU; ++j) {
-                    const uint32_t q = k + 32u * j;
-                    d[j] = q < blk.n ? __ldcs(dst + blk.e0 + q) : ~0u - lane;   // past the end: distinct keys
-                    v[j] = q < blk.n ? __ldcs(val + blk.e0 + q) : 0.f;
-                }
-#pragma unroll
-                for (int j = 0; j < kU; ++j) {
-                    // 32 consecutive entries, sorted by destination: equal
-                    // destinations sit in adjacent lanes.  Sum each run as a
-                    // tree (segmented suffix sums) and add it once: fewer
-                    // atomics on high-degree vertices and shorter FP32 chains.
-                    float t = v[j];
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const float to = __shfl_down_sync(gsops_full_mask, t, o);
-                        const uint32_t dd = __shfl_down_sync(gsops_full_mask, d[j], o);
-                        if (lane + o < 32 && dd == d[j]) t += to;
+                for (int j = 1; j < 8; ++j) {
+                    if (o[j] == cur) {
+                        sum += v[j];
+                    } else {
+                        atomicAdd(acc + cur, sum);
+                        cur = o[j];
+                        sum = v[j];
                     }
-                    const uint32_t dp = __shfl_up_sync(gsops_full_mask, d[j], 1);
-                    if ((lane == 0 || dp != d[j]) && d[j] < kDstBin) atomicAdd(acc + d[j], t);
                 }
+                atomicAdd(acc + cur, sum);
             }
         }
         __syncthreads();
