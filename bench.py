@@ -1168,22 +1168,24 @@ def main():
         graph.free()
         torch.cuda.empty_cache()
 
-        parts = {"upload": [], "bfs": [], "download": [], "free": [], "step": []}
+        parts = {"upload": [], "bfs": [], "download": [], "state_free": [], "graph_free": [], "step": []}
 
         def e2e_step(root):
             t_a = time.perf_counter()
             g2 = ctx.upload(pin_start.numpy().view(np.uint64), pin_grid.numpy().view(np.uint32),
                             pin_deg.numpy(), V)
             t_b = time.perf_counter()
-            with g2.state("bfs", root) as s:
-                s.run()
-                t_c = time.perf_counter()
-                s.download_into(depth_out.numpy())
-                t_d = time.perf_counter()
-            g2.free()
+            s = g2.state("bfs", root)
+            s.run()
+            t_c = time.perf_counter()
+            s.download_into(depth_out.numpy())
+            t_d = time.perf_counter()
+            s.free()
             t_e = time.perf_counter()
-            for k, a, b in (("upload", t_a, t_b), ("bfs", t_b, t_c), ("download", t_c, t_d), ("free", t_d, t_e),
-                            ("step", t_a, t_e)):
+            g2.free()
+            t_f = time.perf_counter()
+            for k, a, b in (("upload", t_a, t_b), ("bfs", t_b, t_c), ("download", t_c, t_d), ("state_free", t_d, t_e),
+                            ("graph_free", t_e, t_f), ("step", t_a, t_f)):
                 parts[k].append((b - a) * 1e3)
 
         e2e_step(timed_roots[0])

@@ -43,7 +43,11 @@ constexpr uint32_t kSrcSlice = 1u << kPbSrcBits;   // 16,384
 constexpr uint32_t kDstBin = 1u << kPbDstBits;     // 32,768
 constexpr int kKeyLowBits = kPbSrcBits + kPbDstBits;
 constexpr int kGatherThreads = 512;
+constexpr int kGatherCtas = 3;       // resident gather CTAs per SM (64 KB of x each)
+constexpr int kGatherGroups = 2;     // 8-entry groups in flight per gather thread
 constexpr int kAccThreads = 1024;
+constexpr int kAccCtas = 1;          // resident accumulate CTAs per SM (the bin's sums each)
+constexpr int kAccGroups = 2;        // 8-entry groups in flight per accumulate lane
 constexpr long long kWaitLimit = 1ll << 24;
 
 struct __align__(128) GatherSmem {
@@ -68,7 +72,7 @@ __device__ __forceinline__ bool wait_bar(unsigned long long* bar, uint32_t parit
 }
 
 // Pass 1.  Item: entries [e0, e0 + n) of source slice `slice`.
-__global__ void __launch_bounds__(kGatherThreads, 3)
+__global__ void __launch_bounds__(kGatherThreads, kGatherCtas)
     pb_gather_kernel(const gs_pb_item1* __restrict__ items, uint64_t n_items, const uint16_t* __restrict__ src,
                      const float* __restrict__ x, float* __restrict__ val, int* error, unsigned int* ticket) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -117,22 +121,23 @@ __global__ void __launch_bounds__(kGatherThreads, 3)
         const uint4* s8 = reinterpret_cast<const uint4*>(src);
         float4* v4 = reinterpret_cast<float4*>(val);
         const uint64_t c1 = b >> 3;
-        uint64_t c = (a >> 3) + tid;
-        for (; c + kGatherThreads < c1; c += 2 * kGatherThreads) {
-            const uint4 w0 = __ldcs(s8 + c), w1 = __ldcs(s8 + c + kGatherThreads);
-            v4[2 * c] = make_float4(m.xs[w0.x & 0xFFFFu], m.xs[w0.x >> 16], m.xs[w0.y & 0xFFFFu], m.xs[w0.y >> 16]);
-            v4[2 * c + 1] =
-                make_float4(m.xs[w0.z & 0xFFFFu], m.xs[w0.z >> 16], m.xs[w0.w & 0xFFFFu], m.xs[w0.w >> 16]);
-            const uint64_t d = c + kGatherThreads;
-            v4[2 * d] = make_float4(m.xs[w1.x & 0xFFFFu], m.xs[w1.x >> 16], m.xs[w1.y & 0xFFFFu], m.xs[w1.y >> 16]);
-            v4[2 * d + 1] =
-                make_float4(m.xs[w1.z & 0xFFFFu], m.xs[w1.z >> 16], m.xs[w1.w & 0xFFFFu], m.xs[w1.w >> 16]);
-        }
-        if (c < c1) {
-            const uint4 w0 = __ldcs(s8 + c);
-            v4[2 * c] = make_float4(m.xs[w0.x & 0xFFFFu], m.xs[w0.x >> 16], m.xs[w0.y & 0xFFFFu], m.xs[w0.y >> 16]);
-            v4[2 * c + 1] =
-                make_float4(m.xs[w0.z & 0xFFFFu], m.xs[w0.z >> 16], m.xs[w0.w & 0xFFFFu], m.xs[w0.w >> 16]);
+        for (uint64_t c = (a >> 3) + tid; c < c1; c += (uint64_t)kGatherThreads * kGatherGroups) {
+            uint4 w[kGatherGroups];
+#pragma unroll
+            for (int k = 0; k < kGatherGroups; ++k) {
+                const uint64_t ck = c + (uint64_t)k * kGatherThreads;
+                if (ck < c1) w[k] = __ldcs(s8 + ck);
+            }
+#pragma unroll
+            for (int k = 0; k < kGatherGroups; ++k) {
+                const uint64_t ck = c + (uint64_t)k * kGatherThreads;
+                if (ck < c1) {
+                    v4[2 * ck] = make_float4(m.xs[w[k].x & 0xFFFFu], m.xs[w[k].x >> 16], m.xs[w[k].y & 0xFFFFu],
+                                             m.xs[w[k].y >> 16]);
+                    v4[2 * ck + 1] = make_float4(m.xs[w[k].z & 0xFFFFu], m.xs[w[k].z >> 16],
+                                                 m.xs[w[k].w & 0xFFFFu], m.xs[w[k].w >> 16]);
+                }
+            }
         }
         __syncthreads();   // xs is rewritten by the next item
     }
@@ -142,10 +147,25 @@ __global__ void __launch_bounds__(kGatherThreads, 3)
     }
 }
 
+// Adds one lane's 8 consecutive entries, sorted by destination, into the
+// shared sums: each run of equal destinations is summed in registers
+// (suffix sums, no branches) and added once, by its first entry -- fewer
+// shared atomics on high-degree vertices and shorter FP32 chains.
+__device__ __forceinline__ void add_group(float* acc, const uint4 d, const float4 lo, const float4 hi) {
+    const uint32_t o[8] = {d.x & 0xFFFFu, d.x >> 16, d.y & 0xFFFFu, d.y >> 16,
+                           d.z & 0xFFFFu, d.z >> 16, d.w & 0xFFFFu, d.w >> 16};
+    float v[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+#pragma unroll
+    for (int j = 6; j >= 0; --j) v[j] += o[j] == o[j + 1] ? v[j + 1] : 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        if (j == 0 || o[j] != o[j - 1]) atomicAdd(acc + o[j], v[j]);
+}
+
 // Pass 2.  Item: blocks [b0, b1) of the D-major block table, all of bin
 // `bin`; `whole` when the item holds every block of the bin (its sums are
 // then stored, else added to y).
-__global__ void __launch_bounds__(kAccThreads, 1)
+__global__ void __launch_bounds__(kAccThreads, kAccCtas)
     pb_accumulate_kernel(const gs_pb_item2* __restrict__ items, uint64_t n_items,
                          const gs_pb_block* __restrict__ blocks, const uint16_t* __restrict__ dst,
                          const float* __restrict__ val, float* __restrict__ y, unsigned int* ticket) {
@@ -175,31 +195,25 @@ __global__ void __launch_bounds__(kAccThreads, 1)
             if (e0 + lane < a) atomicAdd(acc + __ldcs(dst + e0 + lane), __ldcs(val + e0 + lane));
             if (b + lane < e1) atomicAdd(acc + __ldcs(dst + b + lane), __ldcs(val + b + lane));
             // body: a lane takes 8 consecutive entries (one 16-byte load of
-            // offsets, two of values).  They are sorted by destination, so
-            // equal destinations are adjacent: the lane sums each run in a
-            // register and adds it once (fewer shared atomics on
-            // high-degree vertices, shorter FP32 chains).
+            // offsets, two of values), kAccGroups of them in flight
             const uint4* d8 = reinterpret_cast<const uint4*>(dst);
             const float4* v4 = reinterpret_cast<const float4*>(val);
-            for (uint64_t c = (a >> 3) + lane; c < (b >> 3); c += 32) {
-                const uint4 d = __ldcs(d8 + c);
-                const float4 lo = __ldcs(v4 + 2 * c), hi = __ldcs(v4 + 2 * c + 1);
-                const uint32_t o[8] = {d.x & 0xFFFFu, d.x >> 16, d.y & 0xFFFFu, d.y >> 16,
-                                       d.z & 0xFFFFu, d.z >> 16, d.w & 0xFFFFu, d.w >> 16};
-                const float v[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
-                uint32_t cur = o[0];
-                float sum = v[0];
+            const uint64_t cb = b >> 3;
+            for (uint64_t c = (a >> 3) + lane; c < cb; c += 32 * kAccGroups) {
+                uint4 d[kAccGroups];
+                float4 lo[kAccGroups], hi[kAccGroups];
 #pragma unroll
-                for (int j = 1; j < 8; ++j) {
-                    if (o[j] == cur) {
-                        sum += v[j];
-                    } else {
-                        atomicAdd(acc + cur, sum);
-                        cur = o[j];
-                        sum = v[j];
+                for (int k = 0; k < kAccGroups; ++k) {
+                    const uint64_t ck = c + 32u * k;
+                    if (ck < cb) {
+                        d[k] = __ldcs(d8 + ck);
+                        lo[k] = __ldcs(v4 + 2 * ck);
+                        hi[k] = __ldcs(v4 + 2 * ck + 1);
                     }
                 }
-                atomicAdd(acc + cur, sum);
+#pragma unroll
+                for (int k = 0; k < kAccGroups; ++k)
+                    if (c + 32u * k < cb) add_group(acc, d[k], lo[k], hi[k]);
             }
         }
         __syncthreads();
@@ -385,8 +399,9 @@ gs_status pb_layout_build(gs_graph* g) {
     }
     // Items: entry chunks of every slice (pass 1) and block ranges of every
     // bin (pass 2), sized so that each pass has a few items per resident CTA.
-    const uint64_t per1 = std::clamp<uint64_t>(n_ent / ((uint64_t)ctx->num_sms * 12), 32768, 1ull << 20);
-    const uint64_t per2 = std::clamp<uint64_t>(n_ent / ((uint64_t)ctx->num_sms * 4), 65536, 1ull << 22);
+    const uint64_t per1 =
+        std::clamp<uint64_t>(n_ent / ((uint64_t)ctx->num_sms * kGatherCtas * 4), 32768, 1ull << 20);
+    const uint64_t per2 = std::clamp<uint64_t>(n_ent / ((uint64_t)ctx->num_sms * kAccCtas * 4), 65536, 1ull << 22);
     std::vector<gs_pb_item1> items1;
     for (uint32_t s = 0; s < nS; ++s)
         for (uint64_t e = slice_start[s]; e < slice_start[s + 1]; e += per1)
@@ -438,11 +453,11 @@ gs_status pb_sweep(gs_graph* g, const float* x, float* y, int* error) {
     if (L.n_items1 == 0) return GS_OK;
     GS_CHECK_CUDA(ctx, gs_smem_limit_once<pb_gather_kernel>(ctx->device, (int)sizeof(GatherSmem)));
     GS_CHECK_CUDA(ctx, gs_smem_limit_once<pb_accumulate_kernel>(ctx->device, (int)(kDstBin * 4)));
-    const uint32_t g1 = (uint32_t)std::min<uint64_t>(L.n_items1, gs_grid_size(ctx, 3));
+    const uint32_t g1 = (uint32_t)std::min<uint64_t>(L.n_items1, gs_grid_size(ctx, kGatherCtas));
     pb_gather_kernel<<<g1, kGatherThreads, sizeof(GatherSmem), ctx->stream>>>(L.d_items1, L.n_items1, L.d_src, x,
                                                                              L.d_val, error, ctx->d_ticket + 4);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
-    const uint32_t g2 = (uint32_t)std::min<uint64_t>(L.n_items2, gs_grid_size(ctx, 1));
+    const uint32_t g2 = (uint32_t)std::min<uint64_t>(L.n_items2, gs_grid_size(ctx, kAccCtas));
     pb_accumulate_kernel<<<g2, kAccThreads, kDstBin * 4, ctx->stream>>>(L.d_items2, L.n_items2, L.d_blocks, L.d_dst,
                                                                        L.d_val, y, ctx->d_ticket + 6);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
