@@ -877,7 +877,7 @@ def bench_served(ctx, torch, gs, seconds: float):
         st = srv.stats()
         res["served"] = summarize(lat, t_end, len(lat))
         res["served"].update({"steps": st["steps"], "graph_launches": st["graph_launches"],
-                              "kernel_launches": st["kernel_launches"]})
+                              "kernel_launches": st["kernel_launches"], "host_phases_s": srv.profile()})
 
     def plain_loop(cache: bool):
         # one request at a time in arrival order (bounded: at most 120 s);

@@ -49,7 +49,7 @@ ABI_SYMBOLS = [
     "gs_batch_bfs_levels", "gs_batch_stats", "gs_batch_free",
     "gs_serve_create", "gs_serve_add_graph", "gs_serve_submit", "gs_serve_step", "gs_serve_poll",
     "gs_serve_result", "gs_serve_clock", "gs_serve_stats", "gs_serve_free", "gs_serve_completed",
-    "gs_serve_set_side_streams", "gs_serve_result_view", "gs_serve_release",
+    "gs_serve_set_side_streams", "gs_serve_result_view", "gs_serve_release", "gs_serve_profile",
 ]
 
 
@@ -129,6 +129,7 @@ def lib():
             "gs_serve_result_view": [vp, u64, C.POINTER(C.c_void_p), pu64, C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), C.POINTER(C.c_int64)],
             "gs_serve_release": [vp, u64],
+            "gs_serve_profile": [vp, C.POINTER(C.c_double), i32],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -492,6 +493,12 @@ class Server:
         a, b, c, d = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
         self.ctx._check(lib().gs_serve_stats(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
         return {"steps": a.value, "graph_launches": b.value, "kernel_launches": c.value, "hbm_in_use": d.value}
+
+    def profile(self):
+        """Host seconds in gs_serve_step by phase."""
+        out = (C.c_double * 4)()
+        self.ctx._check(lib().gs_serve_profile(self._h, out, 4))
+        return {"admit_s": out[0], "step_launch_s": out[1], "side_s": out[2], "step_finish_s": out[3]}
 
     def free(self):
         if self._h:

@@ -376,6 +376,9 @@ struct gs_server {
     uint64_t next_id = 1;
     int step = 0;
     uint64_t steps_run = 0, graph_launches = 0, kernel_launches = 0;
+    // host seconds spent in gs_serve_step by phase: admission, BFS step
+    // launch, side requests, BFS step finish (its wait included), retirement
+    double phase_s[4] = {0, 0, 0, 0};
     std::chrono::steady_clock::time_point t0;
     // pools: exact-size free lists
     std::multimap<size_t, void*> dev_free, host_free;
@@ -989,6 +992,12 @@ extern "C" {
 
 gs_status gs_serve_step(gs_server* s, int* n_active, int* n_queued) {
     if (!s) return GS_ERR_ARG;
+    double t_phase = now_s(s);
+    auto phase_end = [&](int k) {
+        const double t = now_s(s);
+        s->phase_s[k] += t - t_phase;
+        t_phase = t;
+    };
     // admission: FIFO while the state fits the budget and a slot is free
     while (!s->queue.empty() && (int)s->active.size() < kMaxJobs) {
         Request& r = s->reqs[s->queue.front()];
@@ -1005,12 +1014,16 @@ gs_status gs_serve_step(gs_server* s, int* n_active, int* n_queued) {
     // beside it on the lower-priority streams)
     std::vector<int> group_job;
     bool launched = false;
+    phase_end(0);
     GS_TRY(bfs_launch(s, group_job, &launched));
+    phase_end(1);
     gs_status st = side_step(s);
+    phase_end(2);
     if (launched) {
         const gs_status st2 = bfs_finish(s, group_job);   // a launched step is always finished
         if (st == GS_OK) st = st2;
     }
+    phase_end(3);
     if (st != GS_OK) return st;
     if (n_active) *n_active = (int)s->active.size();
     if (n_queued) *n_queued = (int)s->queue.size();
@@ -1111,6 +1124,12 @@ gs_status gs_serve_stats(const gs_server* s, uint64_t* steps, uint64_t* graph_la
     if (graph_launches) *graph_launches = s->graph_launches;
     if (kernel_launches) *kernel_launches = s->kernel_launches;
     if (hbm_in_use) *hbm_in_use = s->used;
+    return GS_OK;
+}
+
+gs_status gs_serve_profile(const gs_server* s, double* seconds, int n) {
+    if (!s || !seconds || n < 0) return GS_ERR_ARG;
+    for (int k = 0; k < n && k < 4; ++k) seconds[k] = s->phase_s[k];
     return GS_OK;
 }
 

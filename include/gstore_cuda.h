@@ -312,6 +312,11 @@ gs_status gs_serve_release(gs_server* s, uint64_t request_id);
 gs_status gs_serve_clock(const gs_server* s, double* seconds);
 gs_status gs_serve_stats(const gs_server* s, uint64_t* steps, uint64_t* graph_launches,
                          uint64_t* kernel_launches, uint64_t* hbm_in_use);
+/* Host seconds spent in gs_serve_step so far, by phase (up to n of them):
+ * [0] admission, [1] BFS step launch, [2] side requests (WCC / k-core /
+ * PageRank chunks, their polling and retirement), [3] BFS step finish (the
+ * wait for the step, retirement of BFS slots). */
+gs_status gs_serve_profile(const gs_server* s, double* seconds, int n);
 gs_status gs_serve_free(gs_server* s);
 
 /* PageRank with the reference's int32 inverse-degree truncation
