@@ -313,6 +313,10 @@ bool pb_layout_wanted(const gs_graph* g);
 gs_status pb_layout_build(gs_graph* g);
 void pb_layout_free(gs_graph* g);
 gs_status pb_launch(gs_state* s);
+// One sweep on `stream` into `y`, with the caller's value stream `val`
+// (n_entries floats): one CTA per item, no ticket (the serving loop's side
+// streams).
+gs_status pb_sweep_on(gs_graph* g, cudaStream_t stream, const float* x, float* y, int* error, float* val);
 gs_status pr_finalize(gs_state* s, int64_t* frontier, int* done);
 
 gs_status wcc_init(gs_state* s);

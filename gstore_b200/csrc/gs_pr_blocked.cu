@@ -465,6 +465,24 @@ gs_status pb_sweep(gs_graph* g, const float* x, float* y, int* error) {
     return GS_OK;
 }
 
+gs_status pb_sweep_on(gs_graph* g, cudaStream_t stream, const float* x, float* y, int* error, float* val) {
+    gs_ctx* ctx = g->ctx;
+    const gs_pb_layout& L = g->pb;
+    if (L.n_items1 == 0) return GS_OK;
+    GS_CHECK_CUDA(ctx, gs_smem_limit_once<pb_gather_kernel>(ctx->device, (int)sizeof(GatherSmem)));
+    GS_CHECK_CUDA(ctx, gs_smem_limit_once<pb_accumulate_kernel>(ctx->device, (int)(kDstBin * 4)));
+    // one CTA per item and no ticket: short CTAs, so that a higher-priority
+    // stream's CTAs find free SMs between them
+    pb_gather_kernel<<<(uint32_t)L.n_items1, kGatherThreads, sizeof(GatherSmem), stream>>>(
+        L.d_items1, L.n_items1, L.d_src, x, val, error, nullptr);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    pb_accumulate_kernel<<<(uint32_t)L.n_items2, kAccThreads, kDstBin * 4, stream>>>(
+        L.d_items2, L.n_items2, L.d_blocks, L.d_dst, val, y, nullptr);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    ctx->launches += 2;
+    return GS_OK;
+}
+
 gs_status pb_launch(gs_state* s) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;

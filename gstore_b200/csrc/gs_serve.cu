@@ -337,6 +337,7 @@ struct Request {
     float* x = nullptr;
     float* y = nullptr;
     float* r = nullptr;
+    float* val = nullptr;                // PageRank on the propagation-blocked layout: its own values
     int* flags = nullptr;                // side requests: [0] done, [1] bounded-wait error
     unsigned long long* cnt = nullptr;   // side requests: two iteration counters
     int side = -1;                       // side slot (WCC, k-core, PageRank)
@@ -460,7 +461,7 @@ size_t footprint(const gs_server* s, const Request& r) {
         case GS_ALGO_BFS: return sg.fv ? 0 : group_bytes(g);
         case GS_ALGO_WCC: return g->N * 5 + g->V * 4 + 64;
         case GS_ALGO_KCORE: return g->N * 4 + g->N / 8 + 2 * (size_t)g->nw + 64;
-        default: return g->N * 12 + 64;
+        default: return g->N * 12 + (g->pb.built ? g->pb.n_entries * 4 : 0) + 64;
     }
 }
 
@@ -547,8 +548,11 @@ gs_status admit(gs_server* s, Request& r) {
                 GS_CHECK_CUDA(ctx, cudaMemsetAsync(r.act[1], 0, g->nw, st));
                 break;
             default:
-                // PageRank sweeps the graph's row-slice layout (built once)
-                if (!g->pr.built) GS_TRY(pr_layout_build(sg.g));
+                // PageRank sweeps the graph's propagation-blocked layout with
+                // a value stream of its own (requests on one graph may run
+                // side by side), else the row-slice layout (each built once)
+                if (!g->pb.built && !g->pr.built) GS_TRY(pr_layout_build(sg.g));
+                if (g->pb.built) GS_TRY(pool_dev(s, g->pb.n_entries * 4, (void**)&r.val));
                 GS_TRY(pool_dev(s, N * 4, (void**)&r.x));
                 GS_TRY(pool_dev(s, N * 4, (void**)&r.y));
                 GS_TRY(pool_dev(s, N * 4, (void**)&r.r));
@@ -593,6 +597,8 @@ void release(gs_server* s, Request& r) {
             pool_dev_put(s, r.x, N * 4);
             pool_dev_put(s, r.y, N * 4);
             pool_dev_put(s, r.r, N * 4);
+            if (r.val) pool_dev_put(s, r.val, g->pb.n_entries * 4);
+            r.val = nullptr;
             break;
     }
     if (r.side >= 0) {
@@ -707,7 +713,8 @@ gs_status queue_chunk(gs_server* s, Request& r) {
             break;
         default:
             for (; r.iter < r.arg; ++r.iter) {
-                GS_TRY(pr_slice_sweep(g, st, r.x, r.y, r.flags + 1, true));
+                if (r.val) GS_TRY(pb_sweep_on(g, st, r.x, r.y, r.flags + 1, r.val));
+                else GS_TRY(pr_slice_sweep(g, st, r.x, r.y, r.flags + 1, true));
                 GS_TRY(pr_finalize_launch(ctx, st, r.x, r.y, r.r, g->d_degree, g->N, g->V, 0));
                 s->kernel_launches += 2;
             }
@@ -766,8 +773,12 @@ gs_status gs_serve_add_graph(gs_server* s, gs_graph* g, int* graph_id) {
     if (g->ctx != s->ctx) return gs_fail(s->ctx, GS_ERR_ARG, "graph belongs to another context");
     if (g->stream) return gs_fail(s->ctx, GS_ERR_UNSUPPORTED, "served graphs must be resident in HBM");
     // the PageRank layout and the blocked orders are built here, at set-up,
-    // not under a request
-    if (!g->pr.built && g->E) GS_TRY(pr_layout_build(g));
+    // not under a request: the propagation-blocked layout for a graph dense
+    // enough for it (its own value stream per request), else the row slices
+    if (!g->pb.built && !g->pr.built && g->E) {
+        if (pb_layout_wanted(g)) GS_TRY(pb_layout_build(g));
+        else GS_TRY(pr_layout_build(g));
+    }
     GS_TRY(gs_ensure_blocked(g));
     SrvGraph sg;
     sg.g = g;
