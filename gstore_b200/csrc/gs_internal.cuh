@@ -108,7 +108,7 @@ struct gs_pr_layout {
 // value per entry written by the gather pass, and the (slice, bin) blocks in
 // bin-major order for the accumulate pass.
 constexpr int kPbSrcBits = 14;   // source slice: 16,384 vertices (x staged in shared memory)
-constexpr int kPbDstBits = 15;   // destination bin: 32,768 vertices (sums in shared memory)
+constexpr int kPbDstBits = 14;   // destination bin: 16,384 vertices (sums in shared memory)
 struct gs_pb_item1 {             // gather item: entries [e0, e0 + n) of source slice `slice`
     uint64_t e0;
     uint32_t n, slice;

@@ -13,18 +13,19 @@
 // Propagation Blocking", IPDPS 2017, restated for the tile grid):
 //
 //   * entries: one per (record, direction), sorted by (source slice S =
-//     src >> 14, destination bin D = dst >> 15, dst, src).  Two u16 streams
+//     src >> 14, destination bin D = dst >> 14, dst, src).  Two u16 streams
 //     hold the source's offset in its slice and the destination's offset in
 //     its bin; the (S, D) blocks of the stream are contiguous;
 //   * gather (pass 1): a CTA stages x of one source slice (16,384 floats,
 //     64 KB) in shared memory with one bulk copy and streams the slice's
 //     entries: val[e] = x[src of e] -- a shared-memory gather, a coalesced
 //     16-bit read and a coalesced 32-bit write per entry;
-//   * accumulate (pass 2): a CTA owns one destination bin (32,768 floats,
-//     128 KB of shared memory), walks the bin's blocks (one per source slice,
+//   * accumulate (pass 2): a CTA owns one destination bin (16,384 floats,
+//     64 KB of shared memory), walks the bin's blocks (one per source slice,
 //     D-major block table) and adds val[e] into its shared-memory sums at
-//     the destination offset (a lane merges equal destinations among its 8
-//     consecutive entries first), then writes the bin's sums to y.
+//     the destination offset (equal destinations, adjacent in a block, are
+//     summed in registers and across lanes first: one atomic per run), then
+//     writes the bin's sums to y.
 //
 // Both passes stream; the random accesses stay in shared memory.  DRAM bytes
 // per entry and sweep: 2 (source offset) + 4 + 4 (value written and read) +
@@ -40,14 +41,14 @@
 namespace {
 
 constexpr uint32_t kSrcSlice = 1u << kPbSrcBits;   // 16,384
-constexpr uint32_t kDstBin = 1u << kPbDstBits;     // 32,768
+constexpr uint32_t kDstBin = 1u << kPbDstBits;     // 16,384
 constexpr int kKeyLowBits = kPbSrcBits + kPbDstBits;
 constexpr int kGatherThreads = 512;
 constexpr int kGatherCtas = 3;       // resident gather CTAs per SM (64 KB of x each)
-constexpr int kGatherGroups = 2;     // 8-entry groups in flight per gather thread
-constexpr int kAccThreads = 1024;
-constexpr int kAccCtas = 1;          // resident accumulate CTAs per SM (the bin's sums each)
-constexpr int kAccGroups = 2;        // 8-entry groups in flight per accumulate lane
+constexpr int kGatherGroups = 4;     // 8-entry groups in flight per gather thread
+constexpr int kAccThreads = 512;
+constexpr int kAccCtas = 3;          // resident accumulate CTAs per SM (the bin's sums each)
+constexpr int kAccGroups = 1;        // 8-entry groups in flight per accumulate lane
 constexpr long long kWaitLimit = 1ll << 24;
 
 struct __align__(128) GatherSmem {
@@ -147,19 +148,62 @@ __global__ void __launch_bounds__(kGatherThreads, kGatherCtas)
     }
 }
 
-// Adds one lane's 8 consecutive entries, sorted by destination, into the
-// shared sums: each run of equal destinations is summed in registers
-// (suffix sums, no branches) and added once, by its first entry -- fewer
-// shared atomics on high-degree vertices and shorter FP32 chains.
-__device__ __forceinline__ void add_group(float* acc, const uint4 d, const float4 lo, const float4 hi) {
+// Adds the 8 consecutive entries of every lane of a warp (lane l: entries
+// 8l .. 8l+7 of the warp's 256, sorted by destination; `valid` false for a
+// lane without entries) into the shared sums.  Equal destinations are
+// adjacent, and a run may cross lanes (a high-degree vertex can fill the
+// whole warp): a lane sums its runs in registers and adds the ones inside it
+// at once; its first and last runs join the neighbouring lanes' runs through
+// a segmented prefix scan over the lanes, and each run is added once, by the
+// lane where it ends.  Without the cross-lane step all lanes of a run would
+// hit one address in the same atomic instruction.
+__device__ __forceinline__ void add_warp_groups(float* acc, uint32_t lane, bool valid, const uint4 d,
+                                                const float4 lo, const float4 hi) {
+    const unsigned kAll = 0xFFFFFFFFu;
     const uint32_t o[8] = {d.x & 0xFFFFu, d.x >> 16, d.y & 0xFFFFu, d.y >> 16,
                            d.z & 0xFFFFu, d.z >> 16, d.w & 0xFFFFu, d.w >> 16};
-    float v[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+    const float v[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+    // in-lane runs: the first (f, sf) and the last (t, st) stay open, the
+    // ones between them are added here
+    const uint32_t f = valid ? o[0] : 0x10000u + lane;   // past any offset: links nothing
+    uint32_t t = f;
+    float run = valid ? v[0] : 0.f, sf = 0.f;
+    bool single = true;
 #pragma unroll
-    for (int j = 6; j >= 0; --j) v[j] += o[j] == o[j + 1] ? v[j + 1] : 0.f;
+    for (int j = 1; j < 8; ++j) {
+        if (!valid) break;
+        if (o[j] != t) {
+            if (single) sf = run;
+            else atomicAdd(acc + t, run);
+            single = false;
+            t = o[j];
+            run = v[j];
+        } else {
+            run += v[j];
+        }
+    }
+    // lane l's first run continues lane l-1's last run when their keys match
+    const uint32_t t_prev = __shfl_up_sync(kAll, t, 1);
+    const bool link = lane > 0 && t_prev == f;
+    // segmented prefix sums of the last runs: a segment starts at a lane
+    // whose first run does not continue the previous lane's, or whose first
+    // run is not its last (its last run starts a new chain)
+    float c = run;
+    bool head = !single || !link;
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
-        if (j == 0 || o[j] != o[j - 1]) atomicAdd(acc + o[j], v[j]);
+    for (int k = 1; k < 32; k <<= 1) {
+        const float cu = __shfl_up_sync(kAll, c, k);
+        const bool hu = __shfl_up_sync(kAll, head, k);
+        if (lane >= (uint32_t)k && !head) {
+            c += cu;
+            head = hu;
+        }
+    }
+    const float carry_in = __shfl_up_sync(kAll, c, 1);
+    const bool link_next = __shfl_down_sync(kAll, link, 1) && lane < 31;
+    if (!valid) return;
+    if (!single) atomicAdd(acc + f, sf + (link ? carry_in : 0.f));   // the first run, closed in this lane
+    if (!link_next) atomicAdd(acc + t, c);                           // the chain of the last run ends here
 }
 
 // Pass 2.  Item: blocks [b0, b1) of the D-major block table, all of bin
@@ -195,16 +239,19 @@ __global__ void __launch_bounds__(kAccThreads, kAccCtas)
             if (e0 + lane < a) atomicAdd(acc + __ldcs(dst + e0 + lane), __ldcs(val + e0 + lane));
             if (b + lane < e1) atomicAdd(acc + __ldcs(dst + b + lane), __ldcs(val + b + lane));
             // body: a lane takes 8 consecutive entries (one 16-byte load of
-            // offsets, two of values), kAccGroups of them in flight
+            // offsets, two of values), kAccGroups groups of the warp in flight;
+            // the loop is warp-uniform (add_warp_groups shuffles)
             const uint4* d8 = reinterpret_cast<const uint4*>(dst);
             const float4* v4 = reinterpret_cast<const float4*>(val);
             const uint64_t cb = b >> 3;
-            for (uint64_t c = (a >> 3) + lane; c < cb; c += 32 * kAccGroups) {
+            for (uint64_t c0 = a >> 3; c0 < cb; c0 += 32 * kAccGroups) {
                 uint4 d[kAccGroups];
                 float4 lo[kAccGroups], hi[kAccGroups];
 #pragma unroll
                 for (int k = 0; k < kAccGroups; ++k) {
-                    const uint64_t ck = c + 32u * k;
+                    const uint64_t ck = c0 + 32u * k + lane;
+                    d[k] = make_uint4(0, 0, 0, 0);
+                    lo[k] = hi[k] = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (ck < cb) {
                         d[k] = __ldcs(d8 + ck);
                         lo[k] = __ldcs(v4 + 2 * ck);
@@ -213,7 +260,7 @@ __global__ void __launch_bounds__(kAccThreads, kAccCtas)
                 }
 #pragma unroll
                 for (int k = 0; k < kAccGroups; ++k)
-                    if (c + 32u * k < cb) add_group(acc, d[k], lo[k], hi[k]);
+                    add_warp_groups(acc, lane, c0 + 32u * k + lane < cb, d[k], lo[k], hi[k]);
             }
         }
         __syncthreads();
