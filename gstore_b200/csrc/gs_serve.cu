@@ -310,6 +310,8 @@ struct SrvGraph {
     int slot_start[kSlots];           // step whose sweep sees depth 1
     unsigned long long used = 0;
     size_t group_bytes = 0;
+    float* pb_val = nullptr;          // the server's value stream for this graph's PageRank requests
+    bool pb_val_busy = false;         // a PageRank request is sweeping with it
 };
 
 struct Request {
@@ -337,7 +339,8 @@ struct Request {
     float* x = nullptr;
     float* y = nullptr;
     float* r = nullptr;
-    float* val = nullptr;                // PageRank on the propagation-blocked layout: its own values
+    float* val = nullptr;                // PageRank on the propagation-blocked layout: its value stream
+    bool own_val = false;                // val is this request's (else the graph's stream in the server)
     int* flags = nullptr;                // side requests: [0] done, [1] bounded-wait error
     unsigned long long* cnt = nullptr;   // side requests: two iteration counters
     int side = -1;                       // side slot (WCC, k-core, PageRank)
@@ -461,7 +464,10 @@ size_t footprint(const gs_server* s, const Request& r) {
         case GS_ALGO_BFS: return sg.fv ? 0 : group_bytes(g);
         case GS_ALGO_WCC: return g->N * 5 + g->V * 4 + 64;
         case GS_ALGO_KCORE: return g->N * 4 + g->N / 8 + 2 * (size_t)g->nw + 64;
-        default: return g->N * 12 + (g->pb.built ? g->pb.n_entries * 4 : 0) + 64;
+        default:
+            // a PageRank request takes the value stream the server keeps for
+            // the graph; one beside it needs a stream of its own
+            return g->N * 12 + (g->pb.built && sg.pb_val_busy ? g->pb.n_entries * 4 : 0) + 64;
     }
 }
 
@@ -552,7 +558,14 @@ gs_status admit(gs_server* s, Request& r) {
                 // a value stream of its own (requests on one graph may run
                 // side by side), else the row-slice layout (each built once)
                 if (!g->pb.built && !g->pr.built) GS_TRY(pr_layout_build(sg.g));
-                if (g->pb.built) GS_TRY(pool_dev(s, g->pb.n_entries * 4, (void**)&r.val));
+                if (g->pb.built && !sg.pb_val_busy) {
+                    r.val = sg.pb_val;
+                    r.own_val = false;
+                    sg.pb_val_busy = true;
+                } else if (g->pb.built) {
+                    GS_TRY(pool_dev(s, g->pb.n_entries * 4, (void**)&r.val));
+                    r.own_val = true;
+                }
                 GS_TRY(pool_dev(s, N * 4, (void**)&r.x));
                 GS_TRY(pool_dev(s, N * 4, (void**)&r.y));
                 GS_TRY(pool_dev(s, N * 4, (void**)&r.r));
@@ -597,7 +610,8 @@ void release(gs_server* s, Request& r) {
             pool_dev_put(s, r.x, N * 4);
             pool_dev_put(s, r.y, N * 4);
             pool_dev_put(s, r.r, N * 4);
-            if (r.val) pool_dev_put(s, r.val, g->pb.n_entries * 4);
+            if (r.val && r.own_val) pool_dev_put(s, r.val, g->pb.n_entries * 4);
+            else if (r.val) s->graphs[r.graph].pb_val_busy = false;
             r.val = nullptr;
             break;
     }
@@ -774,7 +788,9 @@ gs_status gs_serve_add_graph(gs_server* s, gs_graph* g, int* graph_id) {
     if (g->stream) return gs_fail(s->ctx, GS_ERR_UNSUPPORTED, "served graphs must be resident in HBM");
     // the PageRank layout and the blocked orders are built here, at set-up,
     // not under a request: the propagation-blocked layout for a graph dense
-    // enough for it (its own value stream per request), else the row slices
+    // enough for it (the server keeps one value stream per graph for its
+    // PageRank requests; a request beside another on the same graph takes a
+    // stream of its own), else the row slices
     if (!g->pb.built && !g->pr.built && g->E) {
         if (pb_layout_wanted(g)) GS_TRY(pb_layout_build(g));
         else GS_TRY(pr_layout_build(g));
@@ -782,6 +798,7 @@ gs_status gs_serve_add_graph(gs_server* s, gs_graph* g, int* graph_id) {
     GS_TRY(gs_ensure_blocked(g));
     SrvGraph sg;
     sg.g = g;
+    if (g->pb.built) GS_TRY(pool_dev(s, g->pb.n_entries * 4, (void**)&sg.pb_val));
     for (int q = 0; q < kSlots; ++q) sg.slot_req[q] = -1;
     s->graphs.push_back(sg);
     *graph_id = (int)s->graphs.size() - 1;
