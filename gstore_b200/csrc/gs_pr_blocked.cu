@@ -15,14 +15,16 @@
 //   * entries: one per (record, direction), sorted by (source slice S =
 //     src >> 14, destination bin D = dst >> 14, dst, src).  Two u16 streams
 //     hold the source's offset in its slice and the destination's offset in
-//     its bin; the (S, D) blocks of the stream are contiguous;
+//     its bin; the (S, D) blocks of the stream are contiguous, each padded to
+//     a multiple of 8 entries (padding points past every destination);
 //   * gather (pass 1): a CTA stages x of one source slice (16,384 floats,
 //     64 KB) in shared memory with one bulk copy and streams the slice's
 //     entries: val[e] = x[src of e] -- a shared-memory gather, a coalesced
 //     16-bit read and a coalesced 32-bit write per entry;
 //   * accumulate (pass 2): a CTA owns one destination bin (16,384 floats,
 //     64 KB of shared memory), walks the bin's blocks (one per source slice,
-//     D-major block table) and adds val[e] into its shared-memory sums at
+//     D-major block table, a half-warp per block) and adds val[e] into its
+//     shared-memory sums at
 //     the destination offset (equal destinations, adjacent in a block, are
 //     summed in registers and across lanes first: one atomic per run), then
 //     writes the bin's sums to y.
@@ -34,6 +36,7 @@
 #include "gs_internal.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <vector>
@@ -50,6 +53,11 @@ constexpr int kAccThreads = 512;
 constexpr int kAccCtas = 3;          // resident accumulate CTAs per SM (the bin's sums each)
 constexpr int kAccGroups = 1;        // 8-entry groups in flight per accumulate lane
 constexpr long long kWaitLimit = 1ll << 24;
+// Blocks are padded to a multiple of 8 entries; a padding entry points at
+// offset 0 of its slice (its value is read and never added) and at
+// destination kPadDst, past every offset of a bin.
+constexpr uint16_t kPadDst = 0xFFFFu;
+static_assert(kPbDstBits < 16, "kPadDst must lie past every destination offset");
 
 struct __align__(128) GatherSmem {
     float xs[kSrcSlice];
@@ -148,24 +156,24 @@ __global__ void __launch_bounds__(kGatherThreads, kGatherCtas)
     }
 }
 
-// Adds the 8 consecutive entries of every lane of a warp (lane l: entries
-// 8l .. 8l+7 of the warp's 256, sorted by destination; `valid` false for a
-// lane without entries) into the shared sums.  Equal destinations are
-// adjacent, and a run may cross lanes (a high-degree vertex can fill the
-// whole warp): a lane sums its runs in registers and adds the ones inside it
-// at once; its first and last runs join the neighbouring lanes' runs through
-// a segmented prefix scan over the lanes, and each run is added once, by the
-// lane where it ends.  Without the cross-lane step all lanes of a run would
-// hit one address in the same atomic instruction.
-__device__ __forceinline__ void add_warp_groups(float* acc, uint32_t lane, bool valid, const uint4 d,
+// Adds the 8 consecutive entries of every lane of a half-warp (lane l of
+// the 16: entries 8l .. 8l+7 of the half's 128, sorted by destination;
+// `valid` false for a lane past its block) into the shared sums.  Equal
+// destinations are adjacent, and a run may cross lanes (a high-degree vertex
+// can fill the whole half): a lane sums its runs in registers and adds the
+// ones inside it at once; its first and last runs join the neighbouring
+// lanes' runs through a segmented prefix scan over the 16 lanes, and each
+// run is added once, by the lane where it ends.  Without the cross-lane step
+// all lanes of a run would hit one address in the same atomic instruction.
+// Padding entries carry kPadDst (past every offset) and are never added.
+__device__ __forceinline__ void add_half_groups(float* acc, uint32_t hl, unsigned mask, bool valid, const uint4 d,
                                                 const float4 lo, const float4 hi) {
-    const unsigned kAll = 0xFFFFFFFFu;
     const uint32_t o[8] = {d.x & 0xFFFFu, d.x >> 16, d.y & 0xFFFFu, d.y >> 16,
                            d.z & 0xFFFFu, d.z >> 16, d.w & 0xFFFFu, d.w >> 16};
     const float v[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
-    // in-lane runs: the first (f, sf) and the last (t, st) stay open, the
+    // in-lane runs: the first (f, sf) and the last (t, run) stay open, the
     // ones between them are added here
-    const uint32_t f = valid ? o[0] : 0x10000u + lane;   // past any offset: links nothing
+    const uint32_t f = valid ? o[0] : 0x10000u + hl;   // past any offset: links nothing
     uint32_t t = f;
     float run = valid ? v[0] : 0.f, sf = 0.f;
     bool single = true;
@@ -174,7 +182,7 @@ __device__ __forceinline__ void add_warp_groups(float* acc, uint32_t lane, bool 
         if (!valid) break;
         if (o[j] != t) {
             if (single) sf = run;
-            else atomicAdd(acc + t, run);
+            else if (t < kDstBin) atomicAdd(acc + t, run);
             single = false;
             t = o[j];
             run = v[j];
@@ -183,27 +191,27 @@ __device__ __forceinline__ void add_warp_groups(float* acc, uint32_t lane, bool 
         }
     }
     // lane l's first run continues lane l-1's last run when their keys match
-    const uint32_t t_prev = __shfl_up_sync(kAll, t, 1);
-    const bool link = lane > 0 && t_prev == f;
+    const uint32_t t_prev = __shfl_up_sync(mask, t, 1, 16);
+    const bool link = hl > 0 && t_prev == f;
     // segmented prefix sums of the last runs: a segment starts at a lane
     // whose first run does not continue the previous lane's, or whose first
     // run is not its last (its last run starts a new chain)
     float c = run;
     bool head = !single || !link;
 #pragma unroll
-    for (int k = 1; k < 32; k <<= 1) {
-        const float cu = __shfl_up_sync(kAll, c, k);
-        const bool hu = __shfl_up_sync(kAll, head, k);
-        if (lane >= (uint32_t)k && !head) {
+    for (int k = 1; k < 16; k <<= 1) {
+        const float cu = __shfl_up_sync(mask, c, k, 16);
+        const bool hu = __shfl_up_sync(mask, head, k, 16);
+        if (hl >= (uint32_t)k && !head) {
             c += cu;
             head = hu;
         }
     }
-    const float carry_in = __shfl_up_sync(kAll, c, 1);
-    const bool link_next = __shfl_down_sync(kAll, link, 1) && lane < 31;
+    const float carry_in = __shfl_up_sync(mask, c, 1, 16);
+    const bool link_next = __shfl_down_sync(mask, link, 1, 16) && hl < 15;
     if (!valid) return;
-    if (!single) atomicAdd(acc + f, sf + (link ? carry_in : 0.f));   // the first run, closed in this lane
-    if (!link_next) atomicAdd(acc + t, c);                           // the chain of the last run ends here
+    if (!single && f < kDstBin) atomicAdd(acc + f, sf + (link ? carry_in : 0.f));   // first run, closed here
+    if (!link_next && t < kDstBin) atomicAdd(acc + t, c);                          // the last run's chain ends here
 }
 
 // Pass 2.  Item: blocks [b0, b1) of the D-major block table, all of bin
@@ -230,37 +238,33 @@ __global__ void __launch_bounds__(kAccThreads, kAccCtas)
         const gs_pb_item2 it = items[i];
         for (uint32_t k = tid; k < kDstBin / 4; k += kAccThreads) acc4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
         __syncthreads();
-        for (uint32_t bi = it.b0 + warp; bi < it.b1; bi += kWarps) {
+        // a half-warp per block (blocks hold a multiple of 8 entries, ~128 at
+        // Kronecker scale 26); a lane takes 8 consecutive entries (one
+        // 16-byte load of offsets, two of values)
+        const uint32_t half = lane >> 4, hl = lane & 15;
+        const unsigned hmask = half ? 0xFFFF0000u : 0x0000FFFFu;
+        const uint4* d8 = reinterpret_cast<const uint4*>(dst);
+        const float4* v4 = reinterpret_cast<const float4*>(val);
+        for (uint32_t bi = it.b0 + 2 * warp + half; bi < it.b1; bi += 2 * kWarps) {
             const gs_pb_block blk = blocks[bi];
-            const uint64_t e0 = blk.e0, e1 = blk.e0 + blk.n;
-            // head up to a multiple of 8 entries and tail: one entry per lane
-            const uint64_t a = ((e0 + 7) & ~7ull) < e1 ? ((e0 + 7) & ~7ull) : e1;
-            const uint64_t b = (e1 & ~7ull) > a ? (e1 & ~7ull) : a;
-            if (e0 + lane < a) atomicAdd(acc + __ldcs(dst + e0 + lane), __ldcs(val + e0 + lane));
-            if (b + lane < e1) atomicAdd(acc + __ldcs(dst + b + lane), __ldcs(val + b + lane));
-            // body: a lane takes 8 consecutive entries (one 16-byte load of
-            // offsets, two of values), kAccGroups groups of the warp in flight;
-            // the loop is warp-uniform (add_warp_groups shuffles)
-            const uint4* d8 = reinterpret_cast<const uint4*>(dst);
-            const float4* v4 = reinterpret_cast<const float4*>(val);
-            const uint64_t cb = b >> 3;
-            for (uint64_t c0 = a >> 3; c0 < cb; c0 += 32 * kAccGroups) {
+            const uint64_t g0 = blk.e0 >> 3, ng = blk.n >> 3;
+            for (uint64_t c0 = 0; c0 < ng; c0 += 16 * kAccGroups) {   // uniform in the half
                 uint4 d[kAccGroups];
                 float4 lo[kAccGroups], hi[kAccGroups];
 #pragma unroll
                 for (int k = 0; k < kAccGroups; ++k) {
-                    const uint64_t ck = c0 + 32u * k + lane;
+                    const uint64_t ck = c0 + 16u * k + hl;
                     d[k] = make_uint4(0, 0, 0, 0);
                     lo[k] = hi[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (ck < cb) {
-                        d[k] = __ldcs(d8 + ck);
-                        lo[k] = __ldcs(v4 + 2 * ck);
-                        hi[k] = __ldcs(v4 + 2 * ck + 1);
+                    if (ck < ng) {
+                        d[k] = __ldcs(d8 + g0 + ck);
+                        lo[k] = __ldcs(v4 + 2 * (g0 + ck));
+                        hi[k] = __ldcs(v4 + 2 * (g0 + ck) + 1);
                     }
                 }
 #pragma unroll
                 for (int k = 0; k < kAccGroups; ++k)
-                    add_warp_groups(acc, lane, c0 + 32u * k + lane < cb, d[k], lo[k], hi[k]);
+                    add_half_groups(acc, hl, hmask, c0 + 16u * k + hl < ng, d[k], lo[k], hi[k]);
             }
         }
         __syncthreads();
@@ -308,14 +312,35 @@ __global__ void pb_keys_kernel(const gs_unit* __restrict__ units, uint64_t n_uni
     }
 }
 
-__global__ void pb_split_kernel(const uint64_t* __restrict__ keys, uint64_t n, uint16_t* __restrict__ src,
-                                uint16_t* __restrict__ dst) {
+// Block counts rounded up to 8 entries: pc[bid] (bid < n_blk), pc[n_blk] = 0.
+__global__ void pb_padded_count_kernel(const uint64_t* __restrict__ start, uint64_t n_blk, uint64_t* __restrict__ pc) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t e = tid; e < n; e += nth) {
-        const uint64_t k = keys[e];
-        src[e] = (uint16_t)(k & (kSrcSlice - 1));
-        dst[e] = (uint16_t)((k >> kPbSrcBits) & (kDstBin - 1));
+    for (uint64_t bid = tid; bid <= n_blk; bid += nth)
+        pc[bid] = bid < n_blk ? (start[bid + 1] - start[bid] + 7) & ~7ull : 0;
+}
+
+// The sorted keys of block bid go to the padded streams at pstart[bid]
+// (source and destination offsets), then the block's padding entries (a warp
+// per block).
+__global__ void pb_split_kernel(const uint64_t* __restrict__ keys, const uint64_t* __restrict__ start,
+                                const uint64_t* __restrict__ pstart, uint64_t n_blk, uint16_t* __restrict__ src,
+                                uint16_t* __restrict__ dst) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t n_warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t bid = warp; bid < n_blk; bid += n_warps) {
+        const uint64_t s0 = start[bid], n = start[bid + 1] - s0, p0 = pstart[bid], pn = pstart[bid + 1] - p0;
+        for (uint64_t k = lane; k < pn; k += 32) {
+            if (k < n) {
+                const uint64_t key = keys[s0 + k];
+                src[p0 + k] = (uint16_t)(key & (kSrcSlice - 1));
+                dst[p0 + k] = (uint16_t)((key >> kPbSrcBits) & (kDstBin - 1));
+            } else {
+                src[p0 + k] = 0;
+                dst[p0 + k] = kPadDst;
+            }
+        }
     }
 }
 
@@ -378,7 +403,7 @@ bool pb_layout_wanted(const gs_graph* g) {
     // building needs the sort's two key buffers too
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return false;
-    const uint64_t need = n_ent * (8 + 16) + (nS * nD + 1) * 24 + (2ull << 30);
+    const uint64_t need = (n_ent + 8 * nS * nD) * 8 + n_ent * 16 + (nS * nD + 1) * 32 + (2ull << 30);
     return free_b > need;
 }
 
@@ -392,7 +417,8 @@ gs_status pb_layout_build(gs_graph* g) {
     int end_bit = kKeyLowBits;
     while ((1ull << (end_bit - kKeyLowBits)) < n_blk) ++end_bit;
 
-    uint64_t *d_k0 = nullptr, *d_k1 = nullptr, *d_start = nullptr;
+    uint64_t *d_k0 = nullptr, *d_k1 = nullptr, *d_start = nullptr, *d_pstart = nullptr;
+    uint64_t n_pad = 0;   // entries with every block padded to a multiple of 8
     void* d_tmp = nullptr;
     size_t tmp_bytes = 0;
     gs_status st = gs_dev_alloc(ctx, (void**)&d_k0, n_ent * 8);
@@ -413,15 +439,35 @@ gs_status pb_layout_build(gs_graph* g) {
         const uint64_t* sorted = keys.Current();
         gs_dev_free(d_tmp);
         d_tmp = nullptr;
-        if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_src, n_ent * 2);
-        if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_dst, n_ent * 2);
         if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&d_start, (n_blk + 1) * 8);
+        if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&d_pstart, (n_blk + 1) * 8);
+        if (st == GS_OK) {
+            pb_block_start_kernel<<<grid_for(n_blk + 1, ctx), 256, 0, ctx->stream>>>(sorted, n_ent, n_blk, d_start);
+            pb_padded_count_kernel<<<grid_for(n_blk + 1, ctx), 256, 0, ctx->stream>>>(d_start, n_blk, d_pstart);
+            ctx->launches += 2;
+            e = cudaGetLastError();
+            size_t scan_bytes = 0;
+            if (e == cudaSuccess)
+                e = cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, d_pstart, d_pstart, n_blk + 1, ctx->stream);
+            if (e == cudaSuccess) st = gs_dev_alloc(ctx, &d_tmp, scan_bytes);
+            if (e == cudaSuccess && st == GS_OK)
+                e = cub::DeviceScan::ExclusiveSum(d_tmp, scan_bytes, d_pstart, d_pstart, n_blk + 1, ctx->stream);
+            ctx->launches++;
+            if (e == cudaSuccess && st == GS_OK)
+                e = cudaMemcpyAsync(&n_pad, d_pstart + n_blk, 8, cudaMemcpyDeviceToHost, ctx->stream);
+            if (e == cudaSuccess && st == GS_OK) e = cudaStreamSynchronize(ctx->stream);
+            gs_dev_free(d_tmp);
+            d_tmp = nullptr;
+            if (e != cudaSuccess && st == GS_OK) st = gs_cuda_fail(ctx, e, "propagation-blocking block starts");
+        }
+        if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_src, n_pad * 2);
+        if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_dst, n_pad * 2);
         if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_blocks, std::max<uint64_t>(1, n_blk) * sizeof(gs_pb_block));
         if (st == GS_OK) {
-            pb_split_kernel<<<grid_for(n_ent, ctx), 256, 0, ctx->stream>>>(sorted, n_ent, L.d_src, L.d_dst);
-            pb_block_start_kernel<<<grid_for(n_blk + 1, ctx), 256, 0, ctx->stream>>>(sorted, n_ent, n_blk, d_start);
-            pb_block_table_kernel<<<grid_for(n_blk, ctx), 256, 0, ctx->stream>>>(d_start, nS, nD, L.d_blocks);
-            ctx->launches += 3;
+            pb_split_kernel<<<gs_grid_size(ctx, 8), 256, 0, ctx->stream>>>(sorted, d_start, d_pstart, n_blk, L.d_src,
+                                                                            L.d_dst);
+            pb_block_table_kernel<<<grid_for(n_blk, ctx), 256, 0, ctx->stream>>>(d_pstart, nS, nD, L.d_blocks);
+            ctx->launches += 2;
             e = cudaGetLastError();
             if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "propagation-blocking layout");
         }
@@ -436,19 +482,21 @@ gs_status pb_layout_build(gs_graph* g) {
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         // entries of slice S start at block (S, 0), the first of the bin-major table
         for (uint32_t s = 0; s < nS; ++s) slice_start[s] = blocks[s].e0;
-        slice_start[nS] = n_ent;
+        slice_start[nS] = n_pad;
         if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "propagation-blocking tables");
     }
     gs_dev_free(d_start);
+    gs_dev_free(d_pstart);
     if (st != GS_OK) {
         pb_layout_free(g);
         return st;
     }
     // Items: entry chunks of every slice (pass 1) and block ranges of every
     // bin (pass 2), sized so that each pass has a few items per resident CTA.
+    // (item boundaries stay multiples of 8 entries: every block starts on one)
     const uint64_t per1 =
-        std::clamp<uint64_t>(n_ent / ((uint64_t)ctx->num_sms * kGatherCtas * 4), 32768, 1ull << 20);
-    const uint64_t per2 = std::clamp<uint64_t>(n_ent / ((uint64_t)ctx->num_sms * kAccCtas * 4), 65536, 1ull << 22);
+        std::clamp<uint64_t>(n_pad / ((uint64_t)ctx->num_sms * kGatherCtas * 4), 32768, 1ull << 20) & ~7ull;
+    const uint64_t per2 = std::clamp<uint64_t>(n_pad / ((uint64_t)ctx->num_sms * kAccCtas * 4), 65536, 1ull << 22);
     std::vector<gs_pb_item1> items1;
     for (uint32_t s = 0; s < nS; ++s)
         for (uint64_t e = slice_start[s]; e < slice_start[s + 1]; e += per1)
@@ -470,11 +518,11 @@ gs_status pb_layout_build(gs_graph* g) {
         if (acc > 0) items2.push_back(gs_pb_item2{b0, (d + 1) * nS, d, 0u});
         if (bin_total > 0 && items2.size() == first + 1) items2.back().whole = 1;
     }
-    L.n_entries = n_ent;
+    L.n_entries = n_pad;
     L.n_blocks = n_blk;
     L.n_items1 = items1.size();
     L.n_items2 = items2.size();
-    st = gs_dev_alloc(ctx, (void**)&L.d_val, n_ent * 4);
+    st = gs_dev_alloc(ctx, (void**)&L.d_val, n_pad * 4);
     if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_items1, std::max<size_t>(1, items1.size()) * sizeof(gs_pb_item1));
     if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_items2, std::max<size_t>(1, items2.size()) * sizeof(gs_pb_item2));
     cudaError_t e = cudaSuccess;
