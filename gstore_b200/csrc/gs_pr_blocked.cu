@@ -501,32 +501,54 @@ gs_status pb_layout_build(gs_graph* g) {
     for (uint32_t s = 0; s < nS; ++s)
         for (uint64_t e = slice_start[s]; e < slice_start[s + 1]; e += per1)
             items1.push_back(gs_pb_item1{e, (uint32_t)std::min<uint64_t>(per1, slice_start[s + 1] - e), s});
+    // The table the accumulate pass walks: each bin's blocks in slice order,
+    // cut into chunks of at most kChunk entries (a half-warp's two passes), so
+    // that the few large blocks of a small graph spread over the CTA's
+    // half-warps; empty blocks dropped.
+    constexpr uint32_t kChunk = 256;
+    std::vector<gs_pb_block> table;
+    std::vector<uint64_t> bin_first(nD + 1);
+    table.reserve(n_blk);
+    for (uint32_t d = 0; d < nD; ++d) {
+        bin_first[d] = table.size();
+        for (uint32_t b = d * nS; b < (d + 1) * nS; ++b)
+            for (uint64_t k = 0; k < blocks[b].n; k += kChunk)
+                table.push_back(gs_pb_block{blocks[b].e0 + k, (uint32_t)std::min<uint64_t>(kChunk, blocks[b].n - k), 0u});
+    }
+    bin_first[nD] = table.size();
     std::vector<gs_pb_item2> items2;
     for (uint32_t d = 0; d < nD; ++d) {
         const uint32_t first = (uint32_t)items2.size();
-        uint64_t acc = 0, bin_total = 0;
-        uint32_t b0 = d * nS;
-        for (uint32_t b = d * nS; b < (d + 1) * nS; ++b) {
-            bin_total += blocks[b].n;
-            if (acc > 0 && acc + blocks[b].n > per2) {
+        uint64_t acc = 0;
+        uint32_t b0 = (uint32_t)bin_first[d];
+        for (uint32_t b = b0; b < bin_first[d + 1]; ++b) {
+            if (acc > 0 && acc + table[b].n > per2) {
                 items2.push_back(gs_pb_item2{b0, b, d, 0u});
                 b0 = b;
                 acc = 0;
             }
-            acc += blocks[b].n;
+            acc += table[b].n;
         }
-        if (acc > 0) items2.push_back(gs_pb_item2{b0, (d + 1) * nS, d, 0u});
-        if (bin_total > 0 && items2.size() == first + 1) items2.back().whole = 1;
+        if (acc > 0) items2.push_back(gs_pb_item2{b0, (uint32_t)bin_first[d + 1], d, 0u});
+        if (items2.size() == first + 1) items2.back().whole = 1;
     }
     L.n_entries = n_pad;
-    L.n_blocks = n_blk;
+    L.n_blocks = table.size();
     L.n_items1 = items1.size();
     L.n_items2 = items2.size();
     st = gs_dev_alloc(ctx, (void**)&L.d_val, n_pad * 4);
     if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_items1, std::max<size_t>(1, items1.size()) * sizeof(gs_pb_item1));
     if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_items2, std::max<size_t>(1, items2.size()) * sizeof(gs_pb_item2));
     cudaError_t e = cudaSuccess;
-    if (st == GS_OK && !items1.empty())
+    if (st == GS_OK && table.size() > n_blk) {   // more chunks than blocks: a larger table
+        gs_dev_free(L.d_blocks);
+        L.d_blocks = nullptr;
+        st = gs_dev_alloc(ctx, (void**)&L.d_blocks, table.size() * sizeof(gs_pb_block));
+    }
+    if (st == GS_OK && !table.empty())
+        e = cudaMemcpyAsync(L.d_blocks, table.data(), table.size() * sizeof(gs_pb_block), cudaMemcpyHostToDevice,
+                            ctx->stream);
+    if (st == GS_OK && e == cudaSuccess && !items1.empty())
         e = cudaMemcpyAsync(L.d_items1, items1.data(), items1.size() * sizeof(gs_pb_item1), cudaMemcpyHostToDevice,
                             ctx->stream);
     if (st == GS_OK && e == cudaSuccess && !items2.empty())
