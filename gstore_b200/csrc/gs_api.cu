@@ -27,6 +27,12 @@ gs_status gs_dev_alloc(gs_ctx* ctx, void** ptr, size_t bytes) {
     *ptr = nullptr;
     if (bytes == 0) bytes = 16;
     cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e == cudaErrorMemoryAllocation && ctx && !ctx->pool_free.empty()) {
+        // the pool's idle blocks hold the memory: release them, try once more
+        cudaGetLastError();
+        gs_pool_clear(ctx);
+        e = cudaMalloc(ptr, bytes);
+    }
     if (e != cudaSuccess) {
         *ptr = nullptr;
         return gs_cuda_fail(ctx, e, "cudaMalloc");
@@ -79,6 +85,30 @@ gs_status gs_alloc_records(gs_ctx* ctx, uint32_t** ptr, uint64_t n_records) {
     GS_TRY(gs_dev_alloc(ctx, (void**)ptr, (n_records + kRecPad) * 4));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(*ptr + n_records, 0, kRecPad * 4, ctx->stream));
     return GS_OK;
+}
+
+gs_status gs_graph_alloc(gs_graph* g, void** ptr, size_t bytes) {
+    GS_TRY(gs_pool_get(g->ctx, bytes, ptr));
+    g->pooled.emplace_back(*ptr, bytes);
+    return GS_OK;
+}
+
+gs_status gs_graph_alloc_records(gs_graph* g, uint32_t** ptr, uint64_t n_records) {
+    GS_TRY(gs_graph_alloc(g, (void**)ptr, (n_records + kRecPad) * 4));
+    GS_CHECK_CUDA(g->ctx, cudaMemsetAsync(*ptr + n_records, 0, kRecPad * 4, g->ctx->stream));
+    return GS_OK;
+}
+
+void gs_graph_release(gs_graph* g, void* ptr) {
+    if (!ptr) return;
+    for (auto it = g->pooled.begin(); it != g->pooled.end(); ++it) {
+        if (it->first == ptr) {
+            gs_pool_put(g->ctx, ptr, it->second);
+            g->pooled.erase(it);
+            return;
+        }
+    }
+    gs_dev_free(ptr);
 }
 
 void gs_geometry_of(uint64_t V, int directed, uint32_t* p, uint32_t* p_s, uint64_t* n_tiles) {
@@ -201,21 +231,18 @@ gs_status gs_kernel_time(gs_ctx* ctx, int algo, uint64_t* launches, double* tota
 
 // ------------------------------------------------------------------ graph --
 static void free_graph_arrays(gs_graph* g) {
+    // pooled buffers are reused by the next request in stream order only:
+    // no copy or kernel may still touch them when they go back to the pool
+    cudaStreamSynchronize(g->ctx->stream);
     gs_stream_close(g);
     pr_layout_free(g);
     pb_layout_free(g);
-    gs_dev_free(g->d_rec);
-    gs_dev_free(g->d_items);
-    gs_dev_free(g->d_tile_off);
-    gs_dev_free(g->d_tile_rc);
-    gs_dev_free(g->d_degree);
-    gs_dev_free(g->d_runs);
-    gs_dev_free(g->d_runs_lpt);
-    gs_dev_free(g->d_units);
-    gs_dev_free(g->d_runs_blk);
-    gs_dev_free(g->d_units_blk);
-    gs_dev_free(g->d_runs_blk2);
-    gs_dev_free(g->d_units_blk2);
+    for (void* p : {(void*)g->d_rec, (void*)g->d_items, (void*)g->d_tile_off, (void*)g->d_tile_rc,
+                    (void*)g->d_degree, (void*)g->d_runs, (void*)g->d_runs_lpt, (void*)g->d_units,
+                    (void*)g->d_runs_blk, (void*)g->d_units_blk, (void*)g->d_runs_blk2, (void*)g->d_units_blk2})
+        gs_graph_release(g, p);
+    for (auto& pb : g->pooled) gs_pool_put(g->ctx, pb.first, pb.second);   // none expected
+    g->pooled.clear();
     g->d_runs_blk2 = nullptr;
     g->d_units_blk2 = nullptr;
     g->d_runs = nullptr;
@@ -280,8 +307,8 @@ static gs_status build_blocked_order(gs_graph* g, uint32_t block, uint64_t* R_ou
         }
     }
     *R_out = runs.size();
-    GS_TRY(gs_dev_alloc(ctx, (void**)d_units_out, std::max<size_t>(1, units.size()) * sizeof(gs_unit)));
-    GS_TRY(gs_dev_alloc(ctx, (void**)d_runs_out, std::max<size_t>(1, runs.size()) * sizeof(gs_tile_run)));
+    GS_TRY(gs_graph_alloc(g, (void**)d_units_out, std::max<size_t>(1, units.size()) * sizeof(gs_unit)));
+    GS_TRY(gs_graph_alloc(g, (void**)d_runs_out, std::max<size_t>(1, runs.size()) * sizeof(gs_tile_run)));
     if (!units.empty())
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(*d_units_out, units.data(), units.size() * sizeof(gs_unit),
                                            cudaMemcpyHostToDevice, ctx->stream));
@@ -376,11 +403,11 @@ static gs_status build_tables(gs_graph* g) {
     g->I = n_items;
     g->R = runs.size();
     g->U = units.size();
-    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_units, std::max<size_t>(1, units.size()) * sizeof(gs_unit)));
+    GS_TRY(gs_graph_alloc(g, (void**)&g->d_units, std::max<size_t>(1, units.size()) * sizeof(gs_unit)));
     if (!units.empty())
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_units, units.data(), units.size() * sizeof(gs_unit),
                                            cudaMemcpyHostToDevice, ctx->stream));
-    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_runs, std::max<size_t>(1, runs.size()) * sizeof(gs_tile_run)));
+    GS_TRY(gs_graph_alloc(g, (void**)&g->d_runs, std::max<size_t>(1, runs.size()) * sizeof(gs_tile_run)));
     if (!runs.empty())
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_runs, runs.data(), runs.size() * sizeof(gs_tile_run),
                                            cudaMemcpyHostToDevice, ctx->stream));
@@ -413,12 +440,12 @@ static gs_status build_tables(gs_graph* g) {
             return x.rec_end - x.rec_beg > y.rec_end - y.rec_beg;
         });
         g->R_lpt = lpt.size();
-        GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_runs_lpt, lpt.size() * sizeof(gs_tile_run)));
+        GS_TRY(gs_graph_alloc(g, (void**)&g->d_runs_lpt, lpt.size() * sizeof(gs_tile_run)));
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_runs_lpt, lpt.data(), lpt.size() * sizeof(gs_tile_run),
                                            cudaMemcpyHostToDevice, ctx->stream));
     }
-    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_tile_off, tile_off.size() * sizeof(uint64_t)));
-    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_tile_rc, std::max<size_t>(1, tile_rc.size()) * sizeof(uint32_t)));
+    GS_TRY(gs_graph_alloc(g, (void**)&g->d_tile_off, tile_off.size() * sizeof(uint64_t)));
+    GS_TRY(gs_graph_alloc(g, (void**)&g->d_tile_rc, std::max<size_t>(1, tile_rc.size()) * sizeof(uint32_t)));
     GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_tile_off, tile_off.data(), tile_off.size() * sizeof(uint64_t),
                                        cudaMemcpyHostToDevice, ctx->stream));
     if (!tile_rc.empty())
@@ -449,7 +476,7 @@ static gs_status check_start(gs_graph* g, uint64_t n_start, uint64_t n_edges) {
 
 static gs_status finish_upload(gs_graph* g, const int32_t* degree, bool degree_on_device) {
     gs_ctx* ctx = g->ctx;
-    GS_TRY(gs_dev_alloc(ctx, (void**)&g->d_degree, g->N * sizeof(int32_t)));
+    GS_TRY(gs_graph_alloc(g, (void**)&g->d_degree, g->N * sizeof(int32_t)));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(g->d_degree, 0, g->N * sizeof(int32_t), ctx->stream));
     if (degree) {
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(g->d_degree, degree, g->V * sizeof(int32_t),
@@ -545,7 +572,7 @@ gs_status gs_upload_graph(gs_ctx* ctx, const uint64_t* start, uint64_t n_start,
     }
     if (st == GS_OK) {
         g->E = n_edges;
-        st = gs_alloc_records(ctx, &g->d_rec, n_edges);
+        st = gs_graph_alloc_records(g, &g->d_rec, n_edges);
         if (st == GS_OK && n_edges) {
             cudaError_t e = cudaMemcpyAsync(g->d_rec, grid, n_edges * 4, cudaMemcpyHostToDevice, ctx->stream);
             if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "cudaMemcpyAsync(grid)");
@@ -652,7 +679,7 @@ gs_status gs_upload_graph_device(gs_ctx* ctx, const uint64_t* d_start, uint64_t 
     if (st == GS_OK) st = check_start(g, n_start, n_edges);
     if (st == GS_OK) {
         g->E = n_edges;
-        st = gs_alloc_records(ctx, &g->d_rec, n_edges);
+        st = gs_graph_alloc_records(g, &g->d_rec, n_edges);
         if (st == GS_OK && n_edges) {
             cudaError_t e = cudaMemcpyAsync(g->d_rec, d_grid, n_edges * 4, cudaMemcpyDeviceToDevice, ctx->stream);
             if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "cudaMemcpyAsync(grid)");

@@ -204,6 +204,9 @@ struct gs_graph {
     std::vector<uint64_t> h_start;    // full .start copy (host), for planners
     std::vector<uint64_t> h_tile_off; // host copy of d_tile_off
     std::vector<uint32_t> h_tile_rc;  // host copy of d_tile_rc
+    // device buffers above taken from the context's pool (gs_graph_alloc),
+    // with their sizes: returned to the pool when the graph is freed
+    std::vector<std::pair<void*, size_t>> pooled;
 };
 
 struct gs_state {
@@ -286,6 +289,12 @@ gs_status gs_state_alloc(gs_state* s, void** ptr, size_t bytes);
 gs_status gs_ensure_blocked(gs_graph* g);
 void gs_pool_put(gs_ctx* ctx, void* ptr, size_t bytes);
 void gs_pool_clear(gs_ctx* ctx);
+// A buffer of a graph from the context's pool, recorded in g->pooled; and
+// the same for a record buffer (n_records + kRecPad zero-padded entries).
+gs_status gs_graph_alloc(gs_graph* g, void** ptr, size_t bytes);
+gs_status gs_graph_alloc_records(gs_graph* g, uint32_t** ptr, uint64_t n_records);
+// Returns a graph buffer: to the pool when it came from there, else cudaFree.
+void gs_graph_release(gs_graph* g, void* ptr);
 
 gs_status launch_validate_records(gs_graph* g, int* d_flag);
 gs_status launch_degree_from_records(gs_graph* g);

@@ -404,7 +404,8 @@ bool pb_layout_wanted(const gs_graph* g) {
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return false;
     const uint64_t need = (n_ent + 8 * nS * nD) * 8 + n_ent * 16 + (nS * nD + 1) * 32 + (2ull << 30);
-    return free_b > need;
+    // (idle pool blocks count as free: an allocation that fails releases them)
+    return free_b + g->ctx->pool_bytes > need;
 }
 
 gs_status pb_layout_build(gs_graph* g) {
