@@ -79,6 +79,10 @@ def parse_args():
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="length of the Poisson arrival trace")
     ap.add_argument("--stream-scale", type=int, default=28)
     ap.add_argument("--stream-budget-gb", type=float, default=4.0)
+    ap.add_argument("--case", choices=["bfs", "pagerank", "wcc", "kcore"],
+                    help="profiling case: build the --scale graph, run this algorithm once, print its time, exit")
+    ap.add_argument("--case-arg", type=int, default=None,
+                    help="the case's argument (PageRank iterations, k of k-core; default 2 and 8)")
     return ap.parse_args()
 
 
@@ -1056,6 +1060,23 @@ def main():
     del d_pairs
     torch.cuda.empty_cache()
     degree = graph.degree()
+    if args.case:
+        # one query of one algorithm, for a profiler's capture (not a bench line)
+        arg = args.case_arg
+        if arg is None:
+            arg = {"pagerank": 2, "kcore": 8, "wcc": 0}.get(args.case)
+        if args.case == "bfs":
+            arg = splitmix64_roots(degree, 1, seed=1)[0]
+        t0 = time.perf_counter()
+        with graph.state(args.case, arg) as s:
+            s.run()
+        torch.cuda.synchronize()
+        print(json.dumps({"case": args.case, "arg": int(arg), "scale": scale,
+                          "ms_incl_layout_build": (time.perf_counter() - t0) * 1e3}))
+        graph.free()
+        ctx.close()
+        dist.close()
+        return
     roots = splitmix64_roots(degree, args.warmup + args.steps, seed=1, skip=dist.rank * (args.warmup + args.steps))
     warm, timed_roots = roots[: args.warmup], roots[args.warmup:]
 

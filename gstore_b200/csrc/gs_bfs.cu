@@ -137,8 +137,13 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
         const bool got = bar_wait(&m.bar, parity);
         parity ^= 1;
         if (!__syncthreads_and(got)) {
-            if (tid == 0) atomicExch(a.error, 1);
-            break;   // uniform; nothing else in flight
+            // the copy is late: flag it and give it one more bounded wait, so
+            // that the CTA does not leave with its copy still in flight
+            if (tid == 0) {
+                atomicExch(a.error, 1);
+                bar_wait(&m.bar, parity ^ 1);
+            }
+            break;   // uniform
         }
         const uint32_t mr = ar ? 1u : 0u;
         for (uint32_t ui = ub + warp; ui < ue; ui += kWarps) {

@@ -105,15 +105,15 @@ struct gs_pr_layout {
 // PageRank propagation-blocked layout (gs_pr_blocked.cu): one entry per
 // (record, direction), sorted by (source slice, destination bin); u16 offsets
 // of the source in its slice and of the destination in its bin, one float
-// value per entry written by the gather pass, and the (slice, bin) blocks in
-// bin-major order for the accumulate pass.
+// value per entry written by the gather pass, and for the accumulate pass the
+// list of every bin's 8-entry groups (its blocks in slice order).
 constexpr int kPbSrcBits = 14;   // source slice: 16,384 vertices (x staged in shared memory)
 constexpr int kPbDstBits = 14;   // destination bin: 16,384 vertices (sums in shared memory)
 struct gs_pb_item1 {             // gather item: entries [e0, e0 + n) of source slice `slice`
     uint64_t e0;
     uint32_t n, slice;
 };
-struct gs_pb_item2 {             // accumulate item: blocks [b0, b1) of bin `bin`
+struct gs_pb_item2 {             // accumulate item: groups [b0, b1) of the group list, all of bin `bin`
     uint32_t b0, b1, bin, whole;
 };
 struct gs_pb_block {             // entries [e0, e0 + n) of one (slice, bin) block
@@ -124,10 +124,10 @@ struct gs_pb_layout {
     uint16_t* d_src = nullptr;
     uint16_t* d_dst = nullptr;
     float* d_val = nullptr;
-    gs_pb_block* d_blocks = nullptr;
+    uint32_t* d_groups = nullptr;   // per bin, in slice order: the 8-entry groups of its blocks (entry index / 8)
     gs_pb_item1* d_items1 = nullptr;
     gs_pb_item2* d_items2 = nullptr;
-    uint64_t n_entries = 0, n_blocks = 0, n_items1 = 0, n_items2 = 0;
+    uint64_t n_entries = 0, n_groups = 0, n_items1 = 0, n_items2 = 0;
     bool built = false;
 };
 

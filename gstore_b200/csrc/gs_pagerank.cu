@@ -141,8 +141,13 @@ __global__ void __launch_bounds__(kPrThreads, 2)
         const bool got = wait_bar(&m.bar, parity);
         parity ^= 1;
         if (!__syncthreads_and(got)) {
-            if (tid == 0) atomicExch(error, 1);
-            break;   // uniform; nothing else in flight
+            // the copy is late: flag it and give it one more bounded wait, so
+            // that the CTA does not leave with its copy still in flight
+            if (tid == 0) {
+                atomicExch(error, 1);
+                wait_bar(&m.bar, parity ^ 1);
+            }
+            break;   // uniform
         }
         for (uint32_t ui = it.unit_beg + warp; ui < it.unit_end; ui += kPrWarps) sweep_unit(units[ui], rec, op, lane);
         __syncthreads();

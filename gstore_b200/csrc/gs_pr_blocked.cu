@@ -23,8 +23,8 @@
 //     16-bit read and a coalesced 32-bit write per entry;
 //   * accumulate (pass 2): a CTA owns one destination bin (16,384 floats,
 //     64 KB of shared memory), walks the bin's blocks (one per source slice,
-//     D-major block table, a half-warp per block) and adds val[e] into its
-//     shared-memory sums at
+//     D-major table, each cut into chunks of at most 256 entries, a
+//     half-warp per chunk) and adds val[e] into its shared-memory sums at
 //     the destination offset (equal destinations, adjacent in a block, are
 //     summed in registers and across lanes first: one atomic per run), then
 //     writes the bin's sums to y.
@@ -51,7 +51,7 @@ constexpr int kGatherCtas = 3;       // resident gather CTAs per SM (64 KB of x 
 constexpr int kGatherGroups = 4;     // 8-entry groups in flight per gather thread
 constexpr int kAccThreads = 512;
 constexpr int kAccCtas = 3;          // resident accumulate CTAs per SM (the bin's sums each)
-constexpr int kAccGroups = 1;        // 8-entry groups in flight per accumulate lane
+constexpr int kAccGroups = 2;        // 8-entry groups in flight per accumulate lane
 constexpr long long kWaitLimit = 1ll << 24;
 // Blocks are padded to a multiple of 8 entries; a padding entry points at
 // offset 0 of its slice (its value is read and never added) and at
@@ -117,8 +117,13 @@ __global__ void __launch_bounds__(kGatherThreads, kGatherCtas)
         const bool got = wait_bar(&m.bar, parity);
         parity ^= 1;
         if (!__syncthreads_and(got)) {
-            if (tid == 0) atomicExch(error, 1);
-            break;   // uniform; nothing else in flight
+            // the copy is late: flag it and give it one more bounded wait, so
+            // that the CTA does not leave with its copy still in flight
+            if (tid == 0) {
+                atomicExch(error, 1);
+                wait_bar(&m.bar, parity ^ 1);
+            }
+            break;   // uniform
         }
         const uint64_t e0 = it.e0, end = it.e0 + it.n;
         // head up to a multiple of 8 entries, 8-entry body (16-byte loads,
@@ -156,17 +161,21 @@ __global__ void __launch_bounds__(kGatherThreads, kGatherCtas)
     }
 }
 
-// Adds the 8 consecutive entries of every lane of a half-warp (lane l of
-// the 16: entries 8l .. 8l+7 of the half's 128, sorted by destination;
-// `valid` false for a lane past its block) into the shared sums.  Equal
-// destinations are adjacent, and a run may cross lanes (a high-degree vertex
-// can fill the whole half): a lane sums its runs in registers and adds the
-// ones inside it at once; its first and last runs join the neighbouring
-// lanes' runs through a segmented prefix scan over the 16 lanes, and each
-// run is added once, by the lane where it ends.  Without the cross-lane step
-// all lanes of a run would hit one address in the same atomic instruction.
-// Padding entries carry kPadDst (past every offset) and are never added.
-__device__ __forceinline__ void add_half_groups(float* acc, uint32_t hl, unsigned mask, bool valid, const uint4 d,
+// Adds the 8 entries of every lane of a group of W lanes (lane l of the W:
+// the l-th 8-entry group of a window of the bin's group list, its entries
+// sorted by destination; `valid` false for a lane past the item) into the
+// shared sums.  Equal destinations are adjacent inside a group, and a run may
+// cross lanes (a high-degree vertex can fill many groups of a block; two
+// groups of neighbouring blocks may also end and start on one destination,
+// whose sum is the same either way): a lane sums its runs in registers and
+// adds the ones inside it at once; its first and last runs join the
+// neighbouring lanes' runs through a segmented prefix scan over the W lanes,
+// and each run is added once, by the lane where it ends.  Without the
+// cross-lane step all lanes of a run would hit one address in the same
+// atomic instruction.  Padding entries carry kPadDst (past every offset) and
+// are never added.
+template <int W>
+__device__ __forceinline__ void add_lane_groups(float* acc, uint32_t hl, unsigned mask, bool valid, const uint4 d,
                                                 const float4 lo, const float4 hi) {
     const uint32_t o[8] = {d.x & 0xFFFFu, d.x >> 16, d.y & 0xFFFFu, d.y >> 16,
                            d.z & 0xFFFFu, d.z >> 16, d.w & 0xFFFFu, d.w >> 16};
@@ -191,7 +200,7 @@ __device__ __forceinline__ void add_half_groups(float* acc, uint32_t hl, unsigne
         }
     }
     // lane l's first run continues lane l-1's last run when their keys match
-    const uint32_t t_prev = __shfl_up_sync(mask, t, 1, 16);
+    const uint32_t t_prev = __shfl_up_sync(mask, t, 1, W);
     const bool link = hl > 0 && t_prev == f;
     // segmented prefix sums of the last runs: a segment starts at a lane
     // whose first run does not continue the previous lane's, or whose first
@@ -199,32 +208,35 @@ __device__ __forceinline__ void add_half_groups(float* acc, uint32_t hl, unsigne
     float c = run;
     bool head = !single || !link;
 #pragma unroll
-    for (int k = 1; k < 16; k <<= 1) {
-        const float cu = __shfl_up_sync(mask, c, k, 16);
-        const bool hu = __shfl_up_sync(mask, head, k, 16);
+    for (int k = 1; k < W; k <<= 1) {
+        const float cu = __shfl_up_sync(mask, c, k, W);
+        const bool hu = __shfl_up_sync(mask, head, k, W);
         if (hl >= (uint32_t)k && !head) {
             c += cu;
             head = hu;
         }
     }
-    const float carry_in = __shfl_up_sync(mask, c, 1, 16);
-    const bool link_next = __shfl_down_sync(mask, link, 1, 16) && hl < 15;
+    const float carry_in = __shfl_up_sync(mask, c, 1, W);
+    const bool link_next = __shfl_down_sync(mask, link, 1, W) && hl < W - 1;
     if (!valid) return;
     if (!single && f < kDstBin) atomicAdd(acc + f, sf + (link ? carry_in : 0.f));   // first run, closed here
     if (!link_next && t < kDstBin) atomicAdd(acc + t, c);                          // the last run's chain ends here
 }
 
-// Pass 2.  Item: blocks [b0, b1) of the D-major block table, all of bin
-// `bin`; `whole` when the item holds every block of the bin (its sums are
-// then stored, else added to y).
+// Pass 2.  Item: groups [b0, b1) of the group list, all of bin `bin`;
+// `whole` when the item holds every group of the bin (its sums are then
+// stored, else added to y).  A warp takes windows of 32 consecutive groups
+// (a lane per group: one 4-byte group index, then one 16-byte load of
+// destination offsets and two of values), kAccGroups windows in flight.
 __global__ void __launch_bounds__(kAccThreads, kAccCtas)
-    pb_accumulate_kernel(const gs_pb_item2* __restrict__ items, uint64_t n_items,
-                         const gs_pb_block* __restrict__ blocks, const uint16_t* __restrict__ dst,
-                         const float* __restrict__ val, float* __restrict__ y, unsigned int* ticket) {
+    pb_accumulate_kernel(const gs_pb_item2* __restrict__ items, uint64_t n_items, const uint32_t* __restrict__ groups,
+                         const uint16_t* __restrict__ dst, const float* __restrict__ val, float* __restrict__ y,
+                         unsigned int* ticket) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float* acc = reinterpret_cast<float*>(smem_raw);
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     constexpr uint32_t kWarps = kAccThreads / 32;
+    constexpr uint32_t kStep = 32 * kAccGroups;
     __shared__ unsigned long long s_item;
     auto advance = [&](uint64_t i) -> uint64_t {
         if (!ticket) return i + gridDim.x;
@@ -234,38 +246,34 @@ __global__ void __launch_bounds__(kAccThreads, kAccCtas)
         return s_item;
     };
     float4* acc4 = reinterpret_cast<float4*>(acc);
+    const uint4* d8 = reinterpret_cast<const uint4*>(dst);
+    const float4* v4 = reinterpret_cast<const float4*>(val);
     for (uint64_t i = ticket ? advance(0) : blockIdx.x; i < n_items; i = advance(i)) {
         const gs_pb_item2 it = items[i];
         for (uint32_t k = tid; k < kDstBin / 4; k += kAccThreads) acc4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
         __syncthreads();
-        // a half-warp per block (blocks hold a multiple of 8 entries, ~128 at
-        // Kronecker scale 26); a lane takes 8 consecutive entries (one
-        // 16-byte load of offsets, two of values)
-        const uint32_t half = lane >> 4, hl = lane & 15;
-        const unsigned hmask = half ? 0xFFFF0000u : 0x0000FFFFu;
-        const uint4* d8 = reinterpret_cast<const uint4*>(dst);
-        const float4* v4 = reinterpret_cast<const float4*>(val);
-        for (uint32_t bi = it.b0 + 2 * warp + half; bi < it.b1; bi += 2 * kWarps) {
-            const gs_pb_block blk = blocks[bi];
-            const uint64_t g0 = blk.e0 >> 3, ng = blk.n >> 3;
-            for (uint64_t c0 = 0; c0 < ng; c0 += 16 * kAccGroups) {   // uniform in the half
-                uint4 d[kAccGroups];
-                float4 lo[kAccGroups], hi[kAccGroups];
+        for (uint64_t w0 = (uint64_t)it.b0 + warp * kStep; w0 < it.b1; w0 += kWarps * kStep) {   // uniform in the warp
+            uint32_t gi[kAccGroups];
 #pragma unroll
-                for (int k = 0; k < kAccGroups; ++k) {
-                    const uint64_t ck = c0 + 16u * k + hl;
-                    d[k] = make_uint4(0, 0, 0, 0);
-                    lo[k] = hi[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (ck < ng) {
-                        d[k] = __ldcs(d8 + g0 + ck);
-                        lo[k] = __ldcs(v4 + 2 * (g0 + ck));
-                        hi[k] = __ldcs(v4 + 2 * (g0 + ck) + 1);
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < kAccGroups; ++k)
-                    add_half_groups(acc, hl, hmask, c0 + 16u * k + hl < ng, d[k], lo[k], hi[k]);
+            for (int k = 0; k < kAccGroups; ++k) {
+                const uint64_t gk = w0 + 32u * k + lane;
+                gi[k] = gk < it.b1 ? __ldcs(groups + gk) : 0u;
             }
+            uint4 d[kAccGroups];
+            float4 lo[kAccGroups], hi[kAccGroups];
+#pragma unroll
+            for (int k = 0; k < kAccGroups; ++k) {
+                d[k] = make_uint4(0, 0, 0, 0);
+                lo[k] = hi[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (w0 + 32u * k + lane < it.b1) {
+                    d[k] = __ldcs(d8 + gi[k]);
+                    lo[k] = __ldcs(v4 + 2 * (uint64_t)gi[k]);
+                    hi[k] = __ldcs(v4 + 2 * (uint64_t)gi[k] + 1);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kAccGroups; ++k)
+                add_lane_groups<32>(acc, lane, 0xFFFFFFFFu, w0 + 32u * k + lane < it.b1, d[k], lo[k], hi[k]);
         }
         __syncthreads();
         float4* y4 = reinterpret_cast<float4*>(y + ((uint64_t)it.bin << kPbDstBits));
@@ -373,6 +381,21 @@ __global__ void pb_block_table_kernel(const uint64_t* __restrict__ start, uint32
     }
 }
 
+// The group list: block p of the D-major table (entries [e0, e0 + n), n a
+// multiple of 8) lists its groups e0/8 .. (e0 + n)/8 - 1 from gpos[p] on.
+// A warp per block.
+__global__ void pb_group_list_kernel(const gs_pb_block* __restrict__ blocks, const uint64_t* __restrict__ gpos,
+                                     uint64_t n_blk, uint32_t* __restrict__ groups) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t n_warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t p = warp; p < n_blk; p += n_warps) {
+        const gs_pb_block b = blocks[p];
+        const uint64_t g0 = b.e0 >> 3, out = gpos[p];
+        for (uint32_t k = lane; k < (b.n >> 3); k += 32) groups[out + k] = (uint32_t)(g0 + k);
+    }
+}
+
 inline uint32_t grid_for(uint64_t n, const gs_ctx* ctx) {
     const uint64_t b = (n + 255) / 256;
     return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(b, gs_grid_size(ctx, 16)));
@@ -385,7 +408,7 @@ void pb_layout_free(gs_graph* g) {
     gs_dev_free(L.d_src);
     gs_dev_free(L.d_dst);
     gs_dev_free(L.d_val);
-    gs_dev_free(L.d_blocks);
+    gs_dev_free(L.d_groups);
     gs_dev_free(L.d_items1);
     gs_dev_free(L.d_items2);
     L = gs_pb_layout();
@@ -396,14 +419,14 @@ bool pb_layout_wanted(const gs_graph* g) {
     const uint64_t n_ent = g->directed ? g->E : 2 * g->E;
     const uint64_t nS = g->N >> kPbSrcBits, nD = g->N >> kPbDstBits;
     // the block table is dense (every (S, D) pair): worth it when blocks hold
-    // many entries on average
-    if (nS * nD * 64 > n_ent || nS * nD >= (1ull << 31)) return false;
+    // many entries on average; group indices (entry / 8) are 32-bit
+    if (nS * nD * 64 > n_ent || nS * nD >= (1ull << 31) || n_ent + 8 * nS * nD >= (1ull << 34)) return false;
     // under an HBM budget the layout (8 B per entry) must fit beside the records
     if (g->ctx->budget && 4 * g->E + 8 * n_ent > g->ctx->budget) return false;
     // building needs the sort's two key buffers too
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return false;
-    const uint64_t need = (n_ent + 8 * nS * nD) * 8 + n_ent * 16 + (nS * nD + 1) * 32 + (2ull << 30);
+    const uint64_t need = (n_ent + 8 * nS * nD) * 8 + n_ent / 2 + n_ent * 16 + (nS * nD + 1) * 40 + (2ull << 30);
     // (idle pool blocks count as free: an allocation that fails releases them)
     return free_b + g->ctx->pool_bytes > need;
 }
@@ -419,6 +442,7 @@ gs_status pb_layout_build(gs_graph* g) {
     while ((1ull << (end_bit - kKeyLowBits)) < n_blk) ++end_bit;
 
     uint64_t *d_k0 = nullptr, *d_k1 = nullptr, *d_start = nullptr, *d_pstart = nullptr;
+    gs_pb_block* d_blocks = nullptr;   // the D-major block table (build only)
     uint64_t n_pad = 0;   // entries with every block padded to a multiple of 8
     void* d_tmp = nullptr;
     size_t tmp_bytes = 0;
@@ -463,11 +487,11 @@ gs_status pb_layout_build(gs_graph* g) {
         }
         if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_src, n_pad * 2);
         if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_dst, n_pad * 2);
-        if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_blocks, std::max<uint64_t>(1, n_blk) * sizeof(gs_pb_block));
+        if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&d_blocks, std::max<uint64_t>(1, n_blk) * sizeof(gs_pb_block));
         if (st == GS_OK) {
             pb_split_kernel<<<gs_grid_size(ctx, 8), 256, 0, ctx->stream>>>(sorted, d_start, d_pstart, n_blk, L.d_src,
                                                                             L.d_dst);
-            pb_block_table_kernel<<<grid_for(n_blk, ctx), 256, 0, ctx->stream>>>(d_pstart, nS, nD, L.d_blocks);
+            pb_block_table_kernel<<<grid_for(n_blk, ctx), 256, 0, ctx->stream>>>(d_pstart, nS, nD, d_blocks);
             ctx->launches += 2;
             e = cudaGetLastError();
             if (e != cudaSuccess) st = gs_cuda_fail(ctx, e, "propagation-blocking layout");
@@ -478,7 +502,7 @@ gs_status pb_layout_build(gs_graph* g) {
     std::vector<gs_pb_block> blocks(n_blk);
     std::vector<uint64_t> slice_start(nS + 1);
     if (st == GS_OK) {
-        cudaError_t e = cudaMemcpyAsync(blocks.data(), L.d_blocks, n_blk * sizeof(gs_pb_block),
+        cudaError_t e = cudaMemcpyAsync(blocks.data(), d_blocks, n_blk * sizeof(gs_pb_block),
                                         cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         // entries of slice S start at block (S, 0), the first of the bin-major table
@@ -489,66 +513,55 @@ gs_status pb_layout_build(gs_graph* g) {
     gs_dev_free(d_start);
     gs_dev_free(d_pstart);
     if (st != GS_OK) {
+        gs_dev_free(d_blocks);
         pb_layout_free(g);
         return st;
     }
-    // Items: entry chunks of every slice (pass 1) and block ranges of every
-    // bin (pass 2), sized so that each pass has a few items per resident CTA.
+    // The group list the accumulate pass walks: every bin's blocks in slice
+    // order, as 8-entry groups, so that a bin is one flat sequence of groups
+    // however its entries are spread over blocks (a lane per group).
+    std::vector<uint64_t> gpos(n_blk + 1);
+    gpos[0] = 0;
+    for (uint64_t b = 0; b < n_blk; ++b) gpos[b + 1] = gpos[b] + (blocks[b].n >> 3);
+    const uint64_t n_groups = gpos[n_blk];
+    // Items: entry chunks of every slice (pass 1) and group ranges of every
+    // bin (pass 2), sized so that each pass has a few items per resident CTA
+    // (pass 2: ~16, so that the last wave of equal items leaves few SMs idle).
     // (item boundaries stay multiples of 8 entries: every block starts on one)
     const uint64_t per1 =
         std::clamp<uint64_t>(n_pad / ((uint64_t)ctx->num_sms * kGatherCtas * 4), 32768, 1ull << 20) & ~7ull;
-    const uint64_t per2 = std::clamp<uint64_t>(n_pad / ((uint64_t)ctx->num_sms * kAccCtas * 4), 65536, 1ull << 22);
+    const uint64_t per2 =
+        std::clamp<uint64_t>(n_groups / ((uint64_t)ctx->num_sms * kAccCtas * 16), 8192, 1ull << 19);
     std::vector<gs_pb_item1> items1;
     for (uint32_t s = 0; s < nS; ++s)
         for (uint64_t e = slice_start[s]; e < slice_start[s + 1]; e += per1)
             items1.push_back(gs_pb_item1{e, (uint32_t)std::min<uint64_t>(per1, slice_start[s + 1] - e), s});
-    // The table the accumulate pass walks: each bin's blocks in slice order,
-    // cut into chunks of at most kChunk entries (a half-warp's two passes), so
-    // that the few large blocks of a small graph spread over the CTA's
-    // half-warps; empty blocks dropped.
-    constexpr uint32_t kChunk = 256;
-    std::vector<gs_pb_block> table;
-    std::vector<uint64_t> bin_first(nD + 1);
-    table.reserve(n_blk);
-    for (uint32_t d = 0; d < nD; ++d) {
-        bin_first[d] = table.size();
-        for (uint32_t b = d * nS; b < (d + 1) * nS; ++b)
-            for (uint64_t k = 0; k < blocks[b].n; k += kChunk)
-                table.push_back(gs_pb_block{blocks[b].e0 + k, (uint32_t)std::min<uint64_t>(kChunk, blocks[b].n - k), 0u});
-    }
-    bin_first[nD] = table.size();
     std::vector<gs_pb_item2> items2;
     for (uint32_t d = 0; d < nD; ++d) {
-        const uint32_t first = (uint32_t)items2.size();
-        uint64_t acc = 0;
-        uint32_t b0 = (uint32_t)bin_first[d];
-        for (uint32_t b = b0; b < bin_first[d + 1]; ++b) {
-            if (acc > 0 && acc + table[b].n > per2) {
-                items2.push_back(gs_pb_item2{b0, b, d, 0u});
-                b0 = b;
-                acc = 0;
-            }
-            acc += table[b].n;
-        }
-        if (acc > 0) items2.push_back(gs_pb_item2{b0, (uint32_t)bin_first[d + 1], d, 0u});
-        if (items2.size() == first + 1) items2.back().whole = 1;
+        const uint64_t g0 = gpos[(uint64_t)d * nS], g1 = gpos[(uint64_t)(d + 1) * nS];
+        const uint64_t parts = (g1 - g0 + per2 - 1) / per2;
+        for (uint64_t k = 0; k < parts; ++k)
+            items2.push_back(gs_pb_item2{(uint32_t)(g0 + (g1 - g0) * k / parts),
+                                         (uint32_t)(g0 + (g1 - g0) * (k + 1) / parts), d, parts == 1 ? 1u : 0u});
     }
     L.n_entries = n_pad;
-    L.n_blocks = table.size();
+    L.n_groups = n_groups;
     L.n_items1 = items1.size();
     L.n_items2 = items2.size();
+    uint64_t* d_gpos = nullptr;
     st = gs_dev_alloc(ctx, (void**)&L.d_val, n_pad * 4);
+    if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_groups, std::max<uint64_t>(1, n_groups) * 4);
+    if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&d_gpos, (n_blk + 1) * 8);
     if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_items1, std::max<size_t>(1, items1.size()) * sizeof(gs_pb_item1));
     if (st == GS_OK) st = gs_dev_alloc(ctx, (void**)&L.d_items2, std::max<size_t>(1, items2.size()) * sizeof(gs_pb_item2));
     cudaError_t e = cudaSuccess;
-    if (st == GS_OK && table.size() > n_blk) {   // more chunks than blocks: a larger table
-        gs_dev_free(L.d_blocks);
-        L.d_blocks = nullptr;
-        st = gs_dev_alloc(ctx, (void**)&L.d_blocks, table.size() * sizeof(gs_pb_block));
+    if (st == GS_OK)
+        e = cudaMemcpyAsync(d_gpos, gpos.data(), (n_blk + 1) * 8, cudaMemcpyHostToDevice, ctx->stream);
+    if (st == GS_OK && e == cudaSuccess) {
+        pb_group_list_kernel<<<gs_grid_size(ctx, 8), 256, 0, ctx->stream>>>(d_blocks, d_gpos, n_blk, L.d_groups);
+        ctx->launches++;
+        e = cudaGetLastError();
     }
-    if (st == GS_OK && !table.empty())
-        e = cudaMemcpyAsync(L.d_blocks, table.data(), table.size() * sizeof(gs_pb_block), cudaMemcpyHostToDevice,
-                            ctx->stream);
     if (st == GS_OK && e == cudaSuccess && !items1.empty())
         e = cudaMemcpyAsync(L.d_items1, items1.data(), items1.size() * sizeof(gs_pb_item1), cudaMemcpyHostToDevice,
                             ctx->stream);
@@ -557,6 +570,8 @@ gs_status pb_layout_build(gs_graph* g) {
                             ctx->stream);
     if (st == GS_OK && e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (st == GS_OK && e != cudaSuccess) st = gs_cuda_fail(ctx, e, "propagation-blocking items");
+    gs_dev_free(d_gpos);
+    gs_dev_free(d_blocks);
     if (st != GS_OK) {
         pb_layout_free(g);
         return st;
@@ -576,7 +591,7 @@ gs_status pb_sweep(gs_graph* g, const float* x, float* y, int* error) {
                                                                              L.d_val, error, ctx->d_ticket + 4);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     const uint32_t g2 = (uint32_t)std::min<uint64_t>(L.n_items2, gs_grid_size(ctx, kAccCtas));
-    pb_accumulate_kernel<<<g2, kAccThreads, kDstBin * 4, ctx->stream>>>(L.d_items2, L.n_items2, L.d_blocks, L.d_dst,
+    pb_accumulate_kernel<<<g2, kAccThreads, kDstBin * 4, ctx->stream>>>(L.d_items2, L.n_items2, L.d_groups, L.d_dst,
                                                                        L.d_val, y, ctx->d_ticket + 6);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches += 2;
@@ -595,7 +610,7 @@ gs_status pb_sweep_on(gs_graph* g, cudaStream_t stream, const float* x, float* y
         L.d_items1, L.n_items1, L.d_src, x, val, error, nullptr);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     pb_accumulate_kernel<<<(uint32_t)L.n_items2, kAccThreads, kDstBin * 4, stream>>>(
-        L.d_items2, L.n_items2, L.d_blocks, L.d_dst, val, y, nullptr);
+        L.d_items2, L.n_items2, L.d_groups, L.d_dst, val, y, nullptr);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches += 2;
     return GS_OK;
