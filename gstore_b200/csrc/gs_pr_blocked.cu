@@ -48,7 +48,7 @@ constexpr uint32_t kDstBin = 1u << kPbDstBits;     // 16,384
 constexpr int kKeyLowBits = kPbSrcBits + kPbDstBits;
 constexpr int kGatherThreads = 512;
 constexpr int kGatherCtas = 3;       // resident gather CTAs per SM (64 KB of x each)
-constexpr int kGatherGroups = 4;     // 8-entry groups in flight per gather thread
+constexpr int kGatherGroups = 2;     // 8-entry groups per gather thread and step (two steps in flight)
 constexpr int kAccThreads = 512;
 constexpr int kAccCtas = 3;          // resident accumulate CTAs per SM (the bin's sums each)
 constexpr int kAccGroups = 2;        // 8-entry groups in flight per accumulate lane
@@ -135,22 +135,32 @@ __global__ void __launch_bounds__(kGatherThreads, kGatherCtas)
         const uint4* s8 = reinterpret_cast<const uint4*>(src);
         float4* v4 = reinterpret_cast<float4*>(val);
         const uint64_t c1 = b >> 3;
-        for (uint64_t c = (a >> 3) + tid; c < c1; c += (uint64_t)kGatherThreads * kGatherGroups) {
-            uint4 w[kGatherGroups];
+        auto emit = [&](const uint4 w, uint64_t ck) {
+            v4[2 * ck] = make_float4(m.xs[w.x & 0xFFFFu], m.xs[w.x >> 16], m.xs[w.y & 0xFFFFu], m.xs[w.y >> 16]);
+            v4[2 * ck + 1] = make_float4(m.xs[w.z & 0xFFFFu], m.xs[w.z >> 16], m.xs[w.w & 0xFFFFu], m.xs[w.w >> 16]);
+        };
+        // the next groups' offsets are loaded before this one's are used, so
+        // the loads overlap the shared-memory gathers and the stores
+        constexpr uint64_t kStride = (uint64_t)kGatherThreads * kGatherGroups;
+        uint4 w[kGatherGroups];
+        uint64_t c = (a >> 3) + tid;
+#pragma unroll
+        for (int k = 0; k < kGatherGroups; ++k) {
+            const uint64_t ck = c + (uint64_t)k * kGatherThreads;
+            if (ck < c1) w[k] = __ldcs(s8 + ck);
+        }
+        for (; c < c1; c += kStride) {
+            uint4 nw[kGatherGroups];
 #pragma unroll
             for (int k = 0; k < kGatherGroups; ++k) {
-                const uint64_t ck = c + (uint64_t)k * kGatherThreads;
-                if (ck < c1) w[k] = __ldcs(s8 + ck);
+                const uint64_t ck = c + kStride + (uint64_t)k * kGatherThreads;
+                nw[k] = ck < c1 ? __ldcs(s8 + ck) : make_uint4(0, 0, 0, 0);
             }
 #pragma unroll
             for (int k = 0; k < kGatherGroups; ++k) {
                 const uint64_t ck = c + (uint64_t)k * kGatherThreads;
-                if (ck < c1) {
-                    v4[2 * ck] = make_float4(m.xs[w[k].x & 0xFFFFu], m.xs[w[k].x >> 16], m.xs[w[k].y & 0xFFFFu],
-                                             m.xs[w[k].y >> 16]);
-                    v4[2 * ck + 1] = make_float4(m.xs[w[k].z & 0xFFFFu], m.xs[w[k].z >> 16],
-                                                 m.xs[w[k].w & 0xFFFFu], m.xs[w[k].w >> 16]);
-                }
+                if (ck < c1) emit(w[k], ck);
+                w[k] = nw[k];
             }
         }
         __syncthreads();   // xs is rewritten by the next item
