@@ -763,6 +763,14 @@ def bench_batched(ctx, torch, gs, checks: bool):
     batch_pass(got)
     same = all(np.array_equal(arr, want[key]) for key, arr in got)
     del want, got
+    # each distinct query alone: no batch can finish before its longest
+    # query does on the whole GPU, so sum / max bounds the speed-up
+    alone = []
+    for gg, a, k in distinct:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        plain_pass([(gg, a, k)])
+        alone.append(time.perf_counter() - t0)
     t_all, t_dist, t_batch, kernel_ms = [], [], [], []
     for _ in range(3):
         torch.cuda.synchronize()
@@ -785,6 +793,8 @@ def bench_batched(ctx, torch, gs, checks: bool):
                         "plain_distinct_queries_per_s": len(qs) / t_dist,
                         "speedup_without_dedup_credit": t_dist / t_batch,
                         "batched_kernel_ms": float(np.median(kernel_ms)), "launches": st["launches"],
+                        "longest_query_alone_ms": max(alone) * 1e3,
+                        "speedup_bound_distinct": sum(alone) / max(alone),
                         "results_equal_plain": same,
                         "note": "the batch runs identical queries once; speedup_without_dedup_credit lets the plain "
                                 "loop skip them too"}
