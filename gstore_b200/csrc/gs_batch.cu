@@ -806,9 +806,15 @@ gs_status run_wk_queries(gs_batch* b, std::vector<int>& idx) {
         GS_CHECK_CUDA(ctx, cudaEventRecord(b->e0, ctx->stream));
         GS_CHECK_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)wk_batch_kernel, dim3(grid), dim3(kThreads), args,
                                                        0, ctx->stream));
-        GS_CHECK_CUDA(ctx, cudaEventRecord(b->e1, ctx->stream));
         ctx->launches += 1;
         b->launches += 1;
+        for (const BQuery& d : dq) {   // WCC post-processing, like the label kernels (not a batch launch)
+            if (d.algo != GS_ALGO_WCC) continue;
+            wcc_mark_touched<<<blocks_for(d.words * 32, ctx), kThreads, 0, ctx->stream>>>(d.parent, d.touched,
+                                                                                         d.words * 32);
+            ctx->launches += 1;
+        }
+        GS_CHECK_CUDA(ctx, cudaEventRecord(b->e1, ctx->stream));
         std::vector<int> h_sweeps(nq);
         int h_err = 0;
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(h_sweeps.data(), sweeps, nq * sizeof(int), cudaMemcpyDeviceToHost,

@@ -138,6 +138,22 @@ __device__ __forceinline__ uint32_t find_root_halving(uint32_t* parent, uint32_t
     }
 }
 
+// After the hooking sweeps: marks every vertex that some record joined to
+// another -- every vertex whose parent is not itself, and every parent of
+// such a vertex -- as touched (the label kernels give the others
+// invalid_cid).  Hooking only ever links the trees of a record's two ends,
+// so a vertex no record names keeps itself as parent and has no child.
+static __global__ void wcc_mark_touched(const uint32_t* __restrict__ parent, uint8_t* touched, uint64_t N) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = tid; v < N; v += nth) {
+        const uint32_t p = __ldcg(parent + v);
+        if (p == v) continue;
+        touched[v] = 1;
+        if (!touched[p]) touched[p] = 1;   // read first: a component's root is every member's parent
+    }
+}
+
 struct WccOp {
     uint32_t* parent;
     uint8_t* touched;  // non-null on the first sweep
@@ -154,10 +170,11 @@ struct WccOp {
     }
     __device__ void record(uint32_t r, Item& c) const {
         const uint32_t a = c.rb + (r & 0xFFFFu), b = c.cb + (r >> 16);
-        if (touched) {          // wcc.cpp:203-217: every record's ends get a label
-            touched[a] = 1;
-            touched[b] = 1;
-        }
+        // wcc.cpp:203-217: every record's ends get a label.  A record with two
+        // ends joins them into one tree, which wcc_mark_touched finds after
+        // the sweeps (a vertex with a parent, or with a child); only a
+        // self-loop leaves its end alone in its tree, so only it is marked here
+        if (touched && a == b) touched[a] = 1;
         // ends with one parent are in one tree (after pointer jumping most
         // vertices point at their root): two loads instead of four
         if (__ldcg(parent + a) == __ldcg(parent + b)) return;

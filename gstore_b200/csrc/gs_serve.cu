@@ -653,9 +653,10 @@ gs_status take_result(gs_server* s, Request& r) {
     cudaStream_t stream = side_stream_of(s, r);
     switch (r.algo) {
         case GS_ALGO_WCC:
+            wcc_mark_touched<<<short_blocks(g->N), kThreads, 0, stream>>>(r.parent, r.touched, g->N);
             serve_wcc_labels<<<short_blocks(g->V), kThreads, 0, stream>>>(r.parent, r.touched, r.labels,
                                                                                  g->V);
-            s->kernel_launches++;
+            s->kernel_launches += 2;
             src = r.labels;
             r.result_bytes = g->V * 4;
             break;

@@ -516,10 +516,11 @@ gs_status gs_wcc_labels(gs_state* s, uint32_t* d_out, uint64_t* count) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
     GS_TRY(zero_scalar(ctx));
+    wcc_mark_touched<<<blocks_for(g->N, ctx), kThreads, 0, ctx->stream>>>(s->d_parent, s->d_touched, g->N);
     wcc_label_kernel<<<blocks_for(g->N, ctx), kThreads, 0, ctx->stream>>>(
         s->d_parent, s->d_touched, d_out, g->N, (unsigned long long*)ctx->d_scalars);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
-    ctx->launches++;
+    ctx->launches += 2;
     return read_scalar(ctx, count);
 }
 
