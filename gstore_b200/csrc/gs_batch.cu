@@ -344,6 +344,8 @@ struct BQuery {
 };
 
 constexpr int kMaxBatch = 64;
+constexpr int kMsCtasPerSm = 4;   // multi-source BFS launches
+constexpr int kWkCtasPerSm = 8;   // WCC / k-core launches (their sweeps wait on dependent loads)
 
 struct BatchArgs {
     BQuery* q;
@@ -598,11 +600,14 @@ gs_status scratch(gs_batch* b, size_t bytes, void** out) {
     return GS_OK;
 }
 
-int coop_grid(gs_ctx* ctx, const void* kernel) {
+// Resident CTAs of a cooperative launch: every SM's share, at most `cap`
+// per SM (fewer CTAs make the grid barriers cheaper; latency-bound sweeps
+// want more warps).
+int coop_grid(gs_ctx* ctx, const void* kernel, int cap) {
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess || per_sm < 1)
         per_sm = 1;
-    return ctx->num_sms * std::min(per_sm, 4);
+    return ctx->num_sms * std::min(per_sm, cap);
 }
 
 // One multi-source BFS launch over the queries of group `gi`.
@@ -681,7 +686,7 @@ gs_status run_bfs_group(gs_batch* b, gs_bfs_group& grp) {
                                                        dim3(ctx->num_sms * per_sm), dim3(kSliceThreads), args, smem,
                                                        ctx->stream));
     } else {
-        const int grid = coop_grid(ctx, (const void*)msbfs_kernel<W>);
+        const int grid = coop_grid(ctx, (const void*)msbfs_kernel<W>, kMsCtasPerSm);
         GS_CHECK_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)msbfs_kernel<W>, dim3(grid), dim3(kThreads), args,
                                                        0, ctx->stream));
     }
@@ -802,7 +807,7 @@ gs_status run_wk_queries(gs_batch* b, std::vector<int>& idx) {
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(d_q, dq.data(), nq * sizeof(BQuery), cudaMemcpyHostToDevice, ctx->stream));
         BatchArgs a{d_q, nq, bar, err, tickets};
         void* args[] = {&a};
-        const int grid = coop_grid(ctx, (const void*)wk_batch_kernel);
+        const int grid = coop_grid(ctx, (const void*)wk_batch_kernel, kWkCtasPerSm);
         GS_CHECK_CUDA(ctx, cudaEventRecord(b->e0, ctx->stream));
         GS_CHECK_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)wk_batch_kernel, dim3(grid), dim3(kThreads), args,
                                                        0, ctx->stream));
