@@ -121,12 +121,10 @@ __device__ __forceinline__ uint32_t find_root(const uint32_t* parent, uint32_t v
 }
 
 // find_root with path halving: every vertex passed on the way points to its
-// grandparent afterwards.  Hooking only lowers pointers toward smaller ids,
-// so a vertex's grandparent is always one of its ancestors and the forest
-// stays a forest; a plain store that overwrites a concurrent hook loses that
-// hook, which the next sweep redoes (a sweep ends the loop only when it
-// changed nothing).  Without it the hooking sweeps build long parent chains
-// and spend their time chasing them.
+// grandparent afterwards.  Only non-roots are written (a vertex that has a
+// parent never becomes a root again), always with one of their ancestors,
+// so the stores never undo a link; without them the hooking sweeps build
+// long parent chains and spend their time chasing them.
 __device__ __forceinline__ uint32_t find_root_halving(uint32_t* parent, uint32_t v) {
     while (true) {
         const uint32_t p = __ldcg(parent + v);
@@ -136,6 +134,28 @@ __device__ __forceinline__ uint32_t find_root_halving(uint32_t* parent, uint32_t
         __stcg(parent + v, gp);
         v = gp;
     }
+}
+
+// Links the trees of a and b (wcc.cpp:218-231, 263-275: toward the smaller
+// id).  The larger root is linked under the smaller one with a
+// compare-and-swap that succeeds only while it is still a root; when another
+// record linked it first, the roots are found again.  No link is ever lost,
+// so once a sweep has passed every record each record's ends share a root.
+// Returns false only if the retries ran out (the record is left to the next
+// sweep): every failed swap is another record's successful link, so this
+// needs more than kHookRetries links to land on the same two trees while
+// one record is being resolved.
+constexpr int kHookRetries = 1 << 12;
+__device__ __forceinline__ bool hook(uint32_t* parent, uint32_t a, uint32_t b) {
+    uint32_t ra = find_root_halving(parent, a), rb = find_root_halving(parent, b);
+    for (int i = 0; i < kHookRetries; ++i) {
+        if (ra == rb) return true;
+        const uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
+        if (atomicCAS(parent + hi, hi, lo) == hi) return true;
+        ra = find_root_halving(parent, hi);
+        rb = find_root_halving(parent, lo);
+    }
+    return false;
 }
 
 // After the hooking sweeps: marks every vertex that some record joined to
@@ -157,7 +177,7 @@ static __global__ void wcc_mark_touched(const uint32_t* __restrict__ parent, uin
 struct WccOp {
     uint32_t* parent;
     uint8_t* touched;  // non-null on the first sweep
-    unsigned long long* changes;
+    unsigned long long* changes;   // records the sweep left unresolved (zero: the forest is final)
     struct Item {
         uint32_t rb, cb;
         uint32_t n;
@@ -178,11 +198,7 @@ struct WccOp {
         // ends with one parent are in one tree (after pointer jumping most
         // vertices point at their root): two loads instead of four
         if (__ldcg(parent + a) == __ldcg(parent + b)) return;
-        const uint32_t ra = find_root_halving(parent, a), rb = find_root_halving(parent, b);
-        if (ra != rb) {         // wcc.cpp:218-231, 263-275: hook toward the smaller
-            const uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
-            if (atomicMin(parent + hi, lo) > lo) c.n += 1;
-        }
+        if (!hook(parent, a, b)) c.n += 1;
     }
     __device__ void end(uint32_t, uint32_t, Item& c) const { warp_add_u64(changes, c.n); }
 };

@@ -20,7 +20,7 @@
 //     without waiting, each kernel first reading the request's device-side
 //     done flag, and the host polls one event per chunk.  WCC: hooking sweep
 //     (wcc.cpp:177-278) + pointer jumping (wcc.cpp:372-390), done when a
-//     sweep changed nothing; k-core: round (kcore.cpp:179-217, first) +
+//     sweep left no record unresolved; k-core: round (kcore.cpp:179-217, first) +
 //     decrement sweep (kcore.cpp:63-177), done when a round removed
 //     nothing; PageRank: row-slice sweep + update, `arg` iterations.
 //
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kThreads) side_sweep_kernel(const gs_tile_run*
 }
 
 // WCC after sweep `it`: pointer jumping (wcc.cpp:372-390); done when the
-// sweep hooked nothing.
+// sweep left no record unresolved (normally after the first).
 __global__ void side_wcc_post(uint32_t* parent, uint64_t N, unsigned long long* cnt, int it, int* done) {
     if (__ldcg(done)) return;
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
