@@ -79,8 +79,9 @@ def parse_args():
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="length of the Poisson arrival trace")
     ap.add_argument("--stream-scale", type=int, default=28)
     ap.add_argument("--stream-budget-gb", type=float, default=4.0)
-    ap.add_argument("--case", choices=["bfs", "pagerank", "wcc", "kcore"],
-                    help="profiling case: build the --scale graph, run this algorithm once, print its time, exit")
+    ap.add_argument("--case", choices=["bfs", "pagerank", "wcc", "kcore", "msbfs", "wk-mix"],
+                    help="profiling case: build the --scale graph, run this algorithm once (msbfs: 64 seeded "
+                         "roots in one batch; wk-mix: the batched WCC / k-core mix), print its time, exit")
     ap.add_argument("--case-arg", type=int, default=None,
                     help="the case's argument (PageRank iterations, k of k-core; default 2 and 8)")
     return ap.parse_args()
@@ -1082,6 +1083,38 @@ def main():
     del d_pairs
     torch.cuda.empty_cache()
     degree = graph.degree()
+    if args.case in ("msbfs", "wk-mix"):
+        # one batch, for a profiler's capture (not a bench line)
+        t0 = time.perf_counter()
+        graphs = [graph]
+        if args.case == "msbfs":   # the autotuner tries each configuration once first
+            for _ in range(8):
+                with gs.Batch(ctx) as b:
+                    for r in splitmix64_roots(degree, 64, seed=1):
+                        b.add(graph, "bfs", r)
+                    b.run()
+        with gs.Batch(ctx) as b:
+            if args.case == "msbfs":
+                for r in splitmix64_roots(degree, 64, seed=1):
+                    b.add(graph, "bfs", r)
+            else:
+                graphs = [make_graph(ctx, torch, 18 + (i % 5), 16, seed1=i + 1) for i in range(8)]
+                rng = np.random.default_rng(1)
+                ks = [int(k) for k in rng.integers(4, 33, 16)]
+                for i in range(16):
+                    b.add(graphs[i % 8], "wcc", 0)
+                for i in range(16):
+                    b.add(graphs[i % 8], "kcore", ks[i])
+            b.run()
+            torch.cuda.synchronize()
+            st = b.stats()
+        print(json.dumps({"case": args.case, "scale": scale, "batch_kernel_ms": st["kernel_ms"],
+                          "ms_incl_setup": (time.perf_counter() - t0) * 1e3}))
+        for gg in graphs:
+            gg.free()
+        ctx.close()
+        dist.close()
+        return
     if args.case:
         # one query of one algorithm, for a profiler's capture (not a bench line)
         arg = args.case_arg
