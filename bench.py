@@ -79,9 +79,10 @@ def parse_args():
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="length of the Poisson arrival trace")
     ap.add_argument("--stream-scale", type=int, default=28)
     ap.add_argument("--stream-budget-gb", type=float, default=4.0)
-    ap.add_argument("--case", choices=["bfs", "pagerank", "wcc", "kcore", "msbfs", "wk-mix"],
+    ap.add_argument("--case", choices=["bfs", "pagerank", "wcc", "kcore", "msbfs", "wk-mix", "serve"],
                     help="profiling case: build the --scale graph, run this algorithm once (msbfs: 64 seeded "
-                         "roots in one batch; wk-mix: the batched WCC / k-core mix), print its time, exit")
+                         "roots in one batch; wk-mix: the batched WCC / k-core mix; serve: the first 500 "
+                         "requests of the serving trace, all at once), print its time, exit")
     ap.add_argument("--case-arg", type=int, default=None,
                     help="the case's argument (PageRank iterations, k of k-core; default 2 and 8)")
     return ap.parse_args()
@@ -1083,6 +1084,31 @@ def main():
     del d_pairs
     torch.cuda.empty_cache()
     degree = graph.degree()
+    if args.case == "serve":
+        graph.free()
+        graphs = [make_graph(ctx, torch, 16 + (i % 9), (8, 16, 32)[i % 3], seed1=i + 1) for i in range(16)]
+        trace = poisson_trace(graphs, 1.0, 2000.0)[:500]
+        t0 = time.perf_counter()
+        with gs.Server(ctx) as srv:
+            gids = [srv.add_graph(g) for g in graphs]
+            for _, gi, a, arg in trace:
+                srv.submit(gids[gi], a, arg)
+            n = 0
+            while True:
+                na, nq = srv.step()
+                for rid in srv.completed():
+                    srv.result(rid, want_data=False)
+                    n += 1
+                if na == 0 and nq == 0:
+                    break
+            st = srv.stats()
+        print(json.dumps({"case": "serve", "requests": n, "steps": st["steps"],
+                          "ms": (time.perf_counter() - t0) * 1e3}))
+        for gg in graphs:
+            gg.free()
+        ctx.close()
+        dist.close()
+        return
     if args.case in ("msbfs", "wk-mix"):
         # one batch, for a profiler's capture (not a bench line)
         t0 = time.perf_counter()
