@@ -50,6 +50,7 @@ ABI_SYMBOLS = [
     "gs_serve_create", "gs_serve_add_graph", "gs_serve_submit", "gs_serve_step", "gs_serve_poll",
     "gs_serve_result", "gs_serve_clock", "gs_serve_stats", "gs_serve_free", "gs_serve_completed",
     "gs_serve_set_side_streams", "gs_serve_result_view", "gs_serve_release", "gs_serve_profile",
+    "gs_serve_reserve_host",
 ]
 
 
@@ -130,6 +131,7 @@ def lib():
                                      C.POINTER(C.c_double), C.POINTER(C.c_int64)],
             "gs_serve_release": [vp, u64],
             "gs_serve_profile": [vp, C.POINTER(C.c_double), i32],
+            "gs_serve_reserve_host": [vp, u64],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -495,10 +497,17 @@ class Server:
         return {"steps": a.value, "graph_launches": b.value, "kernel_launches": c.value, "hbm_in_use": d.value}
 
     def profile(self):
-        """Host seconds in gs_serve_step by phase."""
-        out = (C.c_double * 4)()
-        self.ctx._check(lib().gs_serve_profile(self._h, out, 4))
-        return {"admit_s": out[0], "step_launch_s": out[1], "side_s": out[2], "step_finish_s": out[3]}
+        """Host seconds in gs_serve_step by phase, and the pool misses
+        (pinned host and device allocations) made inside those phases."""
+        out = (C.c_double * 8)()
+        self.ctx._check(lib().gs_serve_profile(self._h, out, 8))
+        return {"admit_s": out[0], "step_launch_s": out[1], "side_s": out[2], "step_finish_s": out[3],
+                "pinned_alloc_s": out[4], "pinned_allocs": int(out[5]), "device_alloc_s": out[6],
+                "device_allocs": int(out[7])}
+
+    def reserve_host(self, nbytes: int):
+        """Pins nbytes into the server's result arena ahead of the requests."""
+        self.ctx._check(lib().gs_serve_reserve_host(self._h, int(nbytes)))
 
     def free(self):
         if self._h:

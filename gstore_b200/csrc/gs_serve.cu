@@ -41,6 +41,7 @@
 #include <map>
 #include <memory>
 #include <new>
+#include <set>
 #include <unordered_map>
 #include <vector>
 
@@ -55,7 +56,9 @@ constexpr int kMaxJobs = 256;
 constexpr int kCounters = 4;
 constexpr int kSideSlots = 64;
 constexpr int kSideStreams = 8;
-constexpr int kWccChunk = 4;        // iterations queued per chunk
+// iterations queued per chunk: one WCC sweep normally finishes (its hooks
+// lose no link), so a WCC chunk is one sweep and its pointer jumping
+constexpr int kWccChunk = 1;
 constexpr int kKcoreChunk = 8;
 
 typedef FvPair<unsigned long long> Fv64;
@@ -381,12 +384,22 @@ struct gs_server {
     int step = 0;
     uint64_t steps_run = 0, graph_launches = 0, kernel_launches = 0;
     // host seconds spent in gs_serve_step by phase: admission, BFS step
-    // launch, side requests, BFS step finish (its wait included), retirement
-    double phase_s[4] = {0, 0, 0, 0};
+    // launch, side requests, BFS step finish (its wait included); then the
+    // seconds and count of pinned-host and device allocations made on pool
+    // misses (inside those phases)
+    double phase_s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double side_in_wait_s = 0;           // side tending inside the step wait
     std::chrono::steady_clock::time_point t0;
-    // pools: exact-size free lists
-    std::multimap<size_t, void*> dev_free, host_free;
-    std::vector<void*> dev_all, host_all;
+    // device pool: exact-size free lists
+    std::multimap<size_t, void*> dev_free;
+    std::vector<void*> dev_all;
+    // pinned host arena for results: chunks from cudaHostAlloc, carved
+    // best-fit into page-rounded blocks; a freed block merges with free
+    // neighbours of the same chunk
+    std::vector<std::pair<char*, size_t>> host_chunks;
+    std::set<char*> chunk_starts;
+    std::map<char*, size_t> host_free_at;           // free blocks by address
+    std::multimap<size_t, char*> host_free_size;    // the same blocks by size
 };
 
 namespace {
@@ -407,7 +420,10 @@ gs_status pool_dev(gs_server* s, size_t bytes, void** out) {
         s->dev_free.erase(it);
         return GS_OK;
     }
+    const double t = now_s(s);
     GS_TRY(gs_dev_alloc(s->ctx, out, bytes));
+    s->phase_s[6] += now_s(s) - t;
+    s->phase_s[7] += 1;
     s->dev_all.push_back(*out);
     return GS_OK;
 }
@@ -416,16 +432,75 @@ void pool_dev_put(gs_server* s, void* p, size_t bytes) {
     if (p) s->dev_free.emplace((bytes + 255) & ~(size_t)255, p);
 }
 
-gs_status pool_host(gs_server* s, size_t bytes, void** out) {
-    bytes = (bytes + 255) & ~(size_t)255;
-    auto it = s->host_free.find(bytes);
-    if (it != s->host_free.end()) {
-        *out = it->second;
-        s->host_free.erase(it);
-        return GS_OK;
+constexpr size_t kHostPage = 4096;
+constexpr size_t kHostChunk = 64ull << 20;   // least bytes pinned per arena miss
+
+inline size_t host_round(size_t bytes) { return (std::max<size_t>(bytes, 1) + kHostPage - 1) & ~(kHostPage - 1); }
+
+void arena_insert(gs_server* s, char* p, size_t n) {
+    s->host_free_at.emplace(p, n);
+    s->host_free_size.emplace(n, p);
+}
+
+void arena_erase(gs_server* s, std::map<char*, size_t>::iterator it) {
+    auto range = s->host_free_size.equal_range(it->second);
+    for (auto j = range.first; j != range.second; ++j)
+        if (j->second == it->first) {
+            s->host_free_size.erase(j);
+            break;
+        }
+    s->host_free_at.erase(it);
+}
+
+// Returns a block to the arena, merged with the free blocks on either side
+// that lie in the same chunk.
+void arena_put(gs_server* s, char* p, size_t n) {
+    auto nx = s->host_free_at.find(p + n);
+    if (nx != s->host_free_at.end() && !s->chunk_starts.count(p + n)) {
+        n += nx->second;
+        arena_erase(s, nx);
     }
-    GS_CHECK_CUDA(s->ctx, cudaHostAlloc(out, bytes, cudaHostAllocDefault));
-    s->host_all.push_back(*out);
+    auto pv = s->host_free_at.lower_bound(p);
+    if (pv != s->host_free_at.begin() && !s->chunk_starts.count(p)) {
+        --pv;
+        if (pv->first + pv->second == p) {
+            p = pv->first;
+            n += pv->second;
+            arena_erase(s, pv);
+        }
+    }
+    arena_insert(s, p, n);
+}
+
+// Pins a new chunk of at least `bytes` and adds it to the arena; `miss`
+// counts it as a pool miss (a reservation made ahead of the requests is not).
+gs_status arena_grow(gs_server* s, size_t bytes, bool miss) {
+    const size_t n = host_round(bytes);
+    void* p = nullptr;
+    const double t = now_s(s);
+    GS_CHECK_CUDA(s->ctx, cudaHostAlloc(&p, n, cudaHostAllocDefault));
+    if (miss) {
+        s->phase_s[4] += now_s(s) - t;
+        s->phase_s[5] += 1;
+    }
+    s->host_chunks.emplace_back((char*)p, n);
+    s->chunk_starts.insert((char*)p);
+    arena_insert(s, (char*)p, n);
+    return GS_OK;
+}
+
+gs_status pool_host(gs_server* s, size_t bytes, void** out) {
+    const size_t n = host_round(bytes);
+    auto it = s->host_free_size.lower_bound(n);
+    if (it == s->host_free_size.end()) {
+        GS_TRY(arena_grow(s, std::max(n, kHostChunk), true));
+        it = s->host_free_size.lower_bound(n);
+    }
+    char* p = it->second;
+    const size_t have = it->first;
+    arena_erase(s, s->host_free_at.find(p));
+    if (have > n) arena_insert(s, p + n, have - n);
+    *out = p;
     return GS_OK;
 }
 
@@ -435,7 +510,7 @@ std::shared_ptr<HostBuf> host_buf(gs_server* s, size_t bytes, gs_status* st) {
     if (*st != GS_OK) return nullptr;
     HostBuf* hb = new HostBuf{p, bytes};
     return std::shared_ptr<HostBuf>(hb, [s](HostBuf* b) {
-        s->host_free.emplace((b->bytes + 255) & ~(size_t)255, b->p);
+        arena_put(s, (char*)b->p, host_round(b->bytes));
         delete b;
     });
 }
@@ -916,9 +991,25 @@ gs_status bfs_launch(gs_server* s, std::vector<int>& group_job, bool* launched) 
     return GS_OK;
 }
 
+gs_status side_step(gs_server* s);
+
 gs_status bfs_finish(gs_server* s, const std::vector<int>& group_job) {
     gs_ctx* ctx = s->ctx;
-    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(s->stream));
+    // the side requests are tended while the step runs: a chunk that ends
+    // mid-step has its next one (or its result copy) queued at once
+    gs_status side_st = GS_OK;   // a side failure is returned after the step is finished
+    for (;;) {
+        const cudaError_t q = cudaStreamQuery(s->stream);
+        if (q == cudaSuccess) break;
+        if (q != cudaErrorNotReady) return gs_cuda_fail(ctx, q, "BFS step");
+        if (side_st != GS_OK) {
+            GS_CHECK_CUDA(ctx, cudaStreamSynchronize(s->stream));
+            break;
+        }
+        const double t = now_s(s);
+        side_st = side_step(s);
+        s->side_in_wait_s += now_s(s) - t;
+    }
     s->graph_launches++;
     s->kernel_launches += 2;
     s->steps_run++;
@@ -940,7 +1031,7 @@ gs_status bfs_finish(gs_server* s, const std::vector<int>& group_job) {
         if (done) finished.push_back(id);
     }
     s->step += 1;
-    if (finished.empty()) return GS_OK;
+    if (finished.empty()) return side_st;
     // per graph: the retiring slots' bits cleared in one pass; per request:
     // its depth plane copied to pinned host memory, then zeroed
     std::vector<unsigned long long> retiring(s->graphs.size(), 0);
@@ -970,7 +1061,7 @@ gs_status bfs_finish(gs_server* s, const std::vector<int>& group_job) {
     }
     GS_CHECK_CUDA(ctx, cudaStreamSynchronize(s->stream));
     retire(s, finished, now_s(s));
-    return GS_OK;
+    return side_st;
 }
 
 // Progress of the side requests: queue a chunk where none is in flight,
@@ -1027,17 +1118,33 @@ gs_status gs_serve_step(gs_server* s, int* n_active, int* n_queued) {
         s->phase_s[k] += t - t_phase;
         t_phase = t;
     };
-    // admission: FIFO while the state fits the budget and a slot is free
-    while (!s->queue.empty() && (int)s->active.size() < kMaxJobs) {
-        Request& r = s->reqs[s->queue.front()];
-        const SrvGraph& sg = s->graphs[r.graph];
-        if (r.algo == GS_ALGO_BFS && sg.fv && sg.used == ~0ull) break;
-        if (r.algo != GS_ALGO_BFS && s->side_free.empty()) break;
-        const size_t need = footprint(s, r);
-        if (s->used + need > s->budget && !s->active.empty()) break;
-        GS_TRY(admit(s, r));
-        s->active.push_back(r.id);
-        s->queue.pop_front();
+    // admission in arrival order while the state fits the budget: a request
+    // whose slot kind is full (its graph's BFS group, or the side slots)
+    // waits in place while later requests of other kinds go ahead; the
+    // first request that does not fit the budget stops the scan
+    {
+        std::deque<uint64_t> wait;
+        while (!s->queue.empty() && (int)s->active.size() < kMaxJobs) {
+            const uint64_t id = s->queue.front();
+            Request& r = s->reqs[id];
+            const SrvGraph& sg = s->graphs[r.graph];
+            const bool full = r.algo == GS_ALGO_BFS ? (sg.fv && sg.used == ~0ull) : s->side_free.empty();
+            if (full) {
+                wait.push_back(id);
+                s->queue.pop_front();
+                continue;
+            }
+            const size_t need = footprint(s, r);
+            if (s->used + need > s->budget && !s->active.empty()) break;
+            const gs_status st = admit(s, r);
+            if (st != GS_OK) {
+                s->queue.insert(s->queue.begin(), wait.begin(), wait.end());
+                return st;
+            }
+            s->active.push_back(r.id);
+            s->queue.pop_front();
+        }
+        s->queue.insert(s->queue.begin(), wait.begin(), wait.end());
     }
     // the step runs while the host tends the side requests (their chunks run
     // beside it on the lower-priority streams)
@@ -1053,6 +1160,9 @@ gs_status gs_serve_step(gs_server* s, int* n_active, int* n_queued) {
         if (st == GS_OK) st = st2;
     }
     phase_end(3);
+    s->phase_s[3] -= s->side_in_wait_s;
+    s->phase_s[2] += s->side_in_wait_s;
+    s->side_in_wait_s = 0;
     if (st != GS_OK) return st;
     if (n_active) *n_active = (int)s->active.size();
     if (n_queued) *n_queued = (int)s->queue.size();
@@ -1158,8 +1268,14 @@ gs_status gs_serve_stats(const gs_server* s, uint64_t* steps, uint64_t* graph_la
 
 gs_status gs_serve_profile(const gs_server* s, double* seconds, int n) {
     if (!s || !seconds || n < 0) return GS_ERR_ARG;
-    for (int k = 0; k < n && k < 4; ++k) seconds[k] = s->phase_s[k];
+    for (int k = 0; k < n && k < 8; ++k) seconds[k] = s->phase_s[k];
     return GS_OK;
+}
+
+gs_status gs_serve_reserve_host(gs_server* s, uint64_t bytes) {
+    if (!s) return GS_ERR_ARG;
+    if (bytes == 0) return GS_OK;
+    return arena_grow(s, bytes, false);
 }
 
 gs_status gs_serve_free(gs_server* s) {
@@ -1171,7 +1287,7 @@ gs_status gs_serve_free(gs_server* s) {
     if (s->step_exec) cudaGraphExecDestroy(s->step_exec);
     if (s->step_graph) cudaGraphDestroy(s->step_graph);
     for (void* p : s->dev_all) gs_dev_free(p);
-    for (void* p : s->host_all) cudaFreeHost(p);
+    for (auto& c : s->host_chunks) cudaFreeHost(c.first);
     gs_dev_free(s->d_table);
     gs_dev_free(s->d_cnt);
     if (s->h_table) cudaFreeHost(s->h_table);

@@ -315,8 +315,17 @@ gs_status gs_serve_stats(const gs_server* s, uint64_t* steps, uint64_t* graph_la
 /* Host seconds spent in gs_serve_step so far, by phase (up to n of them):
  * [0] admission, [1] BFS step launch, [2] side requests (WCC / k-core /
  * PageRank chunks, their polling and retirement), [3] BFS step finish (the
- * wait for the step, retirement of BFS slots). */
+ * wait for the step, retirement of BFS slots); then, counted inside those
+ * phases, [4] seconds and [5] number of pinned host allocations (result
+ * arena misses; gs_serve_reserve_host is not one), [6] seconds and [7]
+ * number of device allocations (pool misses). */
 gs_status gs_serve_profile(const gs_server* s, double* seconds, int n);
+/* Pins `bytes` of host memory into the server's result arena now, so that
+ * results up to that total land without pinning pages while requests are
+ * served (pinning runs at a few GB/s on the host).  Results are carved from
+ * the arena best-fit; a miss pins a further chunk of at least 64 MiB.  No
+ * counterpart in the reference, which answers one query per process. */
+gs_status gs_serve_reserve_host(gs_server* s, uint64_t bytes);
 gs_status gs_serve_free(gs_server* s);
 
 /* PageRank with the reference's int32 inverse-degree truncation

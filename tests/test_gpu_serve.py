@@ -259,3 +259,35 @@ def test_serve_result_views(gs, pool, gpu_ctx_factory, oracle_lib):
         with pytest.raises(gs.GStoreError, match="GS_ERR_RANGE"):
             srv.result_view(bad)
     pg.free()
+
+
+def test_serve_result_arena(gs, pool, gpu_ctx_factory, oracle_lib):
+    """Results are carved from one pinned arena.  With enough host memory
+    reserved up front, two rounds of requests whose results are all held at
+    once and released out of order pin nothing more, and every held result
+    stays intact until it is released (a block freed early must not be handed
+    to a result that is still being read)."""
+    ctx = gpu_ctx_factory(False)
+    picks = (0, 1, 3)
+    reqs = []
+    for gi in picks:
+        nz = np.nonzero(pool[gi].degree())[0]
+        reqs += [(gi, "kcore", 6), (gi, "wcc", 0), (gi, "bfs", int(nz[0])), (gi, "bfs", int(nz[-1]))]
+    want = [_plain(pool[gi], algo, arg) for gi, algo, arg in reqs]
+    rng = np.random.default_rng(3)
+    with gs.Server(ctx) as srv:
+        gids = [srv.add_graph(g) for g in pool]
+        srv.reserve_host(64 << 20)
+        for _ in range(2):
+            ids = [srv.submit(gids[gi], algo, arg) for gi, algo, arg in reqs]
+            while srv.step() != (0, 0):
+                pass
+            views = [srv.result_view(rid)[0] for rid in ids]
+            order = rng.permutation(len(ids))
+            for n, k in enumerate(order):
+                for j in order[n:]:           # every result not yet released
+                    _check(reqs[j][1], views[j], want[j])
+                srv.release(ids[k])
+        prof = srv.profile()
+        assert prof["pinned_allocs"] == 0     # every result fit the reservation
+        assert srv.stats()["hbm_in_use"] == 0
