@@ -1,8 +1,13 @@
 // BFS sweep and finalize (sm_100a): the level sweep of bfs.cpp:138-185.
 //
 // Per-vertex state in HBM (L2-resident for the graph sizes of interest):
-//   st[v >> 4]  2 bits per vertex, bit 0 frontier (depth == level), bit 1
-//               visited (depth != 0); 16 KB per 2^16-vertex window
+//   st[v >> 4]  2 bits per vertex, frontier (depth == level) and visited
+//               (depth != 0), 16 KB per 2^16-vertex window: in a word of 16
+//               vertices, vertex k's frontier bit is bit k and its visited bit
+//               bit k + 16 when the word index is even, and the other way
+//               round when it is odd, so that one 32-bit rotation by v & 31
+//               brings any vertex's frontier bit to bit 0 and its visited bit
+//               to bit 16
 //   next[v>>5]  discovered during this sweep
 //   depth[v]    u8, written by the finalize for new vertices
 //
@@ -15,7 +20,8 @@
 // warps, each warp streaming its unit's records with 128-bit evict-first
 // loads, each lane loading its next 2 x 16 bytes before it visits the
 // current ones and classifying four records before it acts on any of them
-// (the discovery path is one branch per four records).  Per record: the row
+// (the discovery path is one branch per four records, its reductions
+// predicated rather than branched around).  Per record: the row
 // end's state comes from shared memory, the
 // column end's from global memory through L1 — tiles written by the device
 // converter are sorted by column offset, so the 32 lookups of a warp fall
@@ -65,6 +71,19 @@ __device__ __forceinline__ bool bar_wait(unsigned long long* bar, uint32_t parit
     return false;
 }
 
+// Predicated reductions: the OR is issued only where cond is non-zero, with
+// no branch around it.
+__device__ __forceinline__ void red_or_if(uint32_t* p, uint32_t v, uint32_t cond) {
+    asm volatile("{\n.reg .pred q;\nsetp.ne.u32 q, %2, 0;\n@q red.global.or.b32 [%0], %1;\n}" ::"l"(p), "r"(v),
+                 "r"(cond)
+                 : "memory");
+}
+__device__ __forceinline__ void red_or_shared_if(uint32_t* p, uint32_t v, uint32_t cond) {
+    asm volatile("{\n.reg .pred q;\nsetp.ne.u32 q, %2, 0;\n@q red.shared.or.b32 [%0], %1;\n}" ::"r"(smem_addr(p)),
+                 "r"(v), "r"(cond)
+                 : "memory");
+}
+
 struct RunArgs {
     const gs_tile_run* runs;
     uint64_t n_runs;
@@ -82,8 +101,8 @@ struct RunArgs {
     unsigned int* ticket;
 };
 
-// Six CTAs per SM (48 warps): the register cap this sets (40) costs a few
-// spilled bytes, and measured faster than 48 registers at five CTAs.
+// Five CTAs per SM (40 warps, a 48-register cap): with the predicated
+// discovery, six CTAs at 40 registers spilled more and measured 4 % slower.
 __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     BfsSmem& m = *reinterpret_cast<BfsSmem*>(smem_raw);
@@ -145,35 +164,33 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
             }
             break;   // uniform
         }
-        const uint32_t mr = ar ? 1u : 0u;
+        const uint32_t mr = ar ? 1u << 16 : 0u;
         for (uint32_t ui = ub + warp; ui < ue; ui += kWarps) {
             const gs_unit d = a.units[ui];
             const uint32_t col = d.rc & 0xFFFFu;
-            const uint32_t mc = (!a.directed && a.act[col]) ? 2u : 0u;
+            const uint32_t mc = (!a.directed && a.act[col]) ? 1u : 0u;
             if (!mr && !mc) continue;                       // warp-uniform
             const uint32_t* colst = a.st + ((size_t)col << 12);
             uint32_t* next_col = a.next + ((size_t)col << 11);
-            bool hit = false;
-            // bit 0: the column end is discovered (row end in the frontier,
-            // column end unvisited, bfs.cpp:158-164); bit 1: the row end
-            // (bfs.cpp:166-172)
-            // a vertex's two state bits rotated down to bits 0-1 (the
-            // rotation takes its amount mod 32); the bits above them do not
-            // reach the class
+            uint32_t hit = 0;
+            // class bit 16: the column end is discovered (row end in the
+            // frontier, column end unvisited, bfs.cpp:158-164); bit 0: the
+            // row end (bfs.cpp:166-172).  The rotations take their amount mod
+            // 32, so the row end rotated by v0 ^ 16 has its frontier bit at
+            // 16 and visited bit at 0, the column end rotated by v1 the other
+            // way round, and one AND-NOT per direction gives the class.
             auto classify = [&](uint32_t r) -> uint32_t {
                 const uint32_t w0 = m.strow[(r & 0xFFFFu) >> 4];
                 const uint32_t w1 = __ldg(colst + (r >> 20));
-                const uint32_t s0 = __funnelshift_r(w0, w0, r << 1);
-                const uint32_t s1 = __funnelshift_r(w1, w1, (r >> 16) << 1);
-                return (s0 & ~(s1 >> 1) & mr) | (((s1 & ~(s0 >> 1)) << 1) & mc);
+                const uint32_t s0 = __funnelshift_r(w0, w0, r ^ 16u);
+                const uint32_t s1 = __funnelshift_r(w1, w1, r >> 16);
+                return (s0 & ~s1 & mr) | (s1 & ~s0 & mc);
             };
             auto discover = [&](uint32_t r, uint32_t c) {
                 const uint32_t v0 = r & 0xFFFFu, v1 = r >> 16;
-                if (c & 1u) {
-                    atomicOr(next_col + (v1 >> 5), 1u << (v1 & 31));
-                    hit = true;
-                }
-                if (c & 2u) atomicOr(m.nx + (v0 >> 5), 1u << (v0 & 31));
+                red_or_if(next_col + (v1 >> 5), 1u << (v1 & 31), c >> 16);
+                red_or_shared_if(m.nx + (v0 >> 5), 1u << (v0 & 31), c & 1u);
+                hit |= c >> 16;
             };
             auto visit = [&](uint32_t r) {
                 const uint32_t c = classify(r);
@@ -184,10 +201,10 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
             auto visit4 = [&](const uint4 q) {
                 const uint32_t c0 = classify(q.x), c1 = classify(q.y), c2 = classify(q.z), c3 = classify(q.w);
                 if (c0 | c1 | c2 | c3) {
-                    if (c0) discover(q.x, c0);
-                    if (c1) discover(q.y, c1);
-                    if (c2) discover(q.z, c2);
-                    if (c3) discover(q.w, c3);
+                    discover(q.x, c0);
+                    discover(q.y, c1);
+                    discover(q.z, c2);
+                    discover(q.w, c3);
                 }
             };
             const uint64_t b = d.rec_beg, e = d.rec_beg + d.n;
@@ -212,7 +229,7 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
                 q0 = p0;
                 q1 = p1;
             }
-            if (__any_sync(0xFFFFFFFFu, hit) && lane == 0) a.act_next[col] = 1;   // read_part_next->set_bit_atomic(j)
+            if (__any_sync(0xFFFFFFFFu, hit != 0) && lane == 0) a.act_next[col] = 1;   // read_part_next->set_bit_atomic(j)
         }
         __syncthreads();
         // row side: OR the run's discovered words into next, clear them
@@ -237,23 +254,6 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
     }
 }
 
-// Bits 1,3,5,... of x gathered into bits 0..15.
-__device__ __forceinline__ uint32_t odd_bits(uint32_t x) {
-    x = (x >> 1) & 0x55555555u;
-    x = (x | (x >> 1)) & 0x33333333u;
-    x = (x | (x >> 2)) & 0x0F0F0F0Fu;
-    x = (x | (x >> 4)) & 0x00FF00FFu;
-    return (x | (x >> 8)) & 0x0000FFFFu;
-}
-// Bits 0..15 of x spread to bits 0,2,4,...
-__device__ __forceinline__ uint32_t spread_bits(uint32_t x) {
-    x &= 0xFFFFu;
-    x = (x | (x << 8)) & 0x00FF00FFu;
-    x = (x | (x << 4)) & 0x0F0F0F0Fu;
-    x = (x | (x << 2)) & 0x33333333u;
-    return (x | (x << 1)) & 0x55555555u;
-}
-
 // Per 32 vertices: new = next & ~visited; frontier := new; visited |= new;
 // depth[v] = level + 1 for new vertices; next := 0 (iteration_finalize,
 // bfs.cpp:187-224 — the level count is exact here).
@@ -267,12 +267,13 @@ __global__ void bfs_finalize_kernel(uint32_t* __restrict__ st, uint32_t* __restr
         const uint32_t nx = next[w];
         const uint2 s = reinterpret_cast<const uint2*>(st)[w];
         if (nx) next[w] = 0;
-        const uint32_t vis = odd_bits(s.x) | (odd_bits(s.y) << 16);
+        // even word: F in bits 0-15, VIS in bits 16-31; odd word swapped
+        const uint32_t vis = (s.x >> 16) | (s.y << 16);
+        const uint32_t fr = (s.x & 0xFFFFu) | (s.y & 0xFFFF0000u);
         const uint32_t fresh = nx & ~vis;
-        if (fresh == 0 && ((s.x | s.y) & 0x55555555u) == 0) continue;
-        const uint32_t e0 = spread_bits(fresh), e1 = spread_bits(fresh >> 16);
-        reinterpret_cast<uint2*>(st)[w] =
-            make_uint2((s.x & 0xAAAAAAAAu) | e0 | (e0 << 1), (s.y & 0xAAAAAAAAu) | e1 | (e1 << 1));
+        if (fresh == 0 && fr == 0) continue;
+        const uint32_t nv = vis | fresh;
+        reinterpret_cast<uint2*>(st)[w] = make_uint2((fresh & 0xFFFFu) | (nv << 16), (nv >> 16) | (fresh & 0xFFFF0000u));
         uint32_t x = fresh;
         while (x) {
             const int k = __ffs(x) - 1;
@@ -288,7 +289,7 @@ __global__ void bfs_finalize_kernel(uint32_t* __restrict__ st, uint32_t* __restr
 
 __global__ void bfs_seed_kernel(uint8_t* depth, uint32_t* st, uint8_t* act, uint64_t root) {
     depth[root] = 1;                                 // bfs.cpp:70
-    st[root >> 4] = 3u << ((root & 15) << 1);        // frontier + visited
+    st[root >> 4] = 0x10001u << (root & 15);         // frontier + visited
     act[root >> 16] = 1;                             // calc_part_needed, bfs.cpp:324-338
 }
 

@@ -54,7 +54,7 @@ constexpr uint32_t kBlockWindowsSmall = 32;
 constexpr uint32_t kBlockRunUnits = 8;
 constexpr uint32_t kBfsMinRunUnits = 8;     // BFS sweep: smallest run piece
 constexpr uint64_t kBfsRunsPerCta = 4;      // BFS sweep: run pieces wanted per CTA
-constexpr int kBfsCtasPerSm = 6;            // BFS sweep: resident CTAs per SM
+constexpr int kBfsCtasPerSm = 5;            // BFS sweep: resident CTAs per SM
 
 // One unit: records [rec_beg, rec_beg + n) of the tile at row rc >> 16,
 // column rc & 0xFFFF (n <= kUnitRecords; units follow the file order).
