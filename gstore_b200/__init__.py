@@ -41,7 +41,7 @@ ABI_SYMBOLS = [
     "gs_launch_count",
     "gs_geometry", "gs_upload_graph", "gs_upload_graph_device", "gs_graph_free", "gs_graph_info",
     "gs_graph_degree", "gs_state_create", "gs_state_free", "gs_state_reset", "gs_sweep", "gs_finalize", "gs_run",
-    "gs_download", "gs_result_count", "gs_bfs_stats", "gs_pagerank_compat",
+    "gs_download", "gs_result_count", "gs_bfs_stats", "gs_bfs_records_read", "gs_pagerank_compat",
     "gs_kron_generate_device", "gs_kron_generate", "gs_convert", "gs_graph_download",
     "gs_bfs_noalloc", "gs_upload_graph_streamed", "gs_upload_graph_file", "gs_stream_stats",
     "gs_read_tile_files", "gs_upload_graph_files",
@@ -96,6 +96,7 @@ def lib():
             "gs_download": [vp, i32, vp, u64],
             "gs_result_count": [vp, pu64],
             "gs_bfs_stats": [vp, pu64, vp, i32, C.POINTER(C.c_int), vp],
+            "gs_bfs_records_read": [vp, vp, i32, C.POINTER(C.c_int)],
             "gs_pagerank_compat": [vp, i32],
             "gs_kron_generate_device": [vp, i32, i64, u64, u64, vp],
             "gs_kron_generate": [vp, i32, i64, u64, u64, vp],
@@ -690,4 +691,8 @@ class State:
         self._check(lib().gs_bfs_stats(self._h, C.byref(e), _ptr(swept), max_levels, C.byref(nl),
                                        _ptr(counts)))
         n = nl.value
-        return {"edges_in_component": e.value, "swept": swept[:n].copy(), "level_counts": counts[:n].copy()}
+        read = np.zeros(max_levels, np.uint64)
+        nr = C.c_int()
+        self._check(lib().gs_bfs_records_read(self._h, _ptr(read), max_levels, C.byref(nr)))
+        return {"edges_in_component": e.value, "swept": swept[:n].copy(), "level_counts": counts[:n].copy(),
+                "read": read[:min(n, nr.value)].copy()}

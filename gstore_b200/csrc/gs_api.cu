@@ -989,4 +989,23 @@ gs_status gs_bfs_stats(gs_state* s, uint64_t* edges_in_component, uint64_t* swep
     return GS_OK;
 }
 
+gs_status gs_bfs_records_read(gs_state* s, uint64_t* read_records, int max_levels, int* n_levels) {
+    if (!s || s->algo != GS_ALGO_BFS || max_levels < 0 || (max_levels && !read_records)) return GS_ERR_ARG;
+    const int nl = std::min((int)s->level_counts.size(), 256);
+    if (n_levels) *n_levels = nl;
+    const int n = std::min(nl, max_levels);
+    if (n <= 0) return GS_OK;
+    // a level that skipped dead chunks counted what it read; any other read
+    // every record of the tiles the reference rule sweeps
+    GS_TRY(gs_bfs_stats(s, nullptr, read_records, n, nullptr, nullptr));
+    std::vector<uint64_t> counted(n, 0);
+    gs_ctx* ctx = s->g->ctx;
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(counted.data(), s->d_read, (size_t)n * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int l = 0; l < n; ++l)
+        if (l < (int)s->level_skip.size() && s->level_skip[l]) read_records[l] = counted[l];
+    return GS_OK;
+}
+
 }  // extern "C"

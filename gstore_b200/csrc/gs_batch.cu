@@ -110,6 +110,9 @@ struct MsArgs {
     const gs_pr_item* items;         // row-slice order: (row, slice, column block) items
     uint64_t n_items;
     unsigned int* tickets;           // [256]: next run of each level's sweep
+    uint8_t* dead;                   // per unit: chunks with no record left to discover (ms_sweep_unit_live)
+    W qmask;                         // the group's queries
+    uint64_t live_pairs;             // (vertex with records, query) pairs: nonisolated x queries
 };
 
 template <class W>
@@ -133,6 +136,12 @@ __global__ void __launch_bounds__(kThreads) msbfs_kernel(MsArgs<W> a) {
             __syncthreads();
             return s_run;
         };
+        // chunks whose records all have both ends visited by every query
+        // are marked, and the marked ones skipped, once at most 1/64 of the
+        // (vertex with records, query) pairs are unvisited (after the peak)
+        uint64_t visited = (uint64_t)popc_w(a.qmask);
+        for (int l = 1; l < level; ++l) visited += __ldcg(a.total + l);
+        const bool mark = a.dead && (a.live_pairs > visited ? a.live_pairs - visited : 0) * 64 <= a.live_pairs;
         for (uint64_t i = draw(); i < a.R; i = draw()) {
             const gs_tile_run run = a.runs[i];
             const uint32_t row = a.units[run.unit_beg].rc >> 16;
@@ -140,7 +149,8 @@ __global__ void __launch_bounds__(kThreads) msbfs_kernel(MsArgs<W> a) {
             for (uint32_t ui = run.unit_beg + warp; ui < run.unit_end; ui += kWarps) {
                 const gs_unit d = a.units[ui];
                 if (!ar && (a.directed || !__ldcg(act + (d.rc & 0xFFFFu)))) continue;
-                ms_sweep_unit<W>(d, a.rec, a.fv, a.next, a.directed, lane);
+                if (mark) ms_sweep_unit_live<W>(d, ui, a.rec, a.fv, a.next, a.directed, lane, a.dead, true, a.qmask);
+                else ms_sweep_unit<W>(d, a.rec, a.fv, a.next, a.directed, lane);
             }
         }
         if (!grid_barrier(a.bar, a.err)) return;
@@ -622,8 +632,9 @@ gs_status run_bfs_group(gs_batch* b, gs_bfs_group& grp) {
     const size_t fv_b = N * sizeof(FvPair<W>), nx_b = N * sizeof(W);
     const size_t act_b = (2 * (size_t)g->nw + 255) & ~(size_t)255;
     const size_t small_b = 256 * 8 + 64 + 8 * kMaxBatch + 64 + 256 * 4;
+    const size_t dead_b = (g->U + 4 + 255) & ~(size_t)255;   // a byte per unit, whole words
     void* base = nullptr;
-    GS_TRY(scratch(b, fv_b + nx_b + act_b + small_b, &base));
+    GS_TRY(scratch(b, fv_b + nx_b + act_b + small_b + dead_b, &base));
     char* p = (char*)base;
     FvPair<W>* fv = (FvPair<W>*)p;
     W* next = (W*)(p + fv_b);
@@ -636,8 +647,10 @@ gs_status run_bfs_group(gs_batch* b, gs_bfs_group& grp) {
     W* overflow = (W*)(small + 256 * 8 + 48);
     uint64_t* roots = (uint64_t*)(small + 256 * 8 + 64);
     unsigned int* tickets = (unsigned int*)(small + 256 * 8 + 64 + 8 * kMaxBatch + 64);
+    uint8_t* dead = (uint8_t*)(small + small_b);
     GS_TRY(gs_pool_get(ctx, N * kBits, (void**)&grp.depth));
-    GS_CHECK_CUDA(ctx, cudaMemsetAsync(base, 0, fv_b + nx_b + act_b + small_b, ctx->stream));
+    GS_TRY(gs_graph_nonisolated(g));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(base, 0, fv_b + nx_b + act_b + small_b + dead_b, ctx->stream));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(grp.depth, 0, N * n, ctx->stream));   // the queries' planes
     std::vector<uint64_t> h_roots(n);
     for (int i = 0; i < n; ++i) h_roots[i] = (uint64_t)b->q[grp.queries[i]].arg;
@@ -666,7 +679,10 @@ gs_status run_bfs_group(gs_batch* b, gs_bfs_group& grp) {
                 g->directed,
                 nullptr,
                 0,
-                tickets};
+                tickets,
+                g->nonisolated_known ? dead : nullptr,
+                n >= kBits ? (W)~(W)0 : (W)(((W)1 << n) - 1),
+                g->nonisolated * (uint64_t)n};
     void* args[] = {&a};
     GS_CHECK_CUDA(ctx, cudaEventRecord(b->e0, ctx->stream));
     if (grp.order == 3) {

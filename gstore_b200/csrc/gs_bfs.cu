@@ -99,10 +99,21 @@ struct RunArgs {
     // [0] next run, [1] CTAs finished; zero at launch, the last CTA to
     // finish zeroes them again for the next launch on the stream
     unsigned int* ticket;
+    // per unit, bit c: chunk c of the unit (its 16-byte groups 64c..64c+63,
+    // chunk 0 with the unaligned head and tail records) holds no record
+    // with an unvisited end, so it can discover nothing for the rest of the
+    // BFS (visited bits are never cleared); null: every chunk is read
+    uint8_t* dead;
+    unsigned long long* read;   // kSkip: records read by the launch are added here (null: not counted)
 };
 
 // Five CTAs per SM (40 warps, a 48-register cap): with the predicated
 // discovery, six CTAs at 40 registers spilled more and measured 4 % slower.
+// kMark: a chunk whose records all have both ends visited at the start of
+// the level is marked dead (a.dead) for the levels after it.  kSkip: dead
+// chunks are not read (set once a level has marked some).  Without either,
+// the unit loop is the plain one.
+template <bool kMark, bool kSkip>
 __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     BfsSmem& m = *reinterpret_cast<BfsSmem*>(smem_raw);
@@ -114,6 +125,7 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
     for (uint32_t w = tid; w < kNxWords; w += kThreads) m.nx[w] = 0;
     __syncthreads();
     uint32_t parity = 0;
+    uint32_t nread = 0;   // kSkip, lane 0: records this warp read
     auto draw = [&]() -> uint64_t {
         // every thread has read the previous draw: a barrier lies between
         if (tid == 0) m.cur = atomicAdd(a.ticket, 1u);
@@ -179,11 +191,15 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
             // 32, so the row end rotated by v0 ^ 16 has its frontier bit at
             // 16 and visited bit at 0, the column end rotated by v1 the other
             // way round, and one AND-NOT per direction gives the class.
+            // allv bit 0 stays set while every record classified has both
+            // ends visited (row end's visited bit 0, column end's bit 16)
+            uint32_t allv = ~0u;
             auto classify = [&](uint32_t r) -> uint32_t {
                 const uint32_t w0 = m.strow[(r & 0xFFFFu) >> 4];
                 const uint32_t w1 = __ldg(colst + (r >> 20));
                 const uint32_t s0 = __funnelshift_r(w0, w0, r ^ 16u);
                 const uint32_t s1 = __funnelshift_r(w1, w1, r >> 16);
+                if constexpr (kMark) allv &= s0 & (s1 >> 16);
                 return (s0 & ~s1 & mr) | (s1 & ~s0 & mc);
             };
             auto discover = [&](uint32_t r, uint32_t c) {
@@ -212,22 +228,70 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
             if (ab > e) ab = e;
             uint64_t ae = e & ~3ull;
             if (ae < ab) ae = ab;
-            if (b + lane < ab) visit(__ldcs(rec + b + lane));
-            if (ae + lane < e) visit(__ldcs(rec + ae + lane));
             const uint4* r4 = reinterpret_cast<const uint4*>(rec + ab);
             const uint32_t n4 = (uint32_t)((ae - ab) >> 2);
-            // the next iteration's records are loaded before this one's are
-            // visited, so the loads overlap the lookups
             const uint4 z = make_uint4(0, 0, 0, 0);
-            uint4 q0 = lane < n4 ? __ldcs(r4 + lane) : z;
-            uint4 q1 = lane + 32 < n4 ? __ldcs(r4 + lane + 32) : z;
-            for (uint32_t k = lane; k < n4; k += 64) {
-                const uint4 p0 = k + 64 < n4 ? __ldcs(r4 + k + 64) : z;
-                const uint4 p1 = k + 96 < n4 ? __ldcs(r4 + k + 96) : z;
-                visit4(q0);
-                if (k + 32 < n4) visit4(q1);
-                q0 = p0;
-                q1 = p1;
+            if constexpr (!kMark && !kSkip) {
+                if (b + lane < ab) visit(__ldcs(rec + b + lane));
+                if (ae + lane < e) visit(__ldcs(rec + ae + lane));
+                // the next iteration's records are loaded before this one's
+                // are visited, so the loads overlap the lookups
+                uint4 q0 = lane < n4 ? __ldcs(r4 + lane) : z;
+                uint4 q1 = lane + 32 < n4 ? __ldcs(r4 + lane + 32) : z;
+                for (uint32_t k = lane; k < n4; k += 64) {
+                    const uint4 p0 = k + 64 < n4 ? __ldcs(r4 + k + 64) : z;
+                    const uint4 p1 = k + 96 < n4 ? __ldcs(r4 + k + 96) : z;
+                    visit4(q0);
+                    if (k + 32 < n4) visit4(q1);
+                    q0 = p0;
+                    q1 = p1;
+                }
+            } else {
+                // chunks of 64 16-byte groups (<= 8 per unit), chunk 0 with
+                // the unaligned head and tail; the live ones are read (all of
+                // them without kSkip), the next one's records loaded before
+                // this one's are visited
+                const uint32_t nch = n4 ? (n4 + 63) >> 6 : 1;
+                const uint32_t dead = kSkip ? (uint32_t)__ldcg(a.dead + ui) : 0u;
+                uint32_t todo = ((1u << nch) - 1u) & ~dead;
+                if (!(dead & 1u)) {
+                    if (b + lane < ab) visit(__ldcs(rec + b + lane));
+                    if (ae + lane < e) visit(__ldcs(rec + ae + lane));
+                    if (kSkip && lane == 0) nread += (uint32_t)((ab - b) + (e - ae));
+                }
+                int c = todo ? __ffs(todo) - 1 : -1;
+                uint4 q0 = z, q1 = z;
+                if (c >= 0) {
+                    const uint32_t k = ((uint32_t)c << 6) + lane;
+                    q0 = k < n4 ? __ldcs(r4 + k) : z;
+                    q1 = k + 32 < n4 ? __ldcs(r4 + k + 32) : z;
+                }
+                uint32_t newdead = 0;
+                while (c >= 0) {   // warp-uniform: todo comes from one byte read by every lane
+                    todo &= todo - 1;
+                    const int cn = todo ? __ffs(todo) - 1 : -1;
+                    uint4 p0 = z, p1 = z;
+                    if (cn >= 0) {
+                        const uint32_t kn = ((uint32_t)cn << 6) + lane;
+                        p0 = kn < n4 ? __ldcs(r4 + kn) : z;
+                        p1 = kn + 32 < n4 ? __ldcs(r4 + kn + 32) : z;
+                    }
+                    const uint32_t k0 = (uint32_t)c << 6;
+                    if (k0 + lane < n4) visit4(q0);
+                    if (k0 + lane + 32 < n4) visit4(q1);
+                    if constexpr (kMark) {
+                        if (__all_sync(0xFFFFFFFFu, allv & 1u)) newdead |= 1u << c;
+                        allv = ~0u;
+                    }
+                    if (kSkip && lane == 0) nread += 4u * min(64u, n4 - min(n4, k0));
+                    q0 = p0;
+                    q1 = p1;
+                    c = cn;
+                }
+                if constexpr (kMark) {
+                    if (lane == 0 && newdead)
+                        atomicOr(reinterpret_cast<unsigned int*>(a.dead) + (ui >> 2), newdead << ((ui & 3u) << 3));
+                }
             }
             if (__any_sync(0xFFFFFFFFu, hit != 0) && lane == 0) a.act_next[col] = 1;   // read_part_next->set_bit_atomic(j)
         }
@@ -247,6 +311,7 @@ __global__ void __launch_bounds__(kThreads, kBfsCtasPerSm) bfs_run_kernel(RunArg
         }
         if (__syncthreads_or(any_row) && tid == 0) a.act_next[row] = 1;        // read_part_next->set_bit_atomic(i)
     }
+    if (kSkip && a.read && lane == 0 && nread) atomicAdd(a.read, (unsigned long long)nread);
     if (tid == 0 && atomicAdd(a.ticket + 1, 1u) == gridDim.x - 1) {
         // every CTA has drawn its last ticket
         atomicExch(a.ticket, 0u);
@@ -287,6 +352,16 @@ __global__ void bfs_finalize_kernel(uint32_t* __restrict__ st, uint32_t* __restr
     if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, (unsigned long long)local);
 }
 
+// Vertices with at least one record (degree > 0).
+__global__ void count_nonisolated_kernel(const int32_t* __restrict__ degree, uint64_t V, unsigned long long* out) {
+    unsigned long long local = 0;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
+        local += degree[v] != 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xFFFFFFFFu, local, o);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(out, local);
+}
+
 __global__ void bfs_seed_kernel(uint8_t* depth, uint32_t* st, uint8_t* act, uint64_t root) {
     depth[root] = 1;                                 // bfs.cpp:70
     st[root >> 4] = 0x10001u << (root & 15);         // frontier + visited
@@ -300,6 +375,22 @@ inline uint32_t blocks_for(uint64_t n, const gs_ctx* ctx) {
 
 }  // namespace
 
+gs_status gs_graph_nonisolated(gs_graph* g) {
+    if (g->nonisolated_known || !g->d_degree) return GS_OK;   // counted once per graph
+    gs_ctx* ctx = g->ctx;
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_scalars, 0, sizeof(uint64_t), ctx->stream));
+    count_nonisolated_kernel<<<blocks_for(g->V, ctx), 256, 0, ctx->stream>>>(g->d_degree, g->V,
+                                                                             (unsigned long long*)ctx->d_scalars);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    ctx->launches++;
+    GS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->h_scalars, ctx->d_scalars, sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    g->nonisolated = ctx->h_scalars[0];
+    g->nonisolated_known = true;
+    return GS_OK;
+}
+
 gs_status bfs_init(gs_state* s) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
@@ -311,7 +402,12 @@ gs_status bfs_init(gs_state* s) {
     if (!s->d_act_next) GS_TRY(gs_state_alloc(s, (void**)&s->d_act_next, g->nw));
     if (!s->d_error) GS_TRY(gs_state_alloc(s, (void**)&s->d_error, sizeof(uint64_t)));
     if (!s->d_ticket) GS_TRY(gs_state_alloc(s, (void**)&s->d_ticket, 2 * sizeof(uint32_t)));
+    const size_t dead_bytes = ((g->U + 3) & ~(uint64_t)3) + 4;   // whole 32-bit words
+    if (!s->d_dead) GS_TRY(gs_state_alloc(s, (void**)&s->d_dead, dead_bytes));
+    if (!s->d_read) GS_TRY(gs_state_alloc(s, (void**)&s->d_read, 256 * sizeof(unsigned long long)));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_ticket, 0, 2 * sizeof(uint32_t), ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_dead, 0, dead_bytes, ctx->stream));
+    GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_read, 0, 256 * sizeof(unsigned long long), ctx->stream));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_depth, 0, g->N, ctx->stream));   // INFTY = 0
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_front, 0, words * 8, ctx->stream));
     GS_CHECK_CUDA(ctx, cudaMemsetAsync(s->d_visited, 0, words * 4, ctx->stream));
@@ -321,6 +417,9 @@ gs_status bfs_init(gs_state* s) {
     bfs_seed_kernel<<<1, 1, 0, ctx->stream>>>(s->d_depth, s->d_front, s->d_act, (uint64_t)s->arg);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
+    GS_TRY(gs_graph_nonisolated(g));
+    s->marking = false;
+    s->level_skip.clear();
     s->level = 1;
     s->level_counts.clear();
     s->n_act_hist = 0;
@@ -337,7 +436,9 @@ gs_status bfs_sweep_begin(gs_state* s) {
         GS_CHECK_CUDA(ctx, cudaMemcpyAsync(s->d_act_hist + (size_t)s->n_act_hist * g->nw, s->d_act, g->nw,
                                            cudaMemcpyDeviceToDevice, ctx->stream));
     s->n_act_hist += 1;
-    GS_CHECK_CUDA(ctx, gs_smem_limit_once<bfs_run_kernel>(ctx->device, (int)sizeof(BfsSmem)));
+    GS_CHECK_CUDA(ctx, (gs_smem_limit_once<bfs_run_kernel<false, false>>(ctx->device, (int)sizeof(BfsSmem))));
+    GS_CHECK_CUDA(ctx, (gs_smem_limit_once<bfs_run_kernel<true, false>>(ctx->device, (int)sizeof(BfsSmem))));
+    GS_CHECK_CUDA(ctx, (gs_smem_limit_once<bfs_run_kernel<true, true>>(ctx->device, (int)sizeof(BfsSmem))));
     return GS_OK;
 }
 
@@ -347,12 +448,31 @@ gs_status bfs_sweep_launch(gs_state* s) {
     // every run of the resident graph, or the entries of the current segment
     const uint64_t n_runs = g->seg.list ? g->seg.n : (g->d_runs_lpt ? g->R_lpt : g->R);
     if (n_runs == 0) return GS_OK;
+    // Dead chunks are kept for resident graphs (a segment's records are
+    // copied whole whatever is skipped).  Marking starts once at most 1/64
+    // of the vertices with records are still unvisited (after the peak,
+    // when most chunks have no record left with an unvisited end) and goes
+    // on at every level after it, which also skips the chunks marked so
+    // far.  Only speed depends on this choice: a dead chunk can discover
+    // nothing.
+    uint8_t* dead = (g->seg.list || !g->nonisolated_known) ? nullptr : s->d_dead;
+    uint64_t visited = 1;
+    for (uint64_t c : s->level_counts) visited += c;
+    const uint64_t unvisited = g->nonisolated > visited ? g->nonisolated - visited : 0;
+    const bool mark = dead && (s->marking || unvisited * 64 <= g->nonisolated);
+    const bool skip = dead && s->marking;
     RunArgs a{g->d_runs_lpt ? g->d_runs_lpt : g->d_runs, n_runs, g->d_units, g->seg.list ? g->seg.buf : g->d_rec,
               s->d_front, s->d_visited,
-              s->d_act, s->d_act_next, g->directed, (int*)s->d_error, g->seg.list, s->d_ticket};
+              s->d_act, s->d_act_next, g->directed, (int*)s->d_error, g->seg.list, s->d_ticket, dead,
+              s->d_read + std::min(s->level - 1, 255)};
     const uint32_t grid = (uint32_t)std::min<uint64_t>(n_runs, gs_grid_size(ctx, kBfsCtasPerSm));
     gs_timer_begin(ctx);
-    bfs_run_kernel<<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
+    if (skip) bfs_run_kernel<true, true><<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
+    else if (mark) bfs_run_kernel<true, false><<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
+    else bfs_run_kernel<false, false><<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
+    if (mark) s->marking = true;
+    if (s->level_skip.size() < s->level) s->level_skip.resize(s->level, 0);
+    s->level_skip[s->level - 1] = skip ? 1 : 0;
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
     gs_timer_end(ctx, GS_ALGO_BFS, 0);
@@ -404,12 +524,12 @@ gs_status bfs_level_into(gs_ctx* ctx, const gs_graph* g, uint8_t* depth, uint32_
                          uint8_t* act, uint8_t* act_next, unsigned long long* count, int* error,
                          unsigned int* ticket, uint8_t next_level) {
     if (g->R) {
-        GS_CHECK_CUDA(ctx, gs_smem_limit_once<bfs_run_kernel>(ctx->device, (int)sizeof(BfsSmem)));
+        GS_CHECK_CUDA(ctx, (gs_smem_limit_once<bfs_run_kernel<false, false>>(ctx->device, (int)sizeof(BfsSmem))));
         const uint64_t n_runs = g->d_runs_lpt ? g->R_lpt : g->R;
         RunArgs a{g->d_runs_lpt ? g->d_runs_lpt : g->d_runs, n_runs, g->d_units, g->d_rec, st, next, act, act_next,
-                  g->directed, error, nullptr, ticket};
+                  g->directed, error, nullptr, ticket, nullptr, nullptr};
         const uint32_t grid = (uint32_t)std::min<uint64_t>(n_runs, gs_grid_size(ctx, kBfsCtasPerSm));
-        bfs_run_kernel<<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
+        bfs_run_kernel<false, false><<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
         GS_CHECK_CUDA(ctx, cudaGetLastError());
         ctx->launches++;
     }

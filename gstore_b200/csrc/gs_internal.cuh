@@ -193,6 +193,8 @@ struct gs_graph {
     uint64_t* d_tile_off = nullptr;   // T + 1 record offsets of non-empty tiles
     uint32_t* d_tile_rc = nullptr;    // T packed (row << 16 | col)
     int32_t* d_degree = nullptr;      // N
+    uint64_t nonisolated = 0;         // vertices with degree > 0 (counted at the first BFS)
+    bool nonisolated_known = false;
     SegView seg;                      // set during segment sweeps
     gs_pr_layout pr;                  // row-slice PageRank layout (serving, batches, smaller graphs)
     gs_pb_layout pb;                  // propagation-blocked PageRank layout (gs_run on large graphs)
@@ -224,6 +226,10 @@ struct gs_state {
     uint32_t* d_visited = nullptr;   // N/32 words: discovered-this-sweep bitmap
     uint64_t* d_error = nullptr;     // bounded-wait failure flag
     uint32_t* d_ticket = nullptr;    // BFS sweep: run ticket, finished CTAs
+    uint8_t* d_dead = nullptr;       // BFS: per unit, chunks with no record left to discover anything
+    bool marking = false;            // BFS: dead chunks are being marked (and skipped)
+    std::vector<uint8_t> level_skip; // BFS: per level, dead chunks were skipped (records read counted)
+    unsigned long long* d_read = nullptr;   // BFS: records read per level (256)
     uint8_t* d_act = nullptr;        // nw window flags (current)
     uint8_t* d_act_next = nullptr;   // nw
     std::vector<uint64_t> level_counts;
@@ -302,6 +308,8 @@ gs_status launch_degree_from_records(gs_graph* g);
 // Per algorithm: init, sweep_begin (once per sweep, before its launches),
 // sweep_launch (once per segment in g->seg, or once over the resident
 // graph), finalize.
+// Counts the graph's vertices with degree > 0 into g->nonisolated (once).
+gs_status gs_graph_nonisolated(gs_graph* g);
 gs_status bfs_init(gs_state* s);
 gs_status bfs_sweep_begin(gs_state* s);
 gs_status bfs_sweep_launch(gs_state* s);

@@ -318,6 +318,75 @@ __device__ __forceinline__ void ms_sweep_unit(const gs_unit d, const uint32_t* _
     }
 }
 
+// ms_sweep_unit over the unit's live chunks only: chunk c (its 16-byte
+// groups 64c..64c+63; chunk 0 also the unaligned head and tail records) is
+// skipped when bit c of dead[ui] is set -- every record in it had both ends
+// visited by every query (qmask) at an earlier level, so it can discover
+// nothing again.  With `mark`, the chunks found so in this sweep are marked
+// for the levels after it (dead is written by other warps meanwhile: read
+// through L2).
+template <class W>
+__device__ __forceinline__ void ms_sweep_unit_live(const gs_unit d, uint32_t ui, const uint32_t* __restrict__ base,
+                                                   FvPair<W>* fv, W* next, int directed, uint32_t lane,
+                                                   uint8_t* dead, bool mark, W qmask) {
+    const uint32_t rb = (d.rc >> 16) << 16, cb = (d.rc & 0xFFFFu) << 16;
+    uint32_t allv = 1;   // every record this lane visited has both ends visited by every query
+    auto act = [&](uint32_t a, uint32_t b, const FvPair<W>& sa, const FvPair<W>& sb) {
+        const W nb = sa.f & ~sb.vis;
+        if (nb) atomicOr(next + b, nb);
+        if (!directed) {            // the half grid stores each edge once
+            const W na = sb.f & ~sa.vis;
+            if (na) atomicOr(next + a, na);
+        }
+        allv &= (W)(sa.vis & sb.vis) == qmask ? 1u : 0u;
+    };
+    auto one = [&](uint32_t r) {
+        const uint32_t a = rb + (r & 0xFFFFu), b = cb + (r >> 16);
+        act(a, b, load_fv(fv + a), load_fv(fv + b));
+    };
+    const uint64_t b = d.rec_beg, e = d.rec_beg + d.n;
+    uint64_t ab = (b + 3) & ~3ull;
+    if (ab > e) ab = e;
+    uint64_t ae = e & ~3ull;
+    if (ae < ab) ae = ab;
+    const uint4* r4 = reinterpret_cast<const uint4*>(base + ab);
+    const uint32_t n4 = (uint32_t)((ae - ab) >> 2);
+    const uint32_t dd = __ldcg(dead + ui);
+    const uint32_t nch = n4 ? (n4 + 63) >> 6 : 1;   // <= 8: a unit holds <= kUnitRecords records
+    uint32_t todo = ((1u << nch) - 1u) & ~dd;
+    if (!(dd & 1u)) {
+        if (b + lane < ab) one(__ldcs(base + b + lane));
+        if (ae + lane < e) one(__ldcs(base + ae + lane));
+    }
+    uint32_t newdead = 0;
+    while (todo) {   // warp-uniform
+        const uint32_t c = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const uint32_t kend = min(n4, (c + 1) << 6);
+        for (uint32_t k = (c << 6) + lane; k < kend; k += 32) {
+            const uint4 q = load_stream(r4 + k);
+            const uint32_t a0 = rb + (q.x & 0xFFFFu), b0 = cb + (q.x >> 16);
+            const uint32_t a1 = rb + (q.y & 0xFFFFu), b1 = cb + (q.y >> 16);
+            const uint32_t a2 = rb + (q.z & 0xFFFFu), b2 = cb + (q.z >> 16);
+            const uint32_t a3 = rb + (q.w & 0xFFFFu), b3 = cb + (q.w >> 16);
+            const FvPair<W> sa0 = load_fv(fv + a0), sb0 = load_fv(fv + b0);
+            const FvPair<W> sa1 = load_fv(fv + a1), sb1 = load_fv(fv + b1);
+            const FvPair<W> sa2 = load_fv(fv + a2), sb2 = load_fv(fv + b2);
+            const FvPair<W> sa3 = load_fv(fv + a3), sb3 = load_fv(fv + b3);
+            act(a0, b0, sa0, sb0);
+            act(a1, b1, sa1, sb1);
+            act(a2, b2, sa2, sb2);
+            act(a3, b3, sa3, sb3);
+        }
+        if (mark) {
+            if (__all_sync(kFull, allv)) newdead |= 1u << c;
+            allv = 1;
+        }
+    }
+    if (mark && lane == 0 && newdead)
+        atomicOr(reinterpret_cast<unsigned int*>(dead) + (ui >> 2), newdead << ((ui & 3u) << 3));
+}
+
 // KcoreOp for a persistent kernel: the removed bits and window flags change
 // between phases, so they are read through L2 (never the non-coherent path).
 struct KcoreOpL2 {

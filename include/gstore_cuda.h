@@ -222,6 +222,13 @@ gs_status gs_result_count(gs_state* s, uint64_t* count);
  * records swept per level under the reference's tile-skip rule. */
 gs_status gs_bfs_stats(gs_state* s, uint64_t* edges_in_component, uint64_t* swept_records,
                        int max_levels, int* n_levels, uint64_t* level_counts);
+/* BFS: records the sweep kernel actually read per level (resident graphs
+ * skip 256-record chunks whose records all had both ends visited at an
+ * earlier level: such a record can discover nothing, so depths are the
+ * same; a streamed graph reads every record of the swept tiles).  Same
+ * reference rule otherwise as gs_bfs_stats; no counterpart in the
+ * reference, which reads every record of a swept tile. */
+gs_status gs_bfs_records_read(gs_state* s, uint64_t* read_records, int max_levels, int* n_levels);
 
 /* BFS without any allocation (no counterpart in the reference; added for
  * callers that may not allocate device memory while they run queries, such

@@ -165,6 +165,10 @@ def test_kron_bfs_matches_oracle(kron, oracle_lib):
         assert np.array_equal(depth, depth_o), f"root {root}"
         assert st["level_counts"].tolist() == counts_o.tolist()
         assert st["swept"].tolist() == swept_o.tolist()
+        # records read: never more than the reference rule's swept tiles hold
+        # (fewer once chunks with every record's ends visited are skipped)
+        assert len(st["read"]) == len(st["swept"])
+        assert (st["read"] <= st["swept"]).all() and st["read"][:2].sum() == st["swept"][:2].sum()
 
 
 def test_kron_wcc_kcore_pr_match_oracle(kron, oracle_lib):
