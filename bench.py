@@ -1219,21 +1219,27 @@ def main():
     e_total = dist.reduce(float(e_comp), "sum")
     value = e_total / (ms_max / 1e3) / 1e9
     peak, peak_kind = measured_peak()
-    # algorithmic bytes: the records the sweep must read, 4 B each -- those
-    # of the tiles the reference's skip rule sweeps, less the chunks whose
-    # records all had both ends visited at an earlier level (they can
-    # discover nothing, and the kernel does not read them)
-    achieved = (4.0 * read_records) / (sweep_ms / 1e3) / 1e9 if sweep_ms > 0 else None
-    alg_per_launch = 4.0 * read_records / max(sweep_launches, 1)
+    # algorithmic bytes: 4 B x the records of the tiles the reference's skip
+    # rule sweeps at each level; the kernel reads fewer (it skips chunks
+    # whose records all had both ends visited at an earlier level: they can
+    # discover nothing), so the line also gives the bandwidth on the bytes
+    # it actually read
+    achieved = (4.0 * swept_records) / (sweep_ms / 1e3) / 1e9 if sweep_ms > 0 else None
+    alg_per_launch = 4.0 * swept_records / max(sweep_launches, 1)
+    read_per_launch = 4.0 * read_records / max(sweep_launches, 1)
+    achieved_read = read_per_launch * max(sweep_launches, 1) / (sweep_ms / 1e3) / 1e9 if sweep_ms > 0 else None
     rl = {"bound": "hbm", "kernel": "bfs_run_kernel", "achieved": achieved, "peak": peak,
           "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-          "traffic": BFS_DRAM_PER_ALG_BYTE * alg_per_launch,
-          "traffic_note": "bytes per launch: DRAM read+write per algorithmic byte from an ncu capture "
-                          "of a full level at scale 25, times this run's algorithmic bytes per launch",
-          "algorithmic_bytes": "4 B x records read per level: the reference rule's swept tiles, less "
-                               "256-record chunks whose records all had both ends visited at an earlier level",
+          "traffic": BFS_DRAM_PER_ALG_BYTE * read_per_launch,
+          "traffic_note": "bytes per launch: DRAM read+write per byte of records read, from an ncu capture "
+                          "of a full level at scale 25, times this run's records read per launch",
+          "algorithmic_bytes": "4 B x records in the tiles the reference's skip rule sweeps per level",
           "algorithmic_bytes_per_launch": alg_per_launch,
-          "reference_rule_bytes_per_launch": 4.0 * swept_records / max(sweep_launches, 1),
+          "read_bytes_per_launch": read_per_launch,
+          "read_note": "4 B x records the kernel read: the swept tiles less the 256-record chunks whose "
+                       "records all had both ends visited at an earlier level",
+          "achieved_on_bytes_read": achieved_read,
+          "frac_on_bytes_read": (achieved_read / peak) if achieved_read else None,
           "launches": sweep_launches, "sweep_ms_total": sweep_ms}
 
     line = {
