@@ -53,10 +53,10 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 HBM_FALLBACK_GBS = 6650.0
-# DRAM bytes (read + write) per algorithmic byte of the BFS sweep kernel,
+# DRAM bytes (read + write) per byte of records read by the BFS sweep kernel,
 # from one ncu capture of a full level at scale 25 (536,867,454 records):
-# 2,215.8 MB read + 22.4 MB written per 2,147.5 MB of records.
-BFS_DRAM_PER_ALG_BYTE = (2215.776 + 22.36288) / (536867454 * 4 / 1e6)
+# 2,210.0 MB read + 11.7 MB written per 2,147.5 MB of records.
+BFS_DRAM_PER_ALG_BYTE = (2210.042 + 11.718) / (536867454 * 4 / 1e6)
 PR_TOL = 1e-6      # relative L1 of FP32 PageRank against the FP64 oracle
 # pinned host memory a server reserves for results before it takes requests
 SERVE_ARENA_BYTES = 4 << 30
