@@ -857,6 +857,23 @@ gs_status gs_sweep(gs_state* s, const gs_segment* segs, int n_segs) {
         // traverse colours v1 from v0 only: its tiles follow their row window
         need.by_col = !g->directed && s->algo != GS_ALGO_TRAVERSE;
     }
+    std::vector<uint8_t> dead_units;
+    if (g->stream && s->algo == GS_ALGO_BFS && s->sweep_skip) {
+        // units whose chunks are all dead need not cross PCIe at all
+        dead_units.resize(g->U);
+        GS_CHECK_CUDA(ctx, cudaMemcpyAsync(dead_units.data(), s->d_dead, g->U, cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        for (uint64_t u = 0; u < g->U; ++u) {
+            const gs_unit& d = g->h_units[u];
+            const uint64_t b = d.rec_beg, e = d.rec_beg + d.n;
+            const uint64_t ab = std::min<uint64_t>((b + 3) & ~3ull, e);
+            const uint64_t ae = std::max<uint64_t>(e & ~3ull, ab);
+            const uint64_t n4 = (ae - ab) >> 2;
+            const uint32_t nch = n4 ? (uint32_t)((n4 + 63) >> 6) : 1u;   // the sweep kernel's chunks
+            dead_units[u] = dead_units[u] == ((1u << nch) - 1u) ? 1 : 0;
+        }
+        need.dead_units = dead_units.data();
+    }
     return gs_each_segment(g, need, s->step & 1, launch);
 }
 

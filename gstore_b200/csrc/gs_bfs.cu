@@ -439,6 +439,21 @@ gs_status bfs_sweep_begin(gs_state* s) {
     GS_CHECK_CUDA(ctx, (gs_smem_limit_once<bfs_run_kernel<false, false>>(ctx->device, (int)sizeof(BfsSmem))));
     GS_CHECK_CUDA(ctx, (gs_smem_limit_once<bfs_run_kernel<true, false>>(ctx->device, (int)sizeof(BfsSmem))));
     GS_CHECK_CUDA(ctx, (gs_smem_limit_once<bfs_run_kernel<true, true>>(ctx->device, (int)sizeof(BfsSmem))));
+    // Dead chunks: marking starts once at most 1/64 of the vertices with
+    // records are still unvisited (after the peak, when most chunks have no
+    // record left with an unvisited end) and goes on at every level after
+    // it, which also skips the chunks marked so far (a streamed graph's
+    // planner then leaves out the units whose chunks are all dead).  Only
+    // speed depends on this choice: a dead chunk can discover nothing.
+    uint64_t visited = 1;
+    for (uint64_t c : s->level_counts) visited += c;
+    const uint64_t unvisited = g->nonisolated > visited ? g->nonisolated - visited : 0;
+    const bool on = g->nonisolated_known && s->d_dead;
+    s->sweep_skip = on && s->marking;
+    s->sweep_mark = on && (s->marking || unvisited * 64 <= g->nonisolated);
+    if (s->sweep_mark) s->marking = true;
+    if (s->level_skip.size() < s->level) s->level_skip.resize(s->level, 0);
+    s->level_skip[s->level - 1] = s->sweep_skip ? 1 : 0;
     return GS_OK;
 }
 
@@ -448,19 +463,9 @@ gs_status bfs_sweep_launch(gs_state* s) {
     // every run of the resident graph, or the entries of the current segment
     const uint64_t n_runs = g->seg.list ? g->seg.n : (g->d_runs_lpt ? g->R_lpt : g->R);
     if (n_runs == 0) return GS_OK;
-    // Dead chunks are kept for resident graphs (a segment's records are
-    // copied whole whatever is skipped).  Marking starts once at most 1/64
-    // of the vertices with records are still unvisited (after the peak,
-    // when most chunks have no record left with an unvisited end) and goes
-    // on at every level after it, which also skips the chunks marked so
-    // far.  Only speed depends on this choice: a dead chunk can discover
-    // nothing.
-    uint8_t* dead = (g->seg.list || !g->nonisolated_known) ? nullptr : s->d_dead;
-    uint64_t visited = 1;
-    for (uint64_t c : s->level_counts) visited += c;
-    const uint64_t unvisited = g->nonisolated > visited ? g->nonisolated - visited : 0;
-    const bool mark = dead && (s->marking || unvisited * 64 <= g->nonisolated);
-    const bool skip = dead && s->marking;
+    // the level's mode (bfs_sweep_begin) holds for every segment of it
+    const bool mark = s->sweep_mark, skip = s->sweep_skip;
+    uint8_t* dead = mark ? s->d_dead : nullptr;
     RunArgs a{g->d_runs_lpt ? g->d_runs_lpt : g->d_runs, n_runs, g->d_units, g->seg.list ? g->seg.buf : g->d_rec,
               s->d_front, s->d_visited,
               s->d_act, s->d_act_next, g->directed, (int*)s->d_error, g->seg.list, s->d_ticket, dead,
@@ -470,9 +475,6 @@ gs_status bfs_sweep_launch(gs_state* s) {
     if (skip) bfs_run_kernel<true, true><<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
     else if (mark) bfs_run_kernel<true, false><<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
     else bfs_run_kernel<false, false><<<grid, kThreads, sizeof(BfsSmem), ctx->stream>>>(a);
-    if (mark) s->marking = true;
-    if (s->level_skip.size() < s->level) s->level_skip.resize(s->level, 0);
-    s->level_skip[s->level - 1] = skip ? 1 : 0;
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
     gs_timer_end(ctx, GS_ALGO_BFS, 0);

@@ -228,6 +228,7 @@ struct gs_state {
     uint32_t* d_ticket = nullptr;    // BFS sweep: run ticket, finished CTAs
     uint8_t* d_dead = nullptr;       // BFS: per unit, chunks with no record left to discover anything
     bool marking = false;            // BFS: dead chunks are being marked (and skipped)
+    bool sweep_mark = false, sweep_skip = false;   // BFS: this level's mode (set per sweep)
     std::vector<uint8_t> level_skip; // BFS: per level, dead chunks were skipped (records read counted)
     unsigned long long* d_read = nullptr;   // BFS: records read per level (256)
     uint8_t* d_act = nullptr;        // nw window flags (current)
@@ -350,6 +351,7 @@ gs_status kcore_finalize(gs_state* s, int64_t* frontier, int* done);
 struct gs_need {
     const uint8_t* act = nullptr;   // host window flags; null = every unit
     bool by_col = true;             // a unit is needed when its row or column window is active
+    const uint8_t* dead_units = nullptr;   // host, per unit: non-zero = no live chunk left (BFS); null = none
 };
 // Calls `launch` once per segment with g->seg set: for a streamed graph the
 // segments are planned from `need` and their records copied from pinned host

@@ -156,22 +156,25 @@ gs_status list_done(gs_graph* g, int k) {
 inline uint64_t unit_end_rec(const gs_unit& u) { return u.rec_beg + u.n; }
 
 // Entries (run, unit range) a sweep needs under `need`, in file order.
+// Units with no live chunk left (need.dead_units) are left out.
 void plan_entries(const gs_graph* g, const gs_need& need, std::vector<gs_seg_run>& out) {
     out.clear();
     const std::vector<gs_unit>& units = g->h_units;
     for (uint32_t r = 0; r < (uint32_t)g->R; ++r) {
         const gs_tile_run& run = g->h_runs[r];
         const uint32_t row = units[run.unit_beg].rc >> 16;
-        if (!need.act || need.act[row]) {
+        const bool row_on = !need.act || need.act[row];
+        if (row_on && !need.dead_units) {
             out.push_back(gs_seg_run{r, run.unit_beg, run.unit_end, 0, 0});
             continue;
         }
-        if (!need.by_col) continue;
+        if (!row_on && !need.by_col) continue;
         bool open = false;
         gs_seg_run cur{r, 0, 0, 0, 0};
         uint64_t cur_hi = 0;
         for (uint32_t u = run.unit_beg; u < run.unit_end; ++u) {
-            if (!need.act[units[u].rc & 0xFFFFu]) continue;
+            if (!row_on && !need.act[units[u].rc & 0xFFFFu]) continue;
+            if (need.dead_units && need.dead_units[u]) continue;
             if (open && units[u].rec_beg - cur_hi <= kGapRecords) {
                 cur.unit_end = u + 1;
             } else {
