@@ -1275,8 +1275,9 @@ def main():
                                                 "4E + 12V per iteration (records; x, s, inverse degree)")}
         keep = ours if leg else None
         for name, algo, arg, gid, kname, note in (
-                ("wcc", "wcc", 0, gs.GS_ALGO_WCC, "sweep_runs<WccOp>",
-                 "4E + 8V per sweep (records; parent read and write)"),
+                ("wcc", "wcc", 0, gs.GS_ALGO_WCC, "wcc_hook_runs (sampled pass + full pass)",
+                 "4E + 8V per sweep (records; parent read and write); the time covers the sampled "
+                 "hooking pass, the largest-tree bitmap and the full pass"),
                 ("kcore8", "kcore", 8, gs.GS_ALGO_KCORE, "sweep_runs<KcoreOp>",
                  "4 x records of the tiles with a removed end window + 8V per round")):
             t_ms, steps, count, (n, kms, kbytes) = time_algo(graph, timer, algo, arg, keep, key=name, kernel=gid)

@@ -243,6 +243,8 @@ struct gs_state {
     // WCC
     uint32_t* d_parent = nullptr;    // N
     uint8_t* d_touched = nullptr;    // N
+    uint32_t* d_giant = nullptr;     // N/32 + 2 words: largest sampled tree's bitmap, then its root
+    bool wcc_giant = false;          // d_giant was built by this run's first sweep
     // k-core
     int32_t* d_deg = nullptr;        // N
     uint32_t* d_kactive = nullptr;   // N/32

@@ -120,6 +120,25 @@ __device__ __forceinline__ uint32_t find_root(const uint32_t* parent, uint32_t v
     return v;
 }
 
+// find_root for kernels during which no tree is linked, so that roots stay
+// roots: `known` is a root this thread found before, and a vertex pointing at
+// it needs no second load.  After pointer jumping nearly every vertex of the
+// largest tree points at one root, whose own entry every warp of the grid
+// would otherwise read from a single L2 slice.  *first = parent[v].
+__device__ __forceinline__ uint32_t find_root_known(const uint32_t* parent, uint32_t v, uint32_t& known,
+                                                    uint32_t* first) {
+    uint32_t p = __ldcg(parent + v);
+    *first = p;
+    if (p == v || p == known) return p;
+    while (true) {
+        const uint32_t pp = __ldcg(parent + p);
+        if (pp == p) break;
+        p = pp;
+    }
+    known = p;
+    return p;
+}
+
 // find_root with path halving: every vertex passed on the way points to its
 // grandparent afterwards.  Only non-roots are written (a vertex that has a
 // parent never becomes a root again), always with one of their ancestors,
@@ -166,18 +185,25 @@ __device__ __forceinline__ bool hook(uint32_t* parent, uint32_t a, uint32_t b) {
 static __global__ void wcc_mark_touched(const uint32_t* __restrict__ parent, uint8_t* touched, uint64_t N) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    uint32_t last = ~0u;   // the parent marked last by this thread
     for (uint64_t v = tid; v < N; v += nth) {
         const uint32_t p = __ldcg(parent + v);
         if (p == v) continue;
         touched[v] = 1;
+        if (p == last) continue;
         if (!touched[p]) touched[p] = 1;   // read first: a component's root is every member's parent
+        last = p;
     }
 }
 
 struct WccOp {
     uint32_t* parent;
     uint8_t* touched;  // non-null on the first sweep
-    unsigned long long* changes;   // records the sweep left unresolved (zero: the forest is final)
+    unsigned long long* changes;   // records the sweep left unresolved (zero: the forest is final); may be null
+    // Optional bitmap of vertices already known to share one tree (the
+    // largest tree after a sampled hooking pass): a record with both ends in
+    // it joins nothing new and is skipped without a parent lookup.
+    const uint32_t* giant = nullptr;
     struct Item {
         uint32_t rb, cb;
         uint32_t n;
@@ -195,12 +221,15 @@ struct WccOp {
         // the sweeps (a vertex with a parent, or with a child); only a
         // self-loop leaves its end alone in its tree, so only it is marked here
         if (touched && a == b) touched[a] = 1;
+        if (giant && (bit_of(giant, a) & bit_of(giant, b))) return;
         // ends with one parent are in one tree (after pointer jumping most
         // vertices point at their root): two loads instead of four
         if (__ldcg(parent + a) == __ldcg(parent + b)) return;
         if (!hook(parent, a, b)) c.n += 1;
     }
-    __device__ void end(uint32_t, uint32_t, Item& c) const { warp_add_u64(changes, c.n); }
+    __device__ void end(uint32_t, uint32_t, Item& c) const {
+        if (changes) warp_add_u64(changes, c.n);
+    }
 };
 
 // ----------------------------------------------------------------- k-core --

@@ -14,6 +14,8 @@
 //   PR      pr.cpp:119-154      s[v1] += x[v0]; s[v0] += x[v1] (half grid)
 //   WCC     wcc.cpp:177-278     hook the larger root onto the smaller one
 //   k-core  kcore.cpp:63-177    --deg[other] for every removed endpoint
+#include <cstdlib>
+
 #include "gs_internal.cuh"
 #include "gs_ops.cuh"
 
@@ -65,10 +67,139 @@ __global__ void __launch_bounds__(kThreads) sweep_runs(const gs_tile_run* __rest
     }
 }
 
+// WCC hooking sweep of a resident graph (wcc.cpp:177-278, the rule of
+// WccOp) over a list of single-row runs, in two forms:
+//   * sampled (shift > 0): a warp hooks only every 2^shift-th 16-byte group
+//     (four records) of its unit, about 1/2^(shift-1) of the record sectors.
+//     It only builds trees early; which records it picks changes no result.
+//   * full (shift == 0): every record; with `giant` (the bitmap of the
+//     largest tree after the sampled pass), a record whose two ends are both
+//     in it joins nothing new and is skipped.  The run's row window of that
+//     bitmap (8 KB) is staged in shared memory, since row ends are scattered
+//     inside a tile; column ends come sorted and are read through L1.
+// The records that need their parents looked at go to a per-warp queue in
+// shared memory and are hooked 32 at a time, one per lane, so the few left
+// after the bitmap test do not run their dependent loads on a lane or two
+// of an otherwise idle warp.  The queue carries over units and runs and is
+// emptied before the CTA leaves.
+constexpr uint32_t kWindowWords = (1u << kTileBits) / 32;
+constexpr int kWccHookCtasPerSm = 6;
+__global__ void __launch_bounds__(kThreads, kWccHookCtasPerSm) wcc_hook_runs(const gs_tile_run* __restrict__ runs, uint64_t n_runs,
+                                                          const gs_unit* __restrict__ units,
+                                                          const uint32_t* __restrict__ rec, uint32_t* parent,
+                                                          uint8_t* touched, const uint32_t* __restrict__ giant,
+                                                          unsigned long long* changes, uint32_t shift,
+                                                          unsigned int* ticket) {
+    constexpr uint32_t kWarps = kThreads / 32;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    __shared__ unsigned long long s_run;
+    __shared__ __align__(16) uint32_t s_row[kWindowWords];
+    __shared__ uint2 s_q[kWarps][64];
+    uint2* q = s_q[warp];
+    uint32_t qn = 0;   // warp-uniform queue length (< 32 between pushes)
+    uint32_t staged = ~0u, unresolved = 0;
+    auto advance = [&]() -> uint64_t {
+        __syncthreads();   // every thread has read the previous draw and is done with s_row
+        if (threadIdx.x == 0) s_run = atomicAdd(ticket, 1u);
+        __syncthreads();
+        return s_run;
+    };
+    auto hook_pair = [&](uint32_t a, uint32_t b) {
+        if (__ldcg(parent + a) == __ldcg(parent + b)) return;   // one tree already
+        if (!gsops::hook(parent, a, b)) unresolved += 1;
+    };
+    // warp-collective: queue (a, b) where need is set; hook 32 once 32 wait
+    auto push = [&](bool need, uint32_t a, uint32_t b) {
+        const uint32_t bal = __ballot_sync(kFull, need);
+        if (need) q[qn + __popc(bal & lt)] = make_uint2(a, b);
+        qn += __popc(bal);
+        if (qn >= 32) {
+            __syncwarp();
+            const uint2 mine = q[lane];
+            const uint2 rest = lane + 32 < qn ? q[lane + 32] : make_uint2(0, 0);
+            __syncwarp();
+            if (lane + 32 < qn) q[lane] = rest;
+            qn -= 32;
+            hook_pair(mine.x, mine.y);
+            __syncwarp();
+        }
+    };
+    for (uint64_t i = advance(); i < n_runs; i = advance()) {
+        const uint32_t ub = runs[i].unit_beg, ue = runs[i].unit_end;
+        if (ub >= ue) continue;
+        const uint32_t row = units[ub].rc >> 16;
+        if (giant && row != staged) {
+            const uint4* src = reinterpret_cast<const uint4*>(giant + (uint64_t)row * kWindowWords);
+            for (uint32_t k = threadIdx.x; k < kWindowWords / 4; k += kThreads)
+                reinterpret_cast<uint4*>(s_row)[k] = __ldg(src + k);
+            staged = row;
+            __syncthreads();
+        }
+        const uint32_t rb = row << kTileBits;
+        for (uint32_t ui = ub + warp; ui < ue; ui += kWarps) {
+            const gs_unit d = units[ui];
+            const uint32_t cb = (d.rc & 0xFFFFu) << kTileBits;
+            const uint32_t* gcol = giant ? giant + (cb >> 5) : nullptr;
+            // does record r (valid on this lane) need its parents looked at?
+            auto need = [&](bool valid, uint32_t r) -> bool {
+                if (!valid) return false;
+                const uint32_t al = r & 0xFFFFu, bl = r >> 16;
+                if (touched && al + rb == bl + cb) touched[al + rb] = 1;   // wcc.cpp:203-217 (self-loop)
+                if (!giant) return true;
+                return !((s_row[al >> 5] >> (al & 31)) & (__ldg(gcol + (bl >> 5)) >> (bl & 31)) & 1u);
+            };
+            auto visit = [&](bool valid, uint32_t r) {
+                push(need(valid, r), rb + (r & 0xFFFFu), cb + (r >> 16));
+            };
+            const uint64_t b = d.rec_beg, e = d.rec_beg + d.n;
+            uint64_t ab = (b + 3) & ~3ull;
+            if (ab > e) ab = e;
+            uint64_t ae = e & ~3ull;
+            if (ae < ab) ae = ab;
+            if (shift == 0) {
+                visit(b + lane < ab, b + lane < ab ? __ldcs(rec + b + lane) : 0u);
+                visit(ae + lane < e, ae + lane < e ? __ldcs(rec + ae + lane) : 0u);
+            }
+            const uint4* r4 = reinterpret_cast<const uint4*>(rec + ab);
+            const uint32_t n4 = (uint32_t)((ae - ab) >> 2);
+            const uint32_t stride = 32u << shift, off = lane << shift;
+            const uint4 z = make_uint4(0, 0, 0, 0);
+            uint4 g = off < n4 ? load_stream(r4 + off) : z;
+            for (uint32_t k0 = 0; k0 < n4; k0 += stride) {   // warp-uniform
+                const bool valid = k0 + off < n4;
+                const uint32_t kn = k0 + stride + off;
+                const uint4 gn = kn < n4 ? load_stream(r4 + kn) : z;   // next group in flight
+                const bool n0 = need(valid, g.x), n1 = need(valid, g.y), n2 = need(valid, g.z),
+                           n3 = need(valid, g.w);
+                if (__any_sync(kFull, n0 | n1 | n2 | n3)) {
+                    push(n0, rb + (g.x & 0xFFFFu), cb + (g.x >> 16));
+                    push(n1, rb + (g.y & 0xFFFFu), cb + (g.y >> 16));
+                    push(n2, rb + (g.z & 0xFFFFu), cb + (g.z >> 16));
+                    push(n3, rb + (g.w & 0xFFFFu), cb + (g.w >> 16));
+                }
+                g = gn;
+            }
+        }
+    }
+    __syncwarp();
+    if (lane < qn) {
+        const uint2 mine = q[lane];
+        hook_pair(mine.x, mine.y);
+    }
+    if (changes) warp_add_u64(changes, unresolved);
+    if (threadIdx.x == 0 && atomicAdd(ticket + 1, 1u) == gridDim.x - 1) {
+        atomicExch(ticket, 0u);   // every CTA has drawn its last ticket
+        atomicExch(ticket + 1, 0u);
+    }
+}
+
 // Sweeps the whole resident graph, or, during a streamed sweep, the runs of
-// the segment the graph points at.
+// the segment the graph points at.  timed = false leaves the kernel timer to
+// the caller (a phase of several launches timed as one).
 template <class Op>
-gs_status launch_sweep(gs_graph* g, const Op& op, int algo, uint64_t bytes, bool blocked = false) {
+gs_status launch_sweep(gs_graph* g, const Op& op, int algo, uint64_t bytes, bool blocked = false,
+                       bool timed = true) {
     gs_ctx* ctx = g->ctx;
     const gs_seg_run* seg = g->seg.list;
     if (blocked && !seg) GS_TRY(gs_ensure_blocked(g));
@@ -77,13 +208,13 @@ gs_status launch_sweep(gs_graph* g, const Op& op, int algo, uint64_t bytes, bool
     const uint32_t* rec = seg ? g->seg.buf : g->d_rec;
     if (n == 0) return GS_OK;
     const uint32_t grid = (uint32_t)std::min<uint64_t>(n, gs_grid_size(ctx, 8));
-    gs_timer_begin(ctx);
+    if (timed) gs_timer_begin(ctx);
     sweep_runs<Op><<<grid, kThreads, 0, ctx->stream>>>(blocked ? g->d_runs_blk : g->d_runs, n,
                                                         blocked ? g->d_units_blk : g->d_units, rec, seg, op,
                                                         ctx->d_ticket);
     GS_CHECK_CUDA(ctx, cudaGetLastError());
     ctx->launches++;
-    gs_timer_end(ctx, algo, seg ? 0 : bytes);
+    if (timed) gs_timer_end(ctx, algo, seg ? 0 : bytes);
     return GS_OK;
 }
 
@@ -200,9 +331,57 @@ __global__ void iota_kernel(uint32_t* parent, uint64_t N) {
 __global__ void compress_kernel(uint32_t* parent, uint64_t N) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    uint32_t known = ~0u, first;
     for (uint64_t v = tid; v < N; v += nth) {
-        const uint32_t r = find_root(parent, (uint32_t)v);
-        if (r != v) parent[v] = r;
+        const uint32_t r = find_root_known(parent, (uint32_t)v, known, &first);
+        if (r != first) parent[v] = r;
+    }
+}
+
+// After the sampled hooking pass: the root shared by most of 1,024 vertices
+// drawn with a fixed splitmix64 stream (vertices still alone in their tree
+// do not vote), written to *root_out (~0u when none has a tree yet).  One
+// CTA of kGiantSamples threads.  Which root wins changes no result: it only
+// picks the tree whose records the full sweep may skip.
+constexpr int kGiantSamples = 1024;
+__global__ void __launch_bounds__(kGiantSamples) wcc_giant_root_kernel(const uint32_t* parent, uint64_t V,
+                                                                        uint32_t* root_out) {
+    __shared__ uint32_t s_root[kGiantSamples];
+    __shared__ unsigned long long s_best;
+    const uint32_t t = threadIdx.x;
+    uint64_t z = (uint64_t)(t + 1) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const uint32_t v = (uint32_t)(z % V);
+    const uint32_t r = find_root(parent, v);
+    const uint32_t mine = r == v ? ~0u : r;   // a root votes for no tree (its own is rarely the largest)
+    s_root[t] = mine;
+    if (t == 0) s_best = 0;
+    __syncthreads();
+    uint32_t n = 0;
+    if (mine != ~0u)
+        for (int i = 0; i < kGiantSamples; ++i) n += s_root[i] == mine;
+    if (n) atomicMax(&s_best, ((unsigned long long)n << 32) | mine);
+    __syncthreads();
+    if (t == 0) *root_out = s_best ? (uint32_t)s_best : ~0u;
+}
+
+// Pointer jumping as compress_kernel, and the bitmap of the vertices whose
+// root is *root (the largest sampled tree): bit v & 31 of word v >> 5.
+// Warps take whole 32-vertex words (N is a multiple of 65,536).
+__global__ void wcc_compress_giant_kernel(uint32_t* parent, uint32_t* giant, const uint32_t* root, uint64_t N) {
+    const uint32_t c = *root;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t nwords = N >> 5;
+    const uint64_t step = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    uint32_t known = c, first;   // c is a root: the sampled pass is over
+    for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nwords; w += step) {
+        const uint32_t v = (uint32_t)(w * 32 + lane);
+        const uint32_t r = find_root_known(parent, v, known, &first);
+        if (r != first) parent[v] = r;
+        const uint32_t bits = __ballot_sync(kFull, r == c);
+        if (lane == 0) giant[w] = bits;
     }
 }
 
@@ -211,12 +390,13 @@ __global__ void wcc_label_kernel(const uint32_t* parent, const uint8_t* touched,
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
     uint64_t local = 0;
+    uint32_t known = ~0u, first;
     for (uint64_t v = tid; v < N; v += nth) {
         if (!touched[v]) {
             out[v] = 0xFFFFFFFFu;  // invalid_cid, wcc.cpp:54
             continue;
         }
-        const uint32_t r = find_root(parent, (uint32_t)v);
+        const uint32_t r = find_root_known(parent, (uint32_t)v, known, &first);
         out[v] = r;
         local += (r == v);
     }
@@ -492,11 +672,67 @@ gs_status wcc_init(gs_state* s) {
 
 gs_status wcc_sweep_begin(gs_state* s) { return zero_scalar(s->g->ctx); }
 
+// The sampled pass of a resident graph's first WCC sweep: one 16-byte group
+// of records in every 2^shift (GS_WCC_SAMPLE_SHIFT overrides the default;
+// 0 turns the pass off), on graphs of at least kWccSampleMinRecords records.
+constexpr uint32_t kWccSampleShift = 4;
+constexpr uint64_t kWccSampleMinRecords = 1ull << 22;
+
+uint32_t wcc_sample_shift(const gs_graph* g) {
+    if (g->seg.list || g->E < kWccSampleMinRecords) return 0;
+    const char* e = std::getenv("GS_WCC_SAMPLE_SHIFT");
+    if (!e || !*e) return kWccSampleShift;
+    const long v = std::strtol(e, nullptr, 10);
+    return v <= 0 ? 0u : (uint32_t)std::min<long>(v, 10);
+}
+
 gs_status wcc_sweep_launch(gs_state* s) {
     gs_graph* g = s->g;
-    WccOp op{s->d_parent, s->step == 0 ? s->d_touched : nullptr,
-             (unsigned long long*)g->ctx->d_scalars};
-    return launch_sweep(g, op, GS_ALGO_WCC, 4 * g->E + 8 * g->V, true);
+    gs_ctx* ctx = g->ctx;
+    const uint64_t bytes = 4 * g->E + 8 * g->V;
+    const uint32_t shift = s->step == 0 ? wcc_sample_shift(g) : 0;
+    if (shift == 0) {
+        // later sweeps (only after a record ran out of hooking retries) keep
+        // the first sweep's bitmap: its vertices still share one tree
+        if (s->step == 0) s->wcc_giant = false;
+        WccOp op{s->d_parent, s->step == 0 ? s->d_touched : nullptr, (unsigned long long*)ctx->d_scalars,
+                 s->wcc_giant ? s->d_giant : nullptr};
+        return launch_sweep(g, op, GS_ALGO_WCC, bytes, true);
+    }
+    // Afforest's order (Sutton, Ben-Nun, Barak, "Optimizing Parallel Graph
+    // Connectivity Computation via Subgraph Sampling", IPDPS 2018), restated
+    // for the tile grid: hook a sample of the records, find the largest tree,
+    // then sweep every record, skipping those with both ends in that tree.
+    GS_TRY(gs_ensure_blocked(g));
+    if (!s->d_giant) GS_TRY(gs_state_alloc(s, (void**)&s->d_giant, (g->N / 32 + 2) * 4));
+    uint32_t* d_root = s->d_giant + g->N / 32;
+    // the sampled pass walks the L2-blocked runs (its hooks land on parents
+    // of a few windows at a time); the full pass walks the longest-first runs
+    // of the BFS sweep (one row window staged per long run), since few of
+    // its records reach the parents
+    const bool blk = g->d_runs_blk != nullptr;
+    const uint64_t n = blk ? g->R_blk : g->R;
+    const bool lpt = g->d_runs_lpt != nullptr;
+    const uint64_t n_full = lpt ? g->R_lpt : g->R;
+    const uint32_t grid =
+        (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n, gs_grid_size(ctx, kWccHookCtasPerSm)));
+    const uint32_t grid_full =
+        (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n_full, gs_grid_size(ctx, kWccHookCtasPerSm)));
+    gs_timer_begin(ctx);
+    wcc_hook_runs<<<grid, kThreads, 0, ctx->stream>>>(blk ? g->d_runs_blk : g->d_runs, n,
+                                                      blk ? g->d_units_blk : g->d_units, g->d_rec, s->d_parent,
+                                                      nullptr, nullptr, nullptr, shift, ctx->d_ticket);
+    wcc_giant_root_kernel<<<1, kGiantSamples, 0, ctx->stream>>>(s->d_parent, g->V, d_root);
+    wcc_compress_giant_kernel<<<blocks_for(g->N, ctx), kThreads, 0, ctx->stream>>>(s->d_parent, s->d_giant,
+                                                                                    d_root, g->N);
+    wcc_hook_runs<<<grid_full, kThreads, 0, ctx->stream>>>(lpt ? g->d_runs_lpt : g->d_runs, n_full, g->d_units,
+                                                           g->d_rec, s->d_parent, s->d_touched, s->d_giant,
+                                                           (unsigned long long*)ctx->d_scalars, 0, ctx->d_ticket);
+    GS_CHECK_CUDA(ctx, cudaGetLastError());
+    ctx->launches += 4;
+    s->wcc_giant = true;
+    gs_timer_end(ctx, GS_ALGO_WCC, bytes);
+    return GS_OK;
 }
 
 gs_status wcc_finalize(gs_state* s, int64_t* frontier, int* done) {

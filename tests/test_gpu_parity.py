@@ -186,6 +186,32 @@ def test_kron_wcc_kcore_pr_match_oracle(kron, oracle_lib):
     assert rel_l1(r, r64) <= PR_TOL and rel_l1(x, x64) <= PR_TOL
 
 
+@pytest.mark.parametrize("shift", ["0", "1", "4", "8"])
+def test_kron_wcc_sampled_pass_matches_oracle(kron, oracle_lib, monkeypatch, shift):
+    """WCC on a resident graph of >= 2^22 records hooks a sample of the
+    records first (one 16-byte group in 2^shift), then sweeps every record
+    but those with both ends in the largest sampled tree.  The sample only
+    changes the order in which trees are linked: the labels (the smallest
+    vertex of each component, wcc.cpp:372-390) and the count must equal the
+    oracle's for any sample size, shift 0 being the plain sweep."""
+    monkeypatch.setenv("GS_WCC_SAMPLE_SHIFT", shift)
+    k = kron[20]
+    p, _, _ = oracle_lib.geometry(k["V"])
+    lab_o, n_o = oracle_lib.wcc(k["start"], k["grid"], p, False, k["V"])
+    before = k["graph"].ctx.launches()
+    with k["graph"].state("wcc", 0) as s:
+        assert s.run() == 1                      # one sweep call, whatever the sample
+        lab, n = s.download(0), s.count()
+        s.reset(0)                               # a second run on the same state
+        s.run()
+        assert np.array_equal(s.download(0), lab)
+    assert np.array_equal(lab, lab_o) and n == n_o
+    # the sampled form launches the sample, the largest-tree vote, the
+    # bitmap and the full pass in place of one sweep
+    launches = k["graph"].ctx.launches() - before
+    assert launches >= (2 * 6 if shift != "0" else 2 * 3)
+
+
 def test_step_protocol_matches_run(kron):
     """algo_t protocol: sweep()/finalize() step by step equals run()."""
     g = kron[16]["graph"]
