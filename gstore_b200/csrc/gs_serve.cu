@@ -390,9 +390,11 @@ struct gs_server {
     double phase_s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     double side_in_wait_s = 0;           // side tending inside the step wait
     std::chrono::steady_clock::time_point t0;
-    // device pool: exact-size free lists
+    // device pool: exact-size free lists over blocks drawn from the
+    // context's pool, which gets them all back when the server is freed (a
+    // later server, batch or query state of the context reuses them)
     std::multimap<size_t, void*> dev_free;
-    std::vector<void*> dev_all;
+    std::vector<std::pair<void*, size_t>> dev_all;
     // pinned host arena for results: chunks from cudaHostAlloc, carved
     // best-fit into page-rounded blocks; a freed block merges with free
     // neighbours of the same chunk
@@ -421,10 +423,13 @@ gs_status pool_dev(gs_server* s, size_t bytes, void** out) {
         return GS_OK;
     }
     const double t = now_s(s);
-    GS_TRY(gs_dev_alloc(s->ctx, out, bytes));
-    s->phase_s[6] += now_s(s) - t;
-    s->phase_s[7] += 1;
-    s->dev_all.push_back(*out);
+    const uint64_t held = s->ctx->pool_bytes;
+    GS_TRY(gs_pool_get(s->ctx, bytes, out));
+    if (s->ctx->pool_bytes == held) {   // the context's pool had no such block: cudaMalloc ran
+        s->phase_s[6] += now_s(s) - t;
+        s->phase_s[7] += 1;
+    }
+    s->dev_all.emplace_back(*out, bytes);
     return GS_OK;
 }
 
@@ -1286,7 +1291,7 @@ gs_status gs_serve_free(gs_server* s) {
     s->reqs.clear();   // drops result buffers into the host pool
     if (s->step_exec) cudaGraphExecDestroy(s->step_exec);
     if (s->step_graph) cudaGraphDestroy(s->step_graph);
-    for (void* p : s->dev_all) gs_dev_free(p);
+    for (auto& pb : s->dev_all) gs_pool_put(s->ctx, pb.first, pb.second);
     for (auto& c : s->host_chunks) cudaFreeHost(c.first);
     gs_dev_free(s->d_table);
     gs_dev_free(s->d_cnt);
