@@ -537,7 +537,8 @@ struct gs_batch_query {
     uint32_t* removed = nullptr;
     uint8_t* act = nullptr;
     unsigned long long* cnt = nullptr;
-    // PageRank: a plain state
+    // PageRank, and WCC on graphs whose plain WCC hooks a sample first: a
+    // plain state (the query runs through gs_run)
     gs_state* pr = nullptr;
 };
 
@@ -939,6 +940,11 @@ gs_status gs_batch_run(gs_batch* b) {
         switch (b->q[i].algo) {
             case GS_ALGO_BFS: bfs.push_back((int)i); break;
             case GS_ALGO_WCC:
+                // the plain WCC's sampled pass (bitmap in shared memory, L1
+                // reads) beats the persistent kernel's one hooking sweep
+                if (gs_wcc_sample_shift(qi.g) > 0) pr.push_back((int)i);
+                else wk.push_back((int)i);
+                break;
             case GS_ALGO_KCORE: wk.push_back((int)i); break;
             default: pr.push_back((int)i); break;
         }
@@ -948,11 +954,12 @@ gs_status gs_batch_run(gs_batch* b) {
     GS_TRY(run_wk_queries(b, wk));
     for (int i : pr) {
         gs_batch_query& q = b->q[i];
-        GS_TRY(gs_state_create(q.g, GS_ALGO_PAGERANK, q.arg, &q.pr));
+        GS_TRY(gs_state_create(q.g, q.algo, q.arg, &q.pr));
         int64_t steps = 0;
         GS_TRY(gs_run(q.pr, &steps));
         q.sweeps = steps;
         q.ran = true;
+        b->launches += 1;   // one plain run (its sweeps and finalizes)
     }
     return GS_OK;
 }
@@ -963,7 +970,7 @@ gs_status gs_batch_download(gs_batch* b, int query_id, int what, void* host_dst,
     if (!host_dst) return GS_ERR_ARG;
     gs_ctx* ctx = b->ctx;
     gs_graph* g = q->g;
-    if (q->algo == GS_ALGO_PAGERANK) return gs_download(q->pr, what, host_dst, bytes);
+    if (q->pr) return gs_download(q->pr, what, host_dst, bytes);
     const uint64_t need = q->algo == GS_ALGO_BFS ? g->V : g->V * 4;
     if (bytes < need) return gs_fail(ctx, GS_ERR_ARG, "destination too small: need " + std::to_string(need));
     void* tmp = nullptr;
@@ -992,7 +999,7 @@ gs_status gs_batch_result_count(gs_batch* b, int query_id, uint64_t* count) {
     if (!count) return GS_ERR_ARG;
     gs_ctx* ctx = b->ctx;
     gs_graph* g = q->g;
-    if (q->algo == GS_ALGO_PAGERANK) return gs_result_count(q->pr, count);
+    if (q->pr) return gs_result_count(q->pr, count);
     if (q->algo == GS_ALGO_BFS) {
         GS_TRY(gs_batch_bfs_levels(b, query_id, nullptr, 0, nullptr));
         const uint64_t* h = b->groups[q->group].hist.data() + (size_t)q->lane * 256;

@@ -342,6 +342,10 @@ gs_status pr_finalize(gs_state* s, int64_t* frontier, int* done);
 gs_status wcc_init(gs_state* s);
 gs_status wcc_sweep_begin(gs_state* s);
 gs_status wcc_sweep_launch(gs_state* s);
+// Sample of the first WCC sweep on graph g (one 16-byte record group in
+// 2^shift hooked before the full pass); 0 = the plain one-sweep form
+// (streamed graphs, graphs under 2^22 records, or GS_WCC_SAMPLE_SHIFT=0).
+uint32_t gs_wcc_sample_shift(const gs_graph* g);
 gs_status wcc_finalize(gs_state* s, int64_t* frontier, int* done);
 
 gs_status kcore_init(gs_state* s);

@@ -678,7 +678,7 @@ gs_status wcc_sweep_begin(gs_state* s) { return zero_scalar(s->g->ctx); }
 constexpr uint32_t kWccSampleShift = 4;
 constexpr uint64_t kWccSampleMinRecords = 1ull << 22;
 
-uint32_t wcc_sample_shift(const gs_graph* g) {
+uint32_t gs_wcc_sample_shift(const gs_graph* g) {
     if (g->seg.list || g->E < kWccSampleMinRecords) return 0;
     const char* e = std::getenv("GS_WCC_SAMPLE_SHIFT");
     if (!e || !*e) return kWccSampleShift;
@@ -690,7 +690,7 @@ gs_status wcc_sweep_launch(gs_state* s) {
     gs_graph* g = s->g;
     gs_ctx* ctx = g->ctx;
     const uint64_t bytes = 4 * g->E + 8 * g->V;
-    const uint32_t shift = s->step == 0 ? wcc_sample_shift(g) : 0;
+    const uint32_t shift = s->step == 0 ? gs_wcc_sample_shift(g) : 0;
     if (shift == 0) {
         // later sweeps (only after a record ran out of hooking retries) keep
         // the first sweep's bitmap: its vertices still share one tree

@@ -255,8 +255,11 @@ gs_status gs_bfs_noalloc(gs_graph* g, uint64_t root, uint8_t* d_depth, int64_t* 
  * launches: BFS roots on the same graph run as a multi-source BFS (one bit
  * per query in 32- or 64-bit frontier words, one persistent launch per
  * group, word width and tile order picked per graph by a measuring
- * autotuner); all WCC and k-core queries, over any graphs, share one
- * persistent launch; PageRank queries run as plain gs_run; identical queries
+ * autotuner); all k-core queries, and WCC queries on graphs of fewer
+ * than 2^22 records, over any graphs, share one persistent launch; WCC
+ * queries on larger graphs (whose plain WCC hooks a sample of the records
+ * first and then skips the records inside the largest tree) and PageRank
+ * queries run as plain gs_run; identical queries
  * (same graph, algorithm and argument) run once.  Results per
  * query equal gs_run's on the same graph and argument (BFS depth, WCC
  * labels, k-core degrees bit for bit).  arg: BFS root, k-core k, PageRank
@@ -273,7 +276,9 @@ gs_status gs_batch_result_count(gs_batch* b, int query_id, uint64_t* count);
  * counts; the last level found none). */
 gs_status gs_batch_bfs_levels(gs_batch* b, int query_id, uint64_t* level_counts, int max_levels,
                               int* n_levels);
-/* Persistent launches made and their device time so far. */
+/* Launches so far: the persistent launches plus one per query run as a
+ * plain gs_run (PageRank, and WCC on graphs of >= 2^22 records); kernel_ms
+ * is the persistent launches' device time. */
 gs_status gs_batch_stats(const gs_batch* b, uint64_t* launches, double* kernel_ms);
 gs_status gs_batch_free(gs_batch* b);
 
