@@ -679,7 +679,7 @@ constexpr uint32_t kWccSampleShift = 4;
 constexpr uint64_t kWccSampleMinRecords = 1ull << 22;
 
 uint32_t gs_wcc_sample_shift(const gs_graph* g) {
-    if (g->seg.list || g->E < kWccSampleMinRecords) return 0;
+    if (g->stream || g->seg.list || g->E < kWccSampleMinRecords) return 0;
     const char* e = std::getenv("GS_WCC_SAMPLE_SHIFT");
     if (!e || !*e) return kWccSampleShift;
     const long v = std::strtol(e, nullptr, 10);
